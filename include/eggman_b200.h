@@ -1,0 +1,151 @@
+/*
+ * eggman_b200.h -- C ABI of libeggman_b200.so, the B200 (sm_100a) engine behind TheEggman.jl's
+ * two hafnian hot paths: the subset DP and the Bjorklund/Glynn sieve.
+ *
+ * Conventions (all entry points):
+ *   - Every function returns an int status: EGG_OK (0) or one of the EGG_ERR_* codes below.
+ *     Nothing throws or aborts across the ABI; egg_last_error() gives a message for the calling
+ *     thread's last failure.
+ *   - Pointers are plain host pointers unless the name ends in _device (then device pointers and
+ *     a cudaStream_t passed as void*).  Inputs are borrowed for the call only.
+ *   - Matrices are column-major (Julia order); complex values are interleaved (re, im) pairs of
+ *     the real type, exactly as Julia lays out Complex{Float64}/Complex{Float32}.
+ *   - One device context per process and one internal lock, mirroring the reference's
+ *     _DEVICE_PLAN_LOCK (src/dp.jl:542): calls are serialised and synchronous to the caller.
+ *   - The library never falls back to a CPU implementation.
+ */
+#ifndef EGGMAN_B200_H
+#define EGGMAN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+#define EGG_OK 0
+#define EGG_ERR_ARGUMENT 1   /* bad argument value (the reference's ArgumentError) */
+#define EGG_ERR_DIMENSION 2  /* inconsistent sizes (the reference's DimensionMismatch) */
+#define EGG_ERR_TOO_LARGE 3  /* plan or batch cannot be represented / would not fit (src/dp.jl:224-243) */
+#define EGG_ERR_NO_PLAN 4    /* no device plan resident for (K, layout): upload or build one first */
+#define EGG_ERR_CUDA 5       /* a CUDA runtime call failed */
+#define EGG_ERR_TIMEOUT 6    /* a bounded device wait ran out */
+#define EGG_ERR_NO_DEVICE 7  /* no usable CUDA device */
+#define EGG_ERR_PLAN_INVALID 8 /* an uploaded plan failed the device-side structure check */
+
+/* ---- element types ----------------------------------------------------------------------- */
+#define EGG_F64 0   /* Float64 */
+#define EGG_C128 1  /* ComplexF64 */
+#define EGG_F32 2   /* Float32 */
+#define EGG_C64 3   /* ComplexF32 */
+#define EGG_I64 4   /* Int64 entries; DP states and results are Int128 (two int64 words, low first) */
+
+/* ---- DP precision modes ------------------------------------------------------------------ */
+#define EGG_PREC_EXACT 0  /* one thread per state, plan order, no FMA contraction: bit-identical to
+                             the reference's CPU _dp_states! (src/dp.jl:344-363) */
+#define EGG_PREC_FMA 1    /* plan order with fused multiply-add (the reference GPU kernel's rounding,
+                             ext/TheEggmanKernelAbstractionsExt.jl:47-51) */
+#define EGG_PREC_MIXED 2  /* FP32 multiplies, FP64 per-state accumulation, FP32 state storage
+                             (F64/C128 inputs only) */
+
+/* ---- library ----------------------------------------------------------------------------- */
+
+/* Library version string. */
+const char *egg_version(void);
+
+/* Message describing the calling thread's most recent failure ("" if none). */
+const char *egg_last_error(void);
+
+/* Select the CUDA device (idempotent; the first call of any other entry point does this with
+ * device 0).  Fails with EGG_ERR_NO_DEVICE if there is none. */
+int egg_init(int device);
+
+/* Device bytes held by resident plans and reusable work buffers.
+ * Replaces gpu_cache_bytes(), src/dp.jl:552-560. */
+int64_t egg_cache_bytes(void);
+
+/* Release every resident plan and work buffer.  Replaces empty_gpu_cache!(), src/dp.jl:567-573. */
+int egg_cache_clear(void);
+
+/* Device bytes one DP batch needs besides the shared plan: B x (nstates + npairs) elements of
+ * the given type.  Replaces dp_batch_bytes(N, T, B), src/dp.jl:584-587.  Returns -1 on a bad
+ * argument. */
+int64_t egg_dp_batch_bytes(int N, int dtype, int64_t B);
+
+/* ---- subset DP plans (HafnianDPPlan{I}, src/dp.jl:150-156) -------------------------------- */
+
+/* Closed-form plan size, _dp_counts(K) (src/dp.jl:192-208). */
+int egg_dp_counts(int K, int64_t *nstates, int64_t *ntrans);
+
+/* Copy a host-built plan to the device and keep it resident, keyed by (K, idx_bytes).
+ * idx_bytes is 4 (Int32 layout, pair bits 9) or 8 (Int64, pair bits 12); arrays are the
+ * reference's 1-based starts[nstates+1], trans[ntrans], levels[nlevels].  Idempotent: a
+ * resident plan for the key is kept.  The structure is checked on the device (every child in
+ * the previous level, every pair index in 1..K(K-1)/2, uniform out-degree per level) and a plan
+ * that fails is refused with EGG_ERR_PLAN_INVALID.
+ * Replaces _device_plan(backend, plan), ext/TheEggmanKernelAbstractionsExt.jl:31-42. */
+int egg_plan_upload(int K, int idx_bytes, const void *starts, const void *trans, const void *levels,
+                    int64_t nlevels, int64_t nstates, int64_t ntrans);
+
+/* Build the degree-K plan directly in device memory, laid out exactly as _build_dp_plan(K, I)
+ * (src/dp.jl:223-304) would, by combinatorial ranking of the level subsets.  Same key and
+ * caching as egg_plan_upload; refuses what the reference refuses (src/dp.jl:224-234) with
+ * EGG_ERR_TOO_LARGE, and plans that would not fit in free device memory likewise. */
+int egg_plan_build(int K, int idx_bytes);
+
+/* Sizes of a resident plan (EGG_ERR_NO_PLAN if absent). */
+int egg_plan_info(int K, int idx_bytes, int64_t *nstates, int64_t *ntrans, int64_t *nlevels,
+                  int64_t *device_bytes);
+
+/* Copy a resident plan back to the host in the reference layout (starts[nstates+1],
+ * trans[ntrans], levels[nlevels], element size idx_bytes). */
+int egg_plan_download(int K, int idx_bytes, void *starts, void *trans, void *levels);
+
+/* Drop one resident plan. */
+int egg_plan_release(int K, int idx_bytes);
+
+/* ---- subset DP evaluation ---------------------------------------------------------------- */
+
+/* Hafnians of B instances of degree K on the resident (K, idx_bytes) plan.
+ * P is the host B x npairs gathered-pair matrix of _gather_pairs_batch (src/dp.jl:479-512),
+ * column-major with the instance index fastest (element (b, q) at b + q*B), npairs = K(K-1)/2;
+ * out receives B values (EGG_I64: B Int128 values).  max_batch > 0 evaluates in chunks of at
+ * most that many instances (0: one chunk).  prec is an EGG_PREC_* mode.
+ * Replaces _haf_dp_backend(backend, P, plan; max_batch),
+ * ext/TheEggmanKernelAbstractionsExt.jl:90-146 (hook declared at src/dp.jl:525). */
+int egg_dp_batch(int K, int idx_bytes, int dtype, int prec, const void *P, int64_t B, int64_t max_batch,
+                 void *out);
+
+/* As egg_dp_batch with P and out in device memory, enqueued on `stream` (a cudaStream_t; NULL
+ * for the library's own stream) without a host synchronisation. */
+int egg_dp_batch_device(int K, int idx_bytes, int dtype, int prec, const void *P, int64_t B, void *out,
+                        void *stream);
+
+/* ---- Bjorklund/Glynn sieve --------------------------------------------------------------- */
+
+/* The sieve of _calc_hafnian(Ax, edge_reps; glynn) (src/hafnian.jl:684-738) for one matrix:
+ * Ax is the 2E x 2E matrix already permuted so row i pairs with row i+E (_permuted, :786-792),
+ * edge_reps the E multiplicities from matched_reps (:142-188).  glynn selects the Glynn
+ * (1) or inclusion-exclusion (0) variant.  FP64 per term, double-double accumulation of the
+ * signed terms; out receives one value (EGG_F64 or EGG_C128).
+ * Replaces _calc_hafnian (src/hafnian.jl:684); the reference has no device sieve. */
+int egg_sieve(int dtype, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, void *out);
+
+/* Same, Ax and out in device memory (edge_reps on the host), enqueued on `stream`. */
+int egg_sieve_device(int dtype, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, void *out,
+                     void *stream);
+
+/* B independent sieves in one call (the batched form the reference lacks: hafnian_repeated
+ * runs its batch as a CPU loop, src/hafnian.jl:1355-1358).  Instance b has E[b] <= Emax edges;
+ * its permuted matrix is the leading 2E[b] x 2E[b] block of the 2Emax x 2Emax column-major
+ * slab at Ax + b*(2Emax)^2 elements; its multiplicities are edge_reps[b*Emax .. b*Emax+E[b]-1];
+ * glynn[b] picks its variant.  out receives B values. */
+int egg_sieve_batch(int dtype, int64_t B, int64_t Emax, const void *Ax, const int64_t *E,
+                    const int64_t *edge_reps, const int32_t *glynn, void *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EGGMAN_B200_H */

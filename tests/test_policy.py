@@ -1,0 +1,178 @@
+"""Host-side logic of the mirror (no GPU): strategy choice, matched_reps, validation and error
+behaviour, checked against the reference's own regression expectations (test/runtests.jl:334-412,
+:425-438, :520-587; test/gpu.jl:110-119, :149-154) and against the oracle's independent
+restatement of the same policy."""
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def pol(egg):
+    from theeggman_b200 import policy
+
+    return policy
+
+
+def test_method_selection(pol):
+    # test/runtests.jl:334-344
+    assert pol._choose_method(8, [1] * 4, 12)[0] == "unrolled"
+    assert pol._choose_method(12, [1] * 6, 12)[0] == "unrolled"
+    assert pol._choose_method(20, [1] * 10, 12)[0] == "dp"
+    assert pol._choose_method(28, [1] * 14, 12)[0] == "dp"
+    assert pol._choose_method(32, [1] * 16, 12)[0] == "dp"
+    assert pol._choose_method(34, [1] * 17, 12)[0] == "sieve"
+    assert pol._choose_method(28, pol.matched_reps([2] * 14)[1], 12)[0] == "sieve"
+    assert pol._choose_method(16, pol.matched_reps([2] * 8)[1], 12)[0] == "dp"
+    assert pol._choose_method(16, pol.matched_reps([2] * 8)[1], 12)[1] is True  # :117
+
+
+def test_choice_thread_independent(pol):
+    # test/runtests.jl:354-372
+    for N in range(14, pol.DP_MAX + 1, 2):
+        picks = [pol._choose_method_distinct(N, N // 2, nt)[0] for nt in (1, 2, 4, 8, 12, 32, 128, 1024)]
+        assert all(p == picks[0] for p in picks) and picks[0] == "dp"
+    for rpt in ([2] * 10, [2] * 14, [3] * 6, [4] * 6, [7, 7, 7, 7]):
+        er = pol.matched_reps(rpt)[1]
+        picks = [pol._choose_method(sum(rpt), er, nt)[0] for nt in (1, 12, 32, 128)]
+        assert all(p == picks[0] for p in picks) and picks[0] == "sieve"
+
+
+def test_backend_steering(pol):
+    # test/runtests.jl:374-393 (the warning has no counterpart: the sieve runs on the device here)
+    for nt in (1, 12, 32):
+        for N in (16, 20, 28, pol.DP_MAX):
+            assert pol._steer_backend(pol._choose_method_distinct(N, N // 2, nt)[0], "b", N, "auto") == "dp"
+        for N in range(2, pol.UNROLL_MAX + 1, 2):
+            assert pol._steer_backend(pol._choose_method_distinct(N, N // 2, nt)[0], "b", N, "auto") == "unrolled"
+    assert pol._steer_backend("sieve", "b", 36, "auto") == "sieve"
+    assert pol._steer_backend("sieve", None, 36, "auto") == "sieve"
+    assert pol._steer_backend("unrolled", None, 8, "auto") == "unrolled"
+
+
+def test_unrolled_crossover(pol):
+    # test/runtests.jl:395-412
+    def bestwork(er):
+        return min(pol._sieve_variant_cost(er, sum(er), True)[0], pol._sieve_variant_cost(er, sum(er), False)[0])
+
+    assert not pol._prefer_unrolled(12, bestwork(pol.matched_reps([6, 6])[1]))
+    assert pol._prefer_unrolled(12, bestwork(pol.matched_reps([5, 5, 1, 1])[1]))
+    for N in range(2, pol.UNROLL_MAX + 1, 2):
+        assert pol._prefer_unrolled(N, bestwork([1] * (N // 2)))
+    assert not pol._prefer_unrolled(pol.UNROLL_MAX + 2, 2**63 - 1)
+
+
+def test_unrolled_muls_readme(pol):
+    # README.md: "232 subsets, 1055 multiplies at N = 12"
+    assert pol._unrolled_muls(12) == 1055
+
+
+def test_dp_counts_and_limits(pol, orc):
+    for K in range(0, 65, 2):
+        assert pol._dp_counts(K) == orc.dp_counts(K)
+    assert pol._dp_index_bytes(pol.DP_MAX) == 4 and pol._dp_index_bytes(pol.DP_MAX + 2) == 8
+    for (nt, n, th) in ((10, 5, 12), (10**6, 3, 12), (10**6, 10**5, 12), (0, 1, 8)):
+        c = pol._dp_level_chunks(nt, n, th)
+        assert 1 <= c <= min(th, n)
+
+
+def test_policy_matches_oracle(pol, orc, W):
+    u = W.uniform(991, 4000)
+    k = 0
+    for trial in range(200):
+        d = 2 + int(u[k] * 10); k += 1
+        rpt = [int(u[k + i] * 5) for i in range(d)]
+        k += d
+        if sum(rpt) % 2:
+            rpt[0] += 1
+        x1, e1 = pol.matched_reps(rpt)
+        x2, e2 = orc.matched_reps(rpt)
+        assert (x1, e1) == (x2, e2), rpt
+        if e1:
+            for nt in (1, 12):
+                assert pol._choose_method(sum(rpt), e1, nt) == orc.choose_method(sum(rpt), e1, nt)
+                for g in (True, False):
+                    assert pol._sieve_variant_cost(e1, sum(e1), g) == orc.sieve_variant_cost(e1, sum(e1), g)
+    for N in range(2, 66, 2):
+        for nt in (1, 12, 32):
+            assert pol._choose_method_distinct(N, N // 2, nt) == orc.choose_method_distinct(N, N // 2, nt)
+
+
+def test_check_method(pol, egg):
+    with pytest.raises(egg.ArgumentError):
+        pol._check_method("nonsense", 8)
+    with pytest.raises(egg.ArgumentError):
+        pol._check_method("unrolled", 14)
+    pol._check_method("dp", pol.DP_HARD_MAX)
+    with pytest.raises(egg.ArgumentError):
+        pol._check_method("dp", pol.DP_HARD_MAX + 2)
+
+
+def test_symmetry_tolerance(egg, W):
+    # test/runtests.jl:520-542
+    from theeggman_b200.hafnian import _check_symmetric
+
+    for cplx in (False, True):
+        A = W.dense_complex(6, 22, 0.5) if cplx else W.dense_real(6, 22)
+        inside = A.copy()
+        inside[1, 4] = A[4, 1] * (1 + np.sqrt(np.finfo(float).eps) / 8)
+        _check_symmetric(inside)
+        outside = A.copy()
+        outside[1, 4] = A[4, 1] * (1 + 8 * np.sqrt(np.finfo(float).eps))
+        with pytest.raises(egg.ArgumentError):
+            _check_symmetric(outside)
+    B = np.ones((4, 4))
+    B[0, 1] = B[1, 0] = np.inf
+    _check_symmetric(B)
+    B[0, 1] = B[1, 0] = np.nan
+    with pytest.raises(egg.ArgumentError):
+        _check_symmetric(B)
+
+
+def test_input_validation(egg, W):
+    # test/runtests.jl:580-587, :346-351; test/gpu.jl:110-119 -- all raised before any device call
+    A = W.dense_complex(4, 11, 0.5)
+    with pytest.raises(egg.DimensionMismatch):
+        egg.hafnian(np.random.default_rng(0).standard_normal((3, 4)))
+    with pytest.raises(egg.ArgumentError):
+        egg.hafnian(np.array([[1.0, 2.0], [3.0, 4.0]]))
+    with pytest.raises(egg.DimensionMismatch):
+        egg.hafnian_repeated(A, [1, 1, 1])
+    with pytest.raises(egg.ArgumentError):
+        egg.hafnian_repeated(A, [-1, 1, 1, 1])
+    B16 = W.dense_complex(16, 16, 0.5)
+    with pytest.raises(egg.ArgumentError):
+        egg.hafnian(B16, method="unrolled")
+    with pytest.raises(egg.ArgumentError):
+        egg.hafnian(B16, method="nonsense")
+    with pytest.raises(egg.ArgumentError):
+        egg.hafnian(W.dense_complex(66, 17, 0.5), method="dp")
+    A10 = W.dense_complex(10, 108, 0.5)
+    with pytest.raises(egg.ArgumentError):
+        egg.hafnian_repeated(A10, [[1] * 10, [1] * 9 + [0]])
+    with pytest.raises(egg.ArgumentError):
+        egg.hafnian_repeated(A10, [[1] * 10, [-1] + [1] * 9])
+    with pytest.raises(egg.DimensionMismatch):
+        egg.hafnian_repeated(A10, [[1] * 10, [1] * 9])
+    with pytest.raises(egg.DimensionMismatch):
+        egg.hafnian([A10, W.dense_complex(12, 1, 0.5)])
+    bad = W.dense_complex(8, 23, 0.5)
+    bad[0, 1] += 1
+    with pytest.raises(egg.ArgumentError):
+        egg.hafnian(bad)
+
+
+def test_degenerate_sizes_need_no_device(egg, W):
+    # N = 0 -> 1, odd -> 0, total 0 -> 1, odd total -> 0: no kernel is reached (src/hafnian.jl:1121-1122)
+    assert egg.hafnian(np.zeros((0, 0))) == 1
+    for N in (1, 3, 5, 7):
+        assert egg.hafnian(W.dense_real(N, 2)) == 0
+    A = W.dense_complex(4, 10, 0.5)
+    assert egg.hafnian_repeated(A, [0, 0, 0, 0]) == 1
+    assert egg.hafnian_repeated(A, [1, 0, 0, 0]) == 0
+
+
+def test_dp_batch_bytes(egg, pol):
+    # test/gpu.jl:149-154
+    ns, _ = pol._dp_counts(20)
+    assert egg.dp_batch_bytes(20, np.complex128, 1) == (ns + 190) * 16
+    assert egg.dp_batch_bytes(20, np.complex64, 8) == 8 * (ns + 190) * 8

@@ -1,0 +1,171 @@
+// egg_internal.cuh -- shared definitions for libeggman_b200 (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/eggman_b200.h"
+
+namespace egg {
+
+// ---- error plumbing ----------------------------------------------------------------------------
+
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+
+#define EGG_CUDA_TRY(expr)                                                                          \
+    do {                                                                                            \
+        cudaError_t e_ = (expr);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return ::egg::fail(EGG_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---- complex / double-double value types -------------------------------------------------------
+
+struct __align__(16) cd { double re, im; };
+struct __align__(8) cf { float re, im; };
+
+// Exact-order arithmetic: every product and sum rounds separately (no FMA contraction), which is
+// how Julia evaluates Float64 and Complex{Float64} on the CPU.  Julia's complex product is
+// (ar*br - ai*bi, ar*bi + ai*br).
+__device__ __forceinline__ double x_madd(double acc, double p, double h) { return __dadd_rn(acc, __dmul_rn(p, h)); }
+__device__ __forceinline__ float x_madd(float acc, float p, float h) { return __fadd_rn(acc, __fmul_rn(p, h)); }
+__device__ __forceinline__ cd x_cmul(cd a, cd b)
+{
+    cd r;
+    r.re = __dsub_rn(__dmul_rn(a.re, b.re), __dmul_rn(a.im, b.im));
+    r.im = __dadd_rn(__dmul_rn(a.re, b.im), __dmul_rn(a.im, b.re));
+    return r;
+}
+__device__ __forceinline__ cf x_cmul(cf a, cf b)
+{
+    cf r;
+    r.re = __fsub_rn(__fmul_rn(a.re, b.re), __fmul_rn(a.im, b.im));
+    r.im = __fadd_rn(__fmul_rn(a.re, b.im), __fmul_rn(a.im, b.re));
+    return r;
+}
+__device__ __forceinline__ cd x_madd(cd acc, cd p, cd h)
+{
+    cd t = x_cmul(p, h);
+    acc.re = __dadd_rn(acc.re, t.re);
+    acc.im = __dadd_rn(acc.im, t.im);
+    return acc;
+}
+__device__ __forceinline__ cf x_madd(cf acc, cf p, cf h)
+{
+    cf t = x_cmul(p, h);
+    acc.re = __fadd_rn(acc.re, t.re);
+    acc.im = __fadd_rn(acc.im, t.im);
+    return acc;
+}
+
+// Fused forms (one rounding per multiply-add).
+__device__ __forceinline__ double f_madd(double acc, double p, double h) { return fma(p, h, acc); }
+__device__ __forceinline__ float f_madd(float acc, float p, float h) { return fmaf(p, h, acc); }
+__device__ __forceinline__ cd f_madd(cd acc, cd p, cd h)
+{
+    acc.re = fma(p.re, h.re, fma(-p.im, h.im, acc.re));
+    acc.im = fma(p.re, h.im, fma(p.im, h.re, acc.im));
+    return acc;
+}
+__device__ __forceinline__ cf f_madd(cf acc, cf p, cf h)
+{
+    acc.re = fmaf(p.re, h.re, fmaf(-p.im, h.im, acc.re));
+    acc.im = fmaf(p.re, h.im, fmaf(p.im, h.re, acc.im));
+    return acc;
+}
+
+// Double-double accumulation (Knuth's TwoSum, then a fast renormalisation).
+struct dd { double hi, lo; };
+__device__ __forceinline__ void dd_add(dd &a, double x)
+{
+    double s = __dadd_rn(a.hi, x);
+    double bp = __dsub_rn(s, a.hi);
+    double e = __dadd_rn(__dsub_rn(a.hi, __dsub_rn(s, bp)), __dsub_rn(x, bp));
+    double t = __dadd_rn(a.lo, e);
+    double h = __dadd_rn(s, t);
+    a.lo = __dsub_rn(t, __dsub_rn(h, s));
+    a.hi = h;
+}
+__device__ __forceinline__ void dd_add(dd &a, dd b)
+{
+    dd_add(a, b.hi);
+    dd_add(a, b.lo);
+}
+
+// ---- device plans ------------------------------------------------------------------------------
+
+// One subset-size level of a plan: states lo..lo+n-1 (0-based), each with `deg` transitions,
+// the first at offset toff (0-based) of trans.  Every state of a level has the same out-degree
+// (|S| - 1, src/dp.jl:384-385), so `starts` is implied and never read on the device.
+struct Level {
+    int64_t lo, n, toff;
+    int deg;
+};
+
+struct DevPlan {
+    int K = 0, idx_bytes = 0;
+    int64_t nstates = 0, ntrans = 0;
+    void *trans = nullptr;        // device, ntrans entries of idx_bytes
+    std::vector<Level> levels;    // levels[0] is the empty set
+    std::vector<int64_t> level_starts;  // the reference's 1-based `levels` vector
+    int64_t bytes() const { return ntrans * (int64_t)idx_bytes; }
+};
+
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct Context {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    std::map<std::pair<int, int>, DevPlan> plans;
+    DevBuf scratch[6];   // H, P, out, misc...: grown on demand, never shrunk
+    std::recursive_mutex mu;
+};
+
+Context &ctx();
+int ensure_init();
+int ensure_buf(DevBuf &b, size_t bytes);
+DevPlan *find_plan(int K, int idx_bytes);
+
+// Closed-form plan size (_dp_counts, src/dp.jl:192-208).
+void dp_counts(int K, int64_t &nstates, int64_t &ntrans);
+inline int pair_bits(int idx_bytes) { return idx_bytes == 4 ? 9 : 12; }
+
+// ---- entry points implemented per file ----------------------------------------------------------
+
+// egg_plan.cu
+int plan_build_device(int K, int idx_bytes, DevPlan &out);
+int plan_validate_device(const DevPlan &p, cudaStream_t st);
+
+// egg_dp.cu
+int dp_run(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t B, void *dout, cudaStream_t st);
+size_t dp_scratch_bytes(const DevPlan &plan, int dtype, int prec, int64_t B);
+
+// egg_sieve.cu
+int sieve_run(int dtype, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, void *dout,
+              cudaStream_t st);
+int sieve_batch_run(int dtype, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
+                    const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st);
+
+inline size_t dtype_size(int dtype)
+{
+    switch (dtype) {
+    case EGG_F64: return 8;
+    case EGG_C128: return 16;
+    case EGG_F32: return 4;
+    case EGG_C64: return 8;
+    case EGG_I64: return 8;
+    }
+    return 0;
+}
+
+}  // namespace egg

@@ -1,0 +1,206 @@
+// egg_plan.cu -- subset-DP plans in device memory.
+//
+// The reference builds a plan on the host (src/dp.jl:223-304): a DFS from the full mask, a sort of
+// every reachable mask by (popcount, mask), a Dict from mask to state number, and a CSR walk.
+// At K = 40 that is 2.84e9 transitions (22.7 GB as Int64) and needs about twice that in host RAM.
+//
+// Here the same layout is produced directly in HBM.  The reachable subsets have a closed form:
+// S is reachable iff, with r = K - |S| removed, its minimum bit (0-based) is >= ceil(r/2)
+// (src/dp.jl:16-27: p - 1 <= r <= 2(p - 1)).  So the level of popcount c is exactly the set of all
+// c-subsets of the top U = K - ceil((K-c)/2) bit positions, and sorting by mask value within a level
+// is colex order.  A state's number is therefore its level's offset plus its colex rank
+// sum_i C(e_i, i) (combinatorial number system, e_i the shifted elements in increasing order), and
+// each thread can unrank its own state and rank each of its children without any table.
+#include "egg_internal.cuh"
+
+namespace egg {
+
+static __device__ __forceinline__ int64_t pair_index(int64_t i, int64_t j, int64_t K)
+{
+    // _pair_index(i, j, K), src/unrolled.jl:60 (1-based, i < j).
+    return (i - 1) * K - (i * (i + 1)) / 2 + j;
+}
+
+// Binomial table C(n, k) for n, k <= 64 (C(64, 32) < 2^63), staged per block in shared memory.
+__constant__ int64_t c_binom_dummy;  // keeps the constant bank initialised on every build
+
+template <class I>
+__global__ void __launch_bounds__(256) plan_level_kernel(I *__restrict__ trans, const int64_t *__restrict__ binom_g,
+                                                         int K, int c, int m0, int64_t n, int64_t toff,
+                                                         int64_t child_lo1, int bits)
+{
+    __shared__ int64_t binom[65 * 65];
+    for (int i = threadIdx.x; i < 65 * 65; i += blockDim.x) binom[i] = binom_g[i];
+    __syncthreads();
+    const int U = K - m0;  // level elements are the shifted positions 0..U-1
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
+        // Unrank s (colex) into c shifted elements e[1] < ... < e[c].
+        int e[65];
+        int64_t R = s;
+        int x = U - 1;
+        for (int i = c; i >= 1; --i) {
+            while (binom[x * 65 + i] > R) --x;
+            e[i] = x;
+            R -= binom[x * 65 + i];
+            --x;
+        }
+        // Child of removing e[1] (the minimum) and e[j]: its elements shift down by one more
+        // position (the child level's offset is m0 + 1).  rank = pre[j] + suf[j] with
+        // pre[j] = sum_{x=2}^{j-1} C(e_x - 1, x - 1), suf[j] = sum_{x=j+1}^{c} C(e_x - 1, x - 2).
+        int64_t suf[66];
+        suf[c + 1] = 0;
+        suf[c] = 0;
+        for (int x2 = c; x2 >= 3; --x2) suf[x2 - 1] = suf[x2] + binom[(e[x2] - 1) * 65 + (x2 - 2)];
+        int64_t pre = 0;
+        const int64_t ib = (int64_t)e[1] + m0 + 1;  // 1-based index of the minimum
+        I *out = trans + toff + s * (int64_t)(c - 1);
+        for (int j = 2; j <= c; ++j) {
+            int64_t child = child_lo1 + pre + suf[j];
+            int64_t jb = (int64_t)e[j] + m0 + 1;
+            out[j - 2] = (I)((child << bits) | pair_index(ib, jb, K));
+            pre += binom[(e[j] - 1) * 65 + (j - 1)];
+        }
+    }
+}
+
+static void host_binom(std::vector<int64_t> &t)
+{
+    t.assign(65 * 65, 0);
+    for (int nn = 0; nn <= 64; ++nn) {
+        t[nn * 65 + 0] = 1;
+        for (int k = 1; k <= nn; ++k) {
+            __int128 v = (__int128)t[(nn - 1) * 65 + (k - 1)] + (k <= nn - 1 ? t[(nn - 1) * 65 + k] : 0);
+            t[nn * 65 + k] = v > INT64_MAX ? INT64_MAX : (int64_t)v;
+        }
+    }
+}
+
+int plan_build_device(int K, int idx_bytes, DevPlan &p)
+{
+    Context &cx = ctx();
+    int64_t ns, nt;
+    dp_counts(K, ns, nt);
+    p.K = K;
+    p.idx_bytes = idx_bytes;
+    p.nstates = ns;
+    p.ntrans = nt;
+    std::vector<int64_t> binom;
+    host_binom(binom);
+    // Levels: popcount c = 0, 2, ..., K.
+    int64_t lo = 0, toff = 0;
+    p.levels.clear();
+    p.level_starts.clear();
+    for (int c = 0; c <= K; c += 2) {
+        int m0 = (K - c + 1) / 2;
+        int U = K - m0;
+        Level lv;
+        lv.lo = lo;
+        lv.n = binom[U * 65 + c];
+        lv.toff = toff;
+        lv.deg = c == 0 ? 0 : c - 1;
+        p.levels.push_back(lv);
+        p.level_starts.push_back(lo + 1);
+        lo += lv.n;
+        toff += lv.n * lv.deg;
+    }
+    p.level_starts.push_back(lo + 1);
+    if (lo != ns || toff != nt) return fail(EGG_ERR_PLAN_INVALID, "closed-form level sizes disagree with _dp_counts");
+    size_t bytes = (size_t)nt * idx_bytes;
+    size_t free_b = 0, total_b = 0;
+    EGG_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    if (bytes + ((size_t)1 << 28) > free_b)
+        return fail(EGG_ERR_TOO_LARGE, "a degree-" + std::to_string(K) + " plan needs " + std::to_string(bytes) +
+                                           " device bytes; " + std::to_string(free_b) + " are free");
+    cudaError_t e = cudaMalloc(&p.trans, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(EGG_ERR_TOO_LARGE, std::string("plan allocation failed: ") + cudaGetErrorString(e));
+    }
+    int64_t *dbinom = nullptr;
+    e = cudaMalloc(&dbinom, binom.size() * sizeof(int64_t));
+    if (e != cudaSuccess) {
+        cudaFree(p.trans);
+        p.trans = nullptr;
+        return fail(EGG_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    int rc = EGG_OK;
+    e = cudaMemcpyAsync(dbinom, binom.data(), binom.size() * sizeof(int64_t), cudaMemcpyHostToDevice, cx.stream);
+    int bits = pair_bits(idx_bytes);
+    for (size_t L = 1; e == cudaSuccess && L < p.levels.size(); ++L) {
+        const Level &lv = p.levels[L];
+        int c = 2 * (int)L;
+        int m0 = (K - c + 1) / 2;
+        int64_t blocks = (lv.n + 255) / 256;
+        int64_t cap = (int64_t)cx.num_sms * 16;
+        if (blocks > cap) blocks = cap;
+        int64_t child_lo1 = p.levels[L - 1].lo + 1;
+        if (idx_bytes == 4)
+            plan_level_kernel<int32_t><<<(unsigned)blocks, 256, 0, cx.stream>>>((int32_t *)p.trans, dbinom, K, c, m0, lv.n,
+                                                                              lv.toff, child_lo1, bits);
+        else
+            plan_level_kernel<int64_t><<<(unsigned)blocks, 256, 0, cx.stream>>>((int64_t *)p.trans, dbinom, K, c, m0, lv.n,
+                                                                              lv.toff, child_lo1, bits);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cx.stream);
+    cudaFree(dbinom);
+    if (e != cudaSuccess) {
+        cudaFree(p.trans);
+        p.trans = nullptr;
+        rc = fail(EGG_ERR_CUDA, std::string("plan build: ") + cudaGetErrorString(e));
+    }
+    return rc;
+}
+
+// Structure check for a plan that came from the host: every transition of level L must name a
+// child in level L-1 and a pair index in 1..K(K-1)/2.  This is what makes the level kernels'
+// unchecked loads safe, so a plan that fails is refused before any evaluation runs.
+template <class I>
+__global__ void plan_check_kernel(const I *__restrict__ trans, int64_t toff, int64_t cnt, int64_t child_lo1,
+                                  int64_t child_hi1, int64_t npairs, int bits, unsigned long long *bad)
+{
+    const I mask = ((I)1 << bits) - 1;
+    unsigned long long local = 0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < cnt; k += (int64_t)gridDim.x * blockDim.x) {
+        I t = trans[toff + k];
+        int64_t pi = (int64_t)(t & mask), ci = (int64_t)(t >> bits);
+        if (t < 0 || pi < 1 || pi > npairs || ci < child_lo1 || ci > child_hi1) ++local;
+    }
+    if (local) atomicAdd(bad, local);
+}
+
+int plan_validate_device(const DevPlan &p, cudaStream_t st)
+{
+    Context &cx = ctx();
+    unsigned long long *dbad = nullptr;
+    EGG_CUDA_TRY(cudaMalloc(&dbad, sizeof(unsigned long long)));
+    cudaError_t e = cudaMemsetAsync(dbad, 0, sizeof(unsigned long long), st);
+    int bits = pair_bits(p.idx_bytes);
+    int64_t npairs = (int64_t)p.K * (p.K - 1) / 2;
+    for (size_t L = 1; e == cudaSuccess && L < p.levels.size(); ++L) {
+        const Level &lv = p.levels[L];
+        int64_t cnt = lv.n * lv.deg;
+        int64_t blocks = (cnt + 255) / 256;
+        int64_t cap = (int64_t)cx.num_sms * 16;
+        if (blocks > cap) blocks = cap;
+        if (blocks < 1) continue;
+        int64_t clo = p.levels[L - 1].lo + 1, chi = p.levels[L - 1].lo + p.levels[L - 1].n;
+        if (p.idx_bytes == 4)
+            plan_check_kernel<int32_t><<<(unsigned)blocks, 256, 0, st>>>((const int32_t *)p.trans, lv.toff, cnt, clo, chi,
+                                                                       npairs, bits, dbad);
+        else
+            plan_check_kernel<int64_t><<<(unsigned)blocks, 256, 0, st>>>((const int64_t *)p.trans, lv.toff, cnt, clo, chi,
+                                                                       npairs, bits, dbad);
+        e = cudaGetLastError();
+    }
+    unsigned long long bad = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, dbad, sizeof(bad), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(dbad);
+    if (e != cudaSuccess) return fail(EGG_ERR_CUDA, std::string("plan check: ") + cudaGetErrorString(e));
+    if (bad) return fail(EGG_ERR_PLAN_INVALID, std::to_string(bad) + " transitions name a child outside the previous level "
+                                                                     "or a pair index out of range");
+    return EGG_OK;
+}
+
+}  // namespace egg

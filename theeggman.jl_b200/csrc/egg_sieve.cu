@@ -1,0 +1,599 @@
+// egg_sieve.cu -- the Bjorklund/Glynn sieve (src/hafnian.jl:528-738) on the device.
+//
+// The reference has no device sieve (README.md:144-148: "roughly a 40 KB workspace per term").
+// Here one warp evaluates one term at a time with its workspace in shared memory; lanes split the
+// independent element updates of each step, and every element is updated in exactly the order and
+// rounding of the reference loop (__dmul_rn/__dadd_rn, no contraction), so each term's value is
+// bit-identical to the CPU's _glynn_term!.  Where the reference sums terms with a plain `+=`
+// (:618-622), each warp keeps a double-double accumulator; the per-warp partials are then summed
+// in a fixed tree, so results do not depend on scheduling.
+//
+// Work layout.  Instance b's terms j = 0..steps-1 are dealt round-robin to that instance's warps
+// (grid.y = instance).  The mixed-radix odometer (edge E least significant, the leading digit
+// clipped to its lower half under Glynn, :655-657) is decoded per term.
+#include "egg_internal.cuh"
+
+namespace egg {
+
+struct SieveInst {
+    int64_t ax_off;     // element offset of this instance's matrix (ld = lda)
+    int64_t steps;      // number of sieve terms
+    int64_t reps_off;   // offset into the reps array
+    int E, n, glynn, lda;
+};
+
+struct SieveArgs {
+    const void *Ax;
+    const int *reps;
+    const double *binoms;  // (maxrep+1) x (maxrep+1), binoms[a + b*(maxrep+1)] = C(a, b)
+    const SieveInst *inst;
+    dd *partial;           // [B][warps_per_inst][2]
+    int maxrep, warps_per_inst, Emax, nmax;
+};
+
+// Per-warp shared workspace, carved from dynamic shared memory.
+struct WarpWs {
+    double *M;   // real: M; complex: Mr
+    double *Mi;  // complex: Mi
+    double *u;   // multipliers (real) / ur
+    double *ui;  // ui
+    double *C;   // (m+1) x (n+1) rows of charpoly coefficients (complex: interleaved)
+    double *f;   // n+1 series coefficients (complex: interleaved)
+    int *kept, *idx, *rows;
+    int ldm;
+};
+
+__host__ __device__ inline size_t ws_doubles(int Emax, int nmax, int cplx)
+{
+    size_t MM = 2 * (size_t)Emax, ld = MM + 1;
+    size_t d = (cplx ? 2 : 1) * ld * MM + 2 * MM + (cplx ? 2 : 1) * (MM + 1) * (nmax + 1) + 2 * (nmax + 1);
+    size_t ints = 2 * (size_t)Emax + MM;
+    return d + (ints + 1) / 2 + 2;
+}
+
+__device__ inline WarpWs carve(double *base, int Emax, int nmax, int cplx)
+{
+    WarpWs w;
+    int MM = 2 * Emax, ld = MM + 1;
+    w.ldm = ld;
+    double *p = base;
+    w.M = p; p += (size_t)ld * MM;
+    w.Mi = cplx ? p : nullptr; if (cplx) p += (size_t)ld * MM;
+    w.u = p; p += MM;
+    w.ui = p; p += MM;
+    w.C = p; p += (size_t)(cplx ? 2 : 1) * (MM + 1) * (nmax + 1);
+    w.f = p; p += 2 * (nmax + 1);
+    int *ip = (int *)p;
+    w.kept = ip; ip += Emax;
+    w.idx = ip; ip += Emax;
+    w.rows = ip;
+    return w;
+}
+
+// Warp argmax with the reference's tie rule (the first index achieving the maximum, :212-221):
+// returns the winning row.  a is this lane's candidate value (NaN entries must never win).
+__device__ __forceinline__ int warp_first_argmax(double a, int i)
+{
+    for (int off = 16; off > 0; off >>= 1) {
+        double a2 = __shfl_down_sync(0xffffffffu, a, off);
+        int i2 = __shfl_down_sync(0xffffffffu, i, off);
+        if (a2 > a || (a2 == a && i2 < i)) {
+            a = a2;
+            i = i2;
+        }
+    }
+    return __shfl_sync(0xffffffffu, i, 0);
+}
+
+// _hessenberg!(M, m, mult), src/hafnian.jl:210-258, one warp, exact order.
+__device__ void hessenberg_real_exact(WarpWs &w, int m, int lane)
+{
+    double *M = w.M;
+    const int ld = w.ldm;
+#define MX(i, j) M[(size_t)(j) * ld + (i)]
+    for (int k = 1; k <= m - 2; ++k) {  // 0-based pivot row k, pivot column k-1
+        const int col = k - 1;
+        double a0 = fabs(MX(k, col));
+        int p = k;
+        if (a0 == a0) {
+            double best = -1.0;
+            int bi = 0x7fffffff;
+            for (int i = k + lane; i < m; i += 32) {
+                double a = fabs(MX(i, col));
+                if (a != a) a = -1.0;
+                if (a > best) {
+                    best = a;
+                    bi = i;
+                }
+            }
+            p = warp_first_argmax(best, bi);
+        }
+        if (p != k) {
+            for (int j = col + lane; j < m; j += 32) {
+                double t = MX(p, j);
+                MX(p, j) = MX(k, j);
+                MX(k, j) = t;
+            }
+            __syncwarp();
+            for (int i = lane; i < m; i += 32) {
+                double t = MX(i, p);
+                MX(i, p) = MX(i, k);
+                MX(i, k) = t;
+            }
+            __syncwarp();
+        }
+        const double x = MX(k, col);
+        if (x == 0.0) continue;
+        for (int i = k + 1 + lane; i < m; i += 32) {
+            w.u[i] = __ddiv_rn(MX(i, col), x);
+            MX(i, col) = 0.0;
+        }
+        __syncwarp();
+        for (int j = k; j < m; ++j) {
+            const double akj = MX(k, j);
+            if (akj == 0.0) continue;
+            for (int i = k + 1 + lane; i < m; i += 32) MX(i, j) = __dsub_rn(MX(i, j), __dmul_rn(w.u[i], akj));
+        }
+        __syncwarp();
+        for (int i = k + 1; i < m; ++i) {
+            const double mi = w.u[i];
+            if (mi == 0.0) continue;
+            for (int l = lane; l < m; l += 32) MX(l, k) = __dadd_rn(MX(l, k), __dmul_rn(mi, MX(l, i)));
+        }
+        __syncwarp();
+    }
+#undef MX
+}
+
+// _hessenberg_split!(Mr, Mi, m, ur, ui), src/hafnian.jl:271-335, one warp, exact order.
+__device__ void hessenberg_split_exact(WarpWs &w, int m, int lane)
+{
+    double *R = w.M, *I = w.Mi;
+    const int ld = w.ldm;
+#define RX(i, j) R[(size_t)(j) * ld + (i)]
+#define IX(i, j) I[(size_t)(j) * ld + (i)]
+    for (int k = 1; k <= m - 2; ++k) {
+        const int col = k - 1;
+        double a0 = __dadd_rn(__dmul_rn(RX(k, col), RX(k, col)), __dmul_rn(IX(k, col), IX(k, col)));
+        int p = k;
+        if (a0 == a0) {
+            double best = -1.0;
+            int bi = 0x7fffffff;
+            for (int i = k + lane; i < m; i += 32) {
+                double a = __dadd_rn(__dmul_rn(RX(i, col), RX(i, col)), __dmul_rn(IX(i, col), IX(i, col)));
+                if (a != a) a = -1.0;
+                if (a > best) {
+                    best = a;
+                    bi = i;
+                }
+            }
+            p = warp_first_argmax(best, bi);
+        }
+        if (p != k) {
+            for (int j = col + lane; j < m; j += 32) {
+                double t = RX(p, j); RX(p, j) = RX(k, j); RX(k, j) = t;
+                t = IX(p, j); IX(p, j) = IX(k, j); IX(k, j) = t;
+            }
+            __syncwarp();
+            for (int i = lane; i < m; i += 32) {
+                double t = RX(i, p); RX(i, p) = RX(i, k); RX(i, k) = t;
+                t = IX(i, p); IX(i, p) = IX(i, k); IX(i, k) = t;
+            }
+            __syncwarp();
+        }
+        const double xr = RX(k, col), xi = IX(k, col);
+        const double d = __dadd_rn(__dmul_rn(xr, xr), __dmul_rn(xi, xi));
+        if (d == 0.0) continue;
+        for (int i = k + 1 + lane; i < m; i += 32) {
+            const double ar = RX(i, col), ai = IX(i, col);
+            w.u[i] = __ddiv_rn(__dadd_rn(__dmul_rn(ar, xr), __dmul_rn(ai, xi)), d);
+            w.ui[i] = __ddiv_rn(__dsub_rn(__dmul_rn(ai, xr), __dmul_rn(ar, xi)), d);
+            RX(i, col) = 0.0;
+            IX(i, col) = 0.0;
+        }
+        __syncwarp();
+        for (int j = k; j < m; ++j) {
+            const double ar = RX(k, j), ai = IX(k, j);
+            for (int i = k + 1 + lane; i < m; i += 32) {
+                const double ur = w.u[i], ui = w.ui[i];
+                RX(i, j) = __dsub_rn(RX(i, j), __dsub_rn(__dmul_rn(ur, ar), __dmul_rn(ui, ai)));
+                IX(i, j) = __dsub_rn(IX(i, j), __dadd_rn(__dmul_rn(ur, ai), __dmul_rn(ui, ar)));
+            }
+        }
+        __syncwarp();
+        for (int i = k + 1; i < m; ++i) {
+            const double mr = w.u[i], mi = w.ui[i];
+            for (int l = lane; l < m; l += 32) {
+                const double r = RX(l, i), im = IX(l, i);
+                RX(l, k) = __dadd_rn(RX(l, k), __dsub_rn(__dmul_rn(mr, r), __dmul_rn(mi, im)));
+                IX(l, k) = __dadd_rn(IX(l, k), __dadd_rn(__dmul_rn(mr, im), __dmul_rn(mi, r)));
+            }
+        }
+        __syncwarp();
+    }
+#undef RX
+#undef IX
+}
+
+// _charpoly_hessenberg!(C, H, m, n), src/hafnian.jl:454-492 (real), exact order.  Row k of C
+// (k = 0..m) holds p_k; C[k*(n+1) + t] is the coefficient of lambda^(k-t).
+__device__ void charpoly_real_exact(WarpWs &w, int m, int n, int lane)
+{
+    const double *H = w.M;
+    const int ld = w.ldm, cs = n + 1;
+    double *C = w.C;
+#define HX(i, j) H[(size_t)(j) * ld + (i)]
+    for (int t = lane; t <= n; t += 32) C[t] = t == 0 ? 1.0 : 0.0;
+    __syncwarp();
+    for (int k = 1; k <= m; ++k) {
+        const double hkk = HX(k - 1, k - 1);
+        const int tmax = k < n ? k : n, prevmax = (k - 1) < n ? (k - 1) : n;
+        const double *Cp = C + (size_t)(k - 1) * cs;
+        double *Ck = C + (size_t)k * cs;
+        for (int t = lane; t <= n; t += 32) {
+            if (t == 0) Ck[0] = Cp[0];
+            else if (t <= tmax) Ck[t] = __dsub_rn(t <= prevmax ? Cp[t] : 0.0, __dmul_rn(hkk, Cp[t - 1]));
+            else Ck[t] = 0.0;
+        }
+        double beta = 1.0;
+        const int ilo = 1 > k - n + 1 ? 1 : k - n + 1;
+        for (int i = k - 1; i >= ilo; --i) {
+            beta = __dmul_rn(beta, HX(i, i - 1));
+            if (beta == 0.0) break;
+            const double coef = __dmul_rn(HX(i - 1, k - 1), beta);
+            const int d = k - i + 1;
+            if (coef != 0.0) {
+                const int tt = n < d + i - 1 ? n : d + i - 1;
+                const double *Ci = C + (size_t)(i - 1) * cs;
+                // Lane <-> t stays fixed across i, so each coefficient is updated in the
+                // reference's order (i descending) by one lane.
+                for (int t = lane; t <= tt; t += 32)
+                    if (t >= d) Ck[t] = __dsub_rn(Ck[t], __dmul_rn(coef, Ci[t - d]));
+            }
+        }
+        __syncwarp();
+    }
+#undef HX
+}
+
+__device__ __forceinline__ cd c_mul_x(cd a, cd b) { return x_cmul(a, b); }
+__device__ __forceinline__ cd c_sub_x(cd a, cd b) { return cd{__dsub_rn(a.re, b.re), __dsub_rn(a.im, b.im)}; }
+
+// Complex charpoly on the split storage (the band of Mr/Mi equals the copied-back M, :358-363).
+__device__ void charpoly_cplx_exact(WarpWs &w, int m, int n, int lane)
+{
+    const int ld = w.ldm, cs = n + 1;
+    cd *C = (cd *)w.C;
+    auto H = [&](int i, int j) { return cd{w.M[(size_t)j * ld + i], w.Mi[(size_t)j * ld + i]}; };
+    for (int t = lane; t <= n; t += 32) C[t] = t == 0 ? cd{1.0, 0.0} : cd{0.0, 0.0};
+    __syncwarp();
+    for (int k = 1; k <= m; ++k) {
+        const cd hkk = H(k - 1, k - 1);
+        const int tmax = k < n ? k : n, prevmax = (k - 1) < n ? (k - 1) : n;
+        const cd *Cp = C + (size_t)(k - 1) * cs;
+        cd *Ck = C + (size_t)k * cs;
+        for (int t = lane; t <= n; t += 32) {
+            if (t == 0) Ck[0] = Cp[0];
+            else if (t <= tmax) Ck[t] = c_sub_x(t <= prevmax ? Cp[t] : cd{0.0, 0.0}, c_mul_x(hkk, Cp[t - 1]));
+            else Ck[t] = cd{0.0, 0.0};
+        }
+        cd beta{1.0, 0.0};
+        const int ilo = 1 > k - n + 1 ? 1 : k - n + 1;
+        for (int i = k - 1; i >= ilo; --i) {
+            beta = c_mul_x(beta, H(i, i - 1));
+            if (beta.re == 0.0 && beta.im == 0.0) break;
+            const cd coef = c_mul_x(H(i - 1, k - 1), beta);
+            const int d = k - i + 1;
+            if (!(coef.re == 0.0 && coef.im == 0.0)) {
+                const int tt = n < d + i - 1 ? n : d + i - 1;
+                const cd *Ci = C + (size_t)(i - 1) * cs;
+                for (int t = lane; t <= tt; t += 32)
+                    if (t >= d) Ck[t] = c_sub_x(Ck[t], c_mul_x(coef, Ci[t - d]));
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// _inv_sqrt_det_coeff!(f, q, m, n), src/hafnian.jl:502-514, on lane 0.
+__device__ double inv_sqrt_real_exact(const double *q, double *f, int m, int n)
+{
+    f[0] = 1.0;
+    for (int t = 1; t <= n; ++t) {
+        double s = 0.0;
+        const int jm = t < m ? t : m;
+        for (int j = 1; j <= jm; ++j) s = __dadd_rn(s, __dmul_rn(__dmul_rn((double)(2 * t - j), q[j]), f[t - j]));
+        f[t] = __ddiv_rn(-s, (double)(2 * t));
+    }
+    return f[n];
+}
+
+__device__ cd inv_sqrt_cplx_exact(const cd *q, cd *f, int m, int n)
+{
+    f[0] = cd{1.0, 0.0};
+    for (int t = 1; t <= n; ++t) {
+        cd s{0.0, 0.0};
+        const int jm = t < m ? t : m;
+        for (int j = 1; j <= jm; ++j) {
+            const double wt = (double)(2 * t - j);
+            const cd wq{__dmul_rn(wt, q[j].re), __dmul_rn(wt, q[j].im)};
+            const cd pr = x_cmul(wq, f[t - j]);
+            s.re = __dadd_rn(s.re, pr.re);
+            s.im = __dadd_rn(s.im, pr.im);
+        }
+        const double dd2 = (double)(2 * t);
+        f[t] = cd{__ddiv_rn(-s.re, dd2), __ddiv_rn(-s.im, dd2)};
+    }
+    return f[n];
+}
+
+// One instance's share of terms for this warp, exact order.  Returns the warp's double-double
+// partial sums (re, im) on lane 0.
+template <bool CPLX>
+__device__ void sieve_warp_exact(const SieveArgs &a, const SieveInst &in, WarpWs &w, int wslot, int lane, dd &acc_re,
+                                 dd &acc_im)
+{
+    const int E = in.E, n = in.n, glynn = in.glynn, lda = in.lda;
+    const int *reps = a.reps + in.reps_off;
+    const int mr1 = a.maxrep + 1;
+    for (int64_t j = wslot; j < in.steps; j += a.warps_per_inst) {
+        // Mixed-radix decode, Glynn substitution, surviving edges (:542-580), on lane 0.
+        int mE = 0;
+        double prefac = 0.0;
+        if (lane == 0) {
+            int64_t num = j, edge_sum = 0;
+            double bp = 1.0;
+            for (int i = E - 1; i >= 0; --i) {
+                const int r = reps[i];
+                const int64_t b = r + 1;
+                const int k = (int)(num % b);
+                num /= b;
+                w.kept[i] = k;
+                edge_sum += k;
+                bp = __dmul_rn(bp, a.binoms[r + k * mr1]);
+            }
+            for (int i = 0; i < E; ++i) {
+                const int k = glynn ? 2 * w.kept[i] - reps[i] : w.kept[i];
+                w.kept[i] = k;
+                if (k != 0) w.idx[mE++] = i;
+            }
+            prefac = ((n - edge_sum) % 2 != 0) ? -bp : bp;
+            if (glynn && w.kept[0] == 0) prefac = __ddiv_rn(prefac, 2.0);
+            for (int q = 0; q < mE; ++q) {
+                w.rows[q] = w.idx[q];
+                w.rows[mE + q] = w.idx[q] + E;
+            }
+        }
+        mE = __shfl_sync(0xffffffffu, mE, 0);
+        prefac = __shfl_sync(0xffffffffu, prefac, 0);
+        __syncwarp();
+        const int m = 2 * mE;
+        if (m == 0) continue;  // empty submatrix contributes zero (:566-567)
+        const int ld = w.ldm;
+        // M = A_S X D (:582-593).
+        if (!CPLX) {
+            const double *Ax = (const double *)a.Ax + in.ax_off;
+            for (int b = 0; b < mE; ++b) {
+                const double kb = (double)w.kept[w.idx[b]];
+                const int cb1 = w.idx[b] + E, cb2 = w.idx[b];
+                for (int r = lane; r < m; r += 32) {
+                    const int ra = w.rows[r];
+                    w.M[(size_t)b * ld + r] = __dmul_rn(kb, Ax[(size_t)cb1 * lda + ra]);
+                    w.M[(size_t)(mE + b) * ld + r] = __dmul_rn(kb, Ax[(size_t)cb2 * lda + ra]);
+                }
+            }
+            __syncwarp();
+            hessenberg_real_exact(w, m, lane);
+            charpoly_real_exact(w, m, n, lane);
+            if (lane == 0) {
+                const double val = inv_sqrt_real_exact(w.C + (size_t)m * (n + 1), w.f, m, n);
+                dd_add(acc_re, __dmul_rn(prefac, val));
+            }
+        } else {
+            const cd *Ax = (const cd *)a.Ax + in.ax_off;
+            for (int b = 0; b < mE; ++b) {
+                const double kb = (double)w.kept[w.idx[b]];
+                const int cb1 = w.idx[b] + E, cb2 = w.idx[b];
+                for (int r = lane; r < m; r += 32) {
+                    const int ra = w.rows[r];
+                    const cd z1 = Ax[(size_t)cb1 * lda + ra], z2 = Ax[(size_t)cb2 * lda + ra];
+                    w.M[(size_t)b * ld + r] = __dmul_rn(kb, z1.re);
+                    w.Mi[(size_t)b * ld + r] = __dmul_rn(kb, z1.im);
+                    w.M[(size_t)(mE + b) * ld + r] = __dmul_rn(kb, z2.re);
+                    w.Mi[(size_t)(mE + b) * ld + r] = __dmul_rn(kb, z2.im);
+                }
+            }
+            __syncwarp();
+            hessenberg_split_exact(w, m, lane);
+            charpoly_cplx_exact(w, m, n, lane);
+            if (lane == 0) {
+                const cd val = inv_sqrt_cplx_exact((const cd *)w.C + (size_t)m * (n + 1), (cd *)w.f, m, n);
+                dd_add(acc_re, __dmul_rn(prefac, val.re));
+                dd_add(acc_im, __dmul_rn(prefac, val.im));
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(256) sieve_exact_kernel(SieveArgs a, int warps_per_block)
+{
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int b = blockIdx.y;
+    const SieveInst in = a.inst[b];
+    WarpWs w = carve(smem + (size_t)wib * ws_doubles(a.Emax, a.nmax, CPLX), a.Emax, a.nmax, CPLX);
+    const int wslot = blockIdx.x * warps_per_block + wib;
+    dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
+    if (wslot < a.warps_per_inst) sieve_warp_exact<CPLX>(a, in, w, wslot, lane, acc_re, acc_im);
+    if (lane == 0 && wslot < a.warps_per_inst) {
+        dd *out = a.partial + ((size_t)b * a.warps_per_inst + wslot) * 2;
+        out[0] = acc_re;
+        out[1] = acc_im;
+    }
+}
+
+// Sums each instance's per-warp partials in a fixed tree, applies the Glynn rescaling 2^-(n-1)
+// (:737) and writes the result.  One block of 256 threads per instance.
+template <bool CPLX>
+__global__ void sieve_reduce_kernel(const dd *partial, int warps_per_inst, const SieveInst *inst, void *out)
+{
+    __shared__ dd sre[256], sim[256];
+    const int b = blockIdx.x, t = threadIdx.x;
+    dd r{0.0, 0.0}, i{0.0, 0.0};
+    const dd *p = partial + (size_t)b * warps_per_inst * 2;
+    for (int w = t; w < warps_per_inst; w += 256) {
+        dd_add(r, p[2 * w]);
+        dd_add(i, p[2 * w + 1]);
+    }
+    sre[t] = r;
+    sim[t] = i;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (t < s) {
+            dd_add(sre[t], sre[t + s]);
+            dd_add(sim[t], sim[t + s]);
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        const SieveInst in = inst[b];
+        double hr, hi;
+        if (in.E == 0) {
+            hr = 1.0;  // E == 0: one(T) (:691)
+            hi = 0.0;
+        } else {
+            hr = __dadd_rn(sre[0].hi, sre[0].lo);
+            hi = __dadd_rn(sim[0].hi, sim[0].lo);
+            if (in.glynn) {
+                const double s = ldexp(1.0, -(in.n - 1));
+                hr = __dmul_rn(hr, s);
+                hi = __dmul_rn(hi, s);
+            }
+        }
+        if (CPLX) ((cd *)out)[b] = cd{hr, hi};
+        else ((double *)out)[b] = hr;
+    }
+}
+
+// ---- host side ---------------------------------------------------------------------------------
+
+static int64_t term_count(const int64_t *reps, int64_t E, int glynn)
+{
+    // The odometer's range: prod(r_i + 1), the leading digit clipped to (r_1 + 2) / 2 under Glynn
+    // (the `total` of _sieve_variant_cost, src/hafnian.jl:865).
+    int64_t steps = 1;
+    for (int64_t i = 0; i < E; ++i) {
+        int64_t f = (glynn && i == 0) ? (reps[i] + 2) / 2 : reps[i] + 1;
+        if (f <= 0) return -1;
+        if (steps > INT64_MAX / f) return -1;
+        steps *= f;
+    }
+    return E == 0 ? 0 : steps;
+}
+
+int sieve_batch_run(int dtype, int64_t B, int64_t Emax, const void *dAx, const int64_t *E, const int64_t *edge_reps,
+                    const int32_t *glynn, void *dout, cudaStream_t st)
+{
+    Context &c = ctx();
+    const int cplx = dtype == EGG_C128;
+    std::vector<SieveInst> inst((size_t)B);
+    std::vector<int> reps;
+    int maxrep = 0, nmax = 0;
+    int64_t maxsteps = 0;
+    const int lda = (int)(2 * Emax);
+    for (int64_t b = 0; b < B; ++b) {
+        SieveInst &s = inst[(size_t)b];
+        s.E = (int)E[b];
+        s.glynn = glynn[b] ? 1 : 0;
+        s.lda = lda > 0 ? lda : 1;
+        s.ax_off = b * (int64_t)lda * lda;
+        s.reps_off = (int64_t)reps.size();
+        int64_t n = 0;
+        for (int64_t i = 0; i < s.E; ++i) {
+            int64_t r = edge_reps[b * Emax + i];
+            if (r < 0 || r > 1000000) return fail(EGG_ERR_ARGUMENT, "edge multiplicities must be non-negative");
+            reps.push_back((int)r);
+            n += r;
+            if (r > maxrep) maxrep = (int)r;
+        }
+        if (n > 64) return fail(EGG_ERR_TOO_LARGE, "the device sieve extracts coefficients up to lambda^64");
+        s.n = (int)n;
+        nmax = s.n > nmax ? s.n : nmax;
+        s.steps = term_count(edge_reps + b * Emax, s.E, s.glynn);
+        if (s.steps < 0) return fail(EGG_ERR_TOO_LARGE, "the sieve's term count overflows Int64");
+        maxsteps = s.steps > maxsteps ? s.steps : maxsteps;
+    }
+    std::vector<double> binoms((size_t)(maxrep + 1) * (maxrep + 1), 0.0);
+    for (int aa = 0; aa <= maxrep; ++aa) {
+        double v = 1.0;  // C(aa, bb) built exactly in doubles for the small multiplicities used here
+        for (int bb = 0; bb <= aa; ++bb) {
+            binoms[(size_t)aa + (size_t)bb * (maxrep + 1)] = v;
+            v = v * (double)(aa - bb) / (double)(bb + 1);
+        }
+    }
+    // Launch shape: warps per block from the shared workspace size; enough warps per instance to
+    // fill the machine when B is small, capped by the instance's term count.
+    const int Ews = (int)(Emax > 0 ? Emax : 1);
+    const size_t wsd = ws_doubles(Ews, nmax, cplx);
+    const size_t per_warp = wsd * sizeof(double);
+    int wpb = (int)((200 * 1024) / per_warp);
+    if (wpb > 8) wpb = 8;
+    if (wpb < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
+    int64_t target_warps = (int64_t)c.num_sms * wpb * 2;  // a couple of blocks per SM overall
+    int64_t per_inst = (target_warps + B - 1) / B;
+    if (per_inst > maxsteps) per_inst = maxsteps;
+    if (per_inst < 1) per_inst = 1;
+    int blocks_x = (int)((per_inst + wpb - 1) / wpb);
+    int warps_per_inst = blocks_x * wpb;
+    if (B > 65535) return fail(EGG_ERR_ARGUMENT, "batch too large for one launch (max 65535)");
+
+    // Device staging: instance table, reps, binoms, partials -- one scratch allocation.
+    size_t off_inst = 0;
+    size_t off_reps = off_inst + ((inst.size() * sizeof(SieveInst) + 255) & ~(size_t)255);
+    size_t off_bin = off_reps + ((reps.size() * sizeof(int) + 256 + 255) & ~(size_t)255);
+    size_t off_part = off_bin + ((binoms.size() * sizeof(double) + 255) & ~(size_t)255);
+    size_t total = off_part + (size_t)B * warps_per_inst * 2 * sizeof(dd);
+    int rc = ensure_buf(c.scratch[5], total);
+    if (rc) return rc;
+    char *base = (char *)c.scratch[5].ptr;
+    EGG_CUDA_TRY(cudaMemcpyAsync(base + off_inst, inst.data(), inst.size() * sizeof(SieveInst), cudaMemcpyHostToDevice, st));
+    if (!reps.empty())
+        EGG_CUDA_TRY(cudaMemcpyAsync(base + off_reps, reps.data(), reps.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    EGG_CUDA_TRY(cudaMemcpyAsync(base + off_bin, binoms.data(), binoms.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    SieveArgs a;
+    a.Ax = dAx;
+    a.reps = (const int *)(base + off_reps);
+    a.binoms = (const double *)(base + off_bin);
+    a.inst = (const SieveInst *)(base + off_inst);
+    a.partial = (dd *)(base + off_part);
+    a.maxrep = maxrep;
+    a.warps_per_inst = warps_per_inst;
+    a.Emax = Ews;
+    a.nmax = nmax;
+    size_t smem = (size_t)wpb * per_warp;
+    dim3 grid((unsigned)blocks_x, (unsigned)B);
+    if (cplx) {
+        EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sieve_exact_kernel<true><<<grid, wpb * 32, smem, st>>>(a, wpb);
+        sieve_reduce_kernel<true><<<(unsigned)B, 256, 0, st>>>(a.partial, warps_per_inst, a.inst, dout);
+    } else {
+        EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sieve_exact_kernel<false><<<grid, wpb * 32, smem, st>>>(a, wpb);
+        sieve_reduce_kernel<false><<<(unsigned)B, 256, 0, st>>>(a.partial, warps_per_inst, a.inst, dout);
+    }
+    EGG_CUDA_TRY(cudaGetLastError());
+    return EGG_OK;
+}
+
+int sieve_run(int dtype, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, void *dout, cudaStream_t st)
+{
+    int32_t g = glynn ? 1 : 0;
+    int64_t e = E;
+    std::vector<int64_t> reps(edge_reps, edge_reps + E);
+    if (reps.empty()) reps.push_back(0);
+    return sieve_batch_run(dtype, 1, E, dAx, &e, reps.data(), &g, dout, st);
+}
+
+}  // namespace egg

@@ -1,0 +1,463 @@
+"""Public API: the reference's `hafnian` / `hafnian_repeated` surface, served by the B200 engine.
+
+This mirrors src/hafnian.jl:1111-1374 (entry points, validation, strategy routing) and the device
+hook of src/dp.jl:514-587.  Validation and routing are host logic; every hafnian is computed on the
+GPU by libeggman_b200 (the subset DP or the sieve), never on the CPU.
+
+Differences from the reference, all additive:
+  * `:unrolled` (straight-line CPU code for degree <= 12, src/unrolled.jl) is served by the device
+    DP, which evaluates the same recursion in the same order and so returns the same bits;
+  * `prec` picks the DP's rounding ("exact" = the reference CPU's, "fma" = the reference GPU
+    kernel's, "mixed" = FP32 multiplies with FP64 accumulation);
+  * `exact=True` runs integer matrices in Int64/Int128 instead of promoting them to Float64.
+"""
+from __future__ import annotations
+
+import os
+import threading
+
+import numpy as np
+
+from . import _native as nat
+from . import policy as pol
+from ._native import ArgumentError, DimensionMismatch
+
+_lock = threading.RLock()
+_resident: set[tuple[int, int]] = set()
+
+
+class B200Backend:
+    """Marker for the device backend (the reference's `backend` keyword takes a KA backend)."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+
+    def __repr__(self):
+        return f"B200Backend({self.device})"
+
+
+def _default_nthreads() -> int:
+    return os.cpu_count() or 1
+
+
+# ----------------------------------------------------------------------------------------------
+# Plans and caches (src/dp.jl:306-329, :536-587)
+# ----------------------------------------------------------------------------------------------
+
+def _dp_plan(K: int, idx_bytes: int | None = None) -> tuple[int, int]:
+    """Make the degree-K plan resident on the device (built there, cached for the session).
+
+    Returns the cache key (K, idx_bytes).  Mirrors _dp_plan (src/dp.jl:325-329) and
+    _device_plan (ext/TheEggmanKernelAbstractionsExt.jl:31-42) in one step.
+    """
+    ib = pol._dp_index_bytes(K) if idx_bytes is None else idx_bytes
+    key = (K, ib)
+    with _lock:
+        if key not in _resident:
+            nat.check(nat.lib().egg_plan_build(K, ib))
+            _resident.add(key)
+    return key
+
+
+def upload_plan(K: int, idx_bytes: int, starts: np.ndarray, trans: np.ndarray, levels: np.ndarray) -> None:
+    """Upload a host-built plan in the reference layout (what the Julia shim does with the
+    HafnianDPPlan it built; src/dp.jl:150-156)."""
+    dt = np.int32 if idx_bytes == 4 else np.int64
+    st = np.ascontiguousarray(starts, dtype=dt)
+    tr = np.ascontiguousarray(trans, dtype=dt)
+    lv = np.ascontiguousarray(levels, dtype=dt)
+    with _lock:
+        nat.check(nat.lib().egg_plan_upload(K, idx_bytes, nat.ptr(st), nat.ptr(tr) if tr.size else None,
+                                            nat.ptr(lv), lv.size, st.size - 1, tr.size))
+        _resident.add((K, idx_bytes))
+
+
+def download_plan(K: int, idx_bytes: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Copy a resident plan back in the reference layout (starts, trans, levels)."""
+    import ctypes
+
+    ns, nt, nl, _ = (ctypes.c_int64() for _ in range(4))
+    nat.check(nat.lib().egg_plan_info(K, idx_bytes, ctypes.byref(ns), ctypes.byref(nt), ctypes.byref(nl), None))
+    dt = np.int32 if idx_bytes == 4 else np.int64
+    starts = np.zeros(ns.value + 1, dt)
+    trans = np.zeros(max(nt.value, 1), dt)
+    levels = np.zeros(nl.value, dt)
+    nat.check(nat.lib().egg_plan_download(K, idx_bytes, nat.ptr(starts), nat.ptr(trans), nat.ptr(levels)))
+    return starts, trans[: nt.value], levels
+
+
+def gpu_cache_bytes() -> int:
+    """Device memory held by resident plans and work buffers (src/dp.jl:552-560)."""
+    return int(nat.lib().egg_cache_bytes())
+
+
+def empty_gpu_cache() -> None:
+    """Drop every resident plan and work buffer (src/dp.jl:567-573)."""
+    with _lock:
+        nat.check(nat.lib().egg_cache_clear())
+        _resident.clear()
+
+
+def dp_batch_bytes(N: int, T, B: int) -> int:
+    """B x (nstates + npairs) x sizeof(T) (src/dp.jl:584-587): an upper bound on the device memory
+    one batch needs besides the plan."""
+    nstates, _ = pol._dp_counts(N)
+    return B * (nstates + N * (N - 1) // 2) * np.dtype(T).itemsize
+
+
+# ----------------------------------------------------------------------------------------------
+# Validation (src/hafnian.jl:744-809)
+# ----------------------------------------------------------------------------------------------
+
+def _haf_dtype(A: np.ndarray) -> np.dtype:
+    """float(eltype(A)) (src/hafnian.jl:744): integers and bools promote to Float64."""
+    if A.dtype.kind in "iub":
+        return np.dtype(np.float64)
+    if A.dtype in (np.float16,):
+        return np.dtype(np.float32)
+    if A.dtype not in (np.float64, np.float32, np.complex128, np.complex64):
+        raise ArgumentError(f"unsupported element type {A.dtype}")
+    return A.dtype
+
+
+def _checksquare(A: np.ndarray) -> int:
+    if A.ndim != 2 or A.shape[0] != A.shape[1]:
+        raise DimensionMismatch(f"matrix is not square: dimensions are {A.shape}")
+    return A.shape[0]
+
+
+def _check_symmetric(A: np.ndarray) -> None:
+    """Symmetric to isapprox's default tolerance, squared (src/hafnian.jl:765-779); reports the
+    first offending (i, j) in the reference's column-major order over the upper triangle."""
+    n = A.shape[0]
+    if n < 2:
+        return
+    X = np.asarray(A)
+    kind = X.dtype.kind
+    real_t = np.float32 if X.dtype in (np.float32, np.complex64) else np.float64
+    tol = float(np.finfo(real_t).eps)
+    with np.errstate(invalid="ignore", over="ignore"):
+        neq = X != X.T
+        if not neq.any():
+            return
+        if kind in "iub":
+            Xf = X.astype(np.float64)
+        else:
+            Xf = X
+        d = Xf - Xf.T
+        ad = (d * np.conj(d)).real if np.iscomplexobj(d) else d * d
+        ax = (Xf * np.conj(Xf)).real if np.iscomplexobj(Xf) else Xf * Xf
+        ok = ad <= tol * np.maximum(ax, ax.T)
+        bad = neq & ~ok
+    bad = np.triu(bad, 1)
+    if bad.any():
+        jj, ii = np.nonzero(bad.T)  # column-major scan: j outer, i inner
+        raise ArgumentError(f"matrix is not symmetric at ({ii[0] + 1}, {jj[0] + 1})")
+
+
+# ----------------------------------------------------------------------------------------------
+# Device calls
+# ----------------------------------------------------------------------------------------------
+
+def _triu_pairs(K: int) -> tuple[np.ndarray, np.ndarray]:
+    """(i, j) 0-based for q = 1..K(K-1)/2 in _pair_index order (row-major upper triangle)."""
+    iu, ju = np.triu_indices(K, 1)
+    return iu, ju
+
+
+def _gather_pairs_batch(T: np.dtype, mats: np.ndarray, idxs: np.ndarray, K: int) -> np.ndarray:
+    """P[b, q] = A_b[idx_b[i], idx_b[j]] for q = _pair_index(i, j, K), instance index fastest
+    (src/dp.jl:479-512).  mats is (B, N, N) or (N, N) shared; idxs is (B, K) 0-based."""
+    iu, ju = _triu_pairs(K)
+    ri = idxs[:, iu]
+    ci = idxs[:, ju]
+    if mats.ndim == 2:
+        P = mats[ri, ci]
+    else:
+        P = mats[np.arange(mats.shape[0])[:, None], ri, ci]
+    return np.asfortranarray(P.astype(T, copy=False))
+
+
+def _dp_device(T: np.dtype, P: np.ndarray, K: int, prec: str, max_batch, exact_int: bool):
+    """The B200 replacement of _haf_dp_backend(backend, P, plan; max_batch)
+    (ext/TheEggmanKernelAbstractionsExt.jl:90-146)."""
+    B = P.shape[0]
+    key = _dp_plan(K)
+    dtype = nat.EGG_I64 if exact_int else nat.DTYPE_OF[np.dtype(T)]
+    P = np.asfortranarray(P)
+    if exact_int:
+        out = np.zeros(2 * B, np.uint64)
+    else:
+        out = np.zeros(B, T)
+    if prec not in nat.PREC:
+        raise ArgumentError(f"prec must be one of {tuple(nat.PREC)}")
+    with _lock:
+        nat.check(nat.lib().egg_dp_batch(key[0], key[1], dtype, nat.PREC[prec], nat.ptr(P), B,
+                                         int(max_batch or 0), nat.ptr(out)))
+    if exact_int:
+        vals = []
+        for b in range(B):
+            v = int(out[2 * b]) | (int(out[2 * b + 1]) << 64)
+            vals.append(v - (1 << 128) if v >= (1 << 127) else v)
+        return vals
+    return out
+
+
+def _sieve_device_batch(T: np.dtype, Axs: list[np.ndarray], reps_list: list[list[int]], glynns: list[bool]) -> np.ndarray:
+    """One egg_sieve_batch call over instances of possibly different edge counts."""
+    B = len(Axs)
+    cplx = np.dtype(T).kind == "c"
+    CT = np.complex128 if cplx else np.float64
+    Emax = max((len(r) for r in reps_list), default=0)
+    lda = max(2 * Emax, 1)
+    slab = np.zeros((B, lda, lda), dtype=CT)  # per instance: column-major leading block
+    for b, (Ax, r) in enumerate(zip(Axs, reps_list)):
+        m = 2 * len(r)
+        if m:
+            slab[b, :m, :m] = np.asarray(Ax, dtype=CT).T  # store transposed so memory is column-major
+    E = np.array([len(r) for r in reps_list], dtype=np.int64)
+    reps = np.zeros((B, max(Emax, 1)), dtype=np.int64)
+    for b, r in enumerate(reps_list):
+        reps[b, : len(r)] = r
+    g = np.array([1 if x else 0 for x in glynns], dtype=np.int32)
+    out = np.zeros(B, CT)
+    with _lock:
+        nat.check(nat.lib().egg_sieve_batch(nat.EGG_C128 if cplx else nat.EGG_F64, B, Emax, nat.ptr(slab), nat.ptr(E),
+                                            nat.ptr(reps), nat.ptr(g), nat.ptr(out)))
+    return out.astype(T, copy=False)
+
+
+def _sieve_one(T: np.dtype, Ax: np.ndarray, edge_reps: list[int], glynn: bool):
+    """The device sieve in place of _calc_hafnian(Ax, edge_reps; glynn) (src/hafnian.jl:684-738).
+    The sieve runs in FP64 (complex: ComplexF64); the result is returned in T."""
+    cplx = np.dtype(T).kind == "c"
+    CT = np.complex128 if cplx else np.float64
+    E = len(edge_reps)
+    A = np.asfortranarray(np.asarray(Ax, dtype=CT))
+    reps = np.ascontiguousarray(edge_reps if E else [0], dtype=np.int64)
+    out = np.zeros(1, CT)
+    with _lock:
+        nat.check(nat.lib().egg_sieve(nat.EGG_C128 if cplx else nat.EGG_F64, nat.ptr(A) if E else None, E, nat.ptr(reps),
+                                      1 if glynn else 0, nat.ptr(out)))
+    return np.dtype(T).type(out[0])
+
+
+def _permuted(T, A: np.ndarray, x: list[int]) -> np.ndarray:
+    """Ax[a, b] = A[x[a], x[b]] (src/hafnian.jl:786-792)."""
+    xi = np.asarray(x, dtype=np.int64) - 1
+    return np.asarray(A)[np.ix_(xi, xi)].astype(T, copy=False)
+
+
+def _expanded_indices(rpt, total: int) -> np.ndarray:
+    """Row i repeated rpt[i] times, 0-based (src/hafnian.jl:1014-1021)."""
+    return np.repeat(np.arange(len(rpt), dtype=np.int64), np.asarray(rpt, dtype=np.int64))
+
+
+def _distinct_x(E: int) -> list[int]:
+    """Match vertex 2i-1 with 2i in the [first halves; second halves] layout (:1140-1145)."""
+    return [2 * i + 1 for i in range(E)] + [2 * i + 2 for i in range(E)]
+
+
+# ----------------------------------------------------------------------------------------------
+# Entry points
+# ----------------------------------------------------------------------------------------------
+
+def _is_batch(A) -> bool:
+    if isinstance(A, (list, tuple)):
+        return True
+    return isinstance(A, np.ndarray) and A.ndim == 3
+
+
+def hafnian(A, *, nthreads: int | None = None, glynn: bool | None = None, method: str = "auto",
+            check_symmetric: bool = True, backend=None, max_batch: int | None = None,
+            prec: str = "exact", exact: bool = False):
+    """Hafnian of the square symmetric matrix A (src/hafnian.jl:1111-1147), or of each matrix of a
+    batch (a list, or a (B, N, N) array; src/hafnian.jl:1263-1301).
+
+    `method` is "auto", "unrolled", "dp" or "sieve"; `glynn` forces the sieve variant; `backend`
+    steers the automatic choice to the DP as the reference does.  The diagonal is ignored; odd N
+    gives 0 and N = 0 gives 1.
+    """
+    if _is_batch(A):
+        return _hafnian_batch(A, nthreads=nthreads, glynn=glynn, method=method, check_symmetric=check_symmetric,
+                              backend=backend, max_batch=max_batch, prec=prec, exact=exact)
+    A = np.asarray(A)
+    N = _checksquare(A)
+    exact_int = exact and A.dtype.kind in "iub"
+    T = np.dtype(np.int64) if exact_int else _haf_dtype(A)
+    nthreads = nthreads or _default_nthreads()
+    if N == 0:
+        return 1 if exact_int else T.type(1)
+    if N % 2:
+        return 0 if exact_int else T.type(0)
+    pol._check_method(method, N)
+    if check_symmetric:
+        _check_symmetric(A)
+    E = N // 2
+    sel, sel_glynn = pol._choose_method_distinct(N, E, nthreads)
+    chosen = pol._steer_backend(sel if method == "auto" else method, backend, N, method)
+    use_glynn = sel_glynn if glynn is None else glynn
+    if exact_int and chosen == "sieve":
+        raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
+    if chosen in ("unrolled", "dp"):
+        P = _gather_pairs_batch(T, A, np.arange(N, dtype=np.int64)[None, :], N)
+        v = _dp_device(T, P, N, prec, None, exact_int)[0]
+        return v if exact_int else T.type(v)
+    return _sieve_one(T, _permuted(T, A, _distinct_x(E)), [1] * E, use_glynn)
+
+
+def hafnian_repeated(A, rpt, *, nthreads: int | None = None, glynn: bool | None = None, method: str = "auto",
+                     check_symmetric: bool = True, backend=None, max_batch: int | None = None,
+                     prec: str = "exact", exact: bool = False):
+    """Hafnian of A with row/column i repeated rpt[i] times, without forming that matrix
+    (src/hafnian.jl:1194-1222); with a list of patterns, one hafnian per pattern
+    (src/hafnian.jl:1317-1359).  The diagonal of A matters when some rpt[i] >= 2."""
+    if len(rpt) and isinstance(rpt[0], (list, tuple, np.ndarray)):
+        return _hafnian_repeated_batch(A, rpt, nthreads=nthreads, glynn=glynn, method=method,
+                                       check_symmetric=check_symmetric, backend=backend, max_batch=max_batch,
+                                       prec=prec, exact=exact)
+    A = np.asarray(A)
+    N = _checksquare(A)
+    rpt = [int(r) for r in rpt]
+    if len(rpt) != N:
+        raise DimensionMismatch(f"rpt has length {len(rpt)}, expected {N}")
+    if any(r < 0 for r in rpt):
+        raise ArgumentError("rpt must contain non-negative integers")
+    exact_int = exact and A.dtype.kind in "iub"
+    T = np.dtype(np.int64) if exact_int else _haf_dtype(A)
+    nthreads = nthreads or _default_nthreads()
+    total = sum(rpt)
+    if total == 0:
+        return 1 if exact_int else T.type(1)
+    if total % 2:
+        return 0 if exact_int else T.type(0)
+    pol._check_method(method, total)
+    if check_symmetric:
+        _check_symmetric(A)
+    x, edge_reps = pol.matched_reps(rpt)
+    sel, sel_glynn = pol._choose_method(total, edge_reps, nthreads)
+    chosen = pol._steer_backend(sel if method == "auto" else method, backend, total, method)
+    use_glynn = sel_glynn if glynn is None else glynn
+    if chosen != "sieve":
+        idx = _expanded_indices(rpt, total)
+        P = _gather_pairs_batch(T, A, idx[None, :], total)
+        v = _dp_device(T, P, total, prec, None, exact_int)[0]
+        return v if exact_int else T.type(v)
+    if exact_int:
+        raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
+    return _sieve_one(T, _permuted(T, A, x), edge_reps, use_glynn)
+
+
+def _hafnian_batch(As, *, nthreads, glynn, method, check_symmetric, backend, max_batch, prec, exact):
+    mats = [np.asarray(a) for a in As] if not isinstance(As, np.ndarray) else list(As)
+    B = len(mats)
+    if B == 0:
+        return np.zeros(0, dtype=np.float64)
+    exact_int = exact and all(m.dtype.kind in "iub" for m in mats)
+    T = np.dtype(np.int64) if exact_int else np.result_type(*[_haf_dtype(m) for m in mats])
+    N = _checksquare(mats[0])
+    for b, m in enumerate(mats):
+        if _checksquare(m) != N:
+            raise DimensionMismatch(f"matrix {b + 1} is {m.shape[0]}×{m.shape[1]}, expected {N}×{N}; a batch shares "
+                                    "one strategy and one plan")
+        if check_symmetric:
+            _check_symmetric(m)
+    if N == 0:
+        return [1] * B if exact_int else np.ones(B, T)
+    if N % 2:
+        return [0] * B if exact_int else np.zeros(B, T)
+    pol._check_method(method, N)
+    nthreads = nthreads or _default_nthreads()
+    if backend is not None:
+        chosen = pol._steer_backend(pol._choose_method_distinct(N, N // 2, nthreads)[0] if method == "auto" else method,
+                                    backend, N, method)
+    else:
+        # Without a backend the reference loops over hafnian(As[b]; nthreads=1, ...) (:1297-1300);
+        # every instance has the same size, so they all choose alike.
+        chosen = pol._choose_method_distinct(N, N // 2, 1)[0] if method == "auto" else method
+    stack = np.stack(mats)
+    if chosen in ("unrolled", "dp"):
+        idxs = np.tile(np.arange(N, dtype=np.int64), (B, 1))
+        P = _gather_pairs_batch(T, stack, idxs, N)
+        return _dp_device(T, P, N, prec, max_batch, exact_int)
+    if exact_int:
+        raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
+    sel_glynn = pol._choose_method_distinct(N, N // 2, 1 if backend is None else nthreads)[1]
+    use_glynn = sel_glynn if glynn is None else glynn
+    x = _distinct_x(N // 2)
+    return _sieve_device_batch(T, [_permuted(T, m, x) for m in mats], [[1] * (N // 2)] * B, [use_glynn] * B)
+
+
+def _hafnian_repeated_batch(A, rpts, *, nthreads, glynn, method, check_symmetric, backend, max_batch, prec, exact):
+    A = np.asarray(A)
+    B = len(rpts)
+    exact_int = exact and A.dtype.kind in "iub"
+    T = np.dtype(np.int64) if exact_int else _haf_dtype(A)
+    if B == 0:
+        return np.zeros(0, dtype=T)
+    N = _checksquare(A)
+    rpts = [[int(r) for r in rp] for rp in rpts]
+    total = sum(rpts[0])
+    for b, rp in enumerate(rpts):
+        if len(rp) != N:
+            raise DimensionMismatch(f"rpt {b + 1} has length {len(rp)}, expected {N}")
+        if any(r < 0 for r in rp):
+            raise ArgumentError(f"rpt {b + 1} contains a negative entry")
+        if sum(rp) != total:
+            raise ArgumentError(f"rpt {b + 1} sums to {sum(rp)}, but rpt 1 sums to {total}; a batch shares one plan, "
+                                "so every pattern must have the same total")
+    if check_symmetric:
+        _check_symmetric(A)
+    if total == 0:
+        return [1] * B if exact_int else np.ones(B, T)
+    if total % 2:
+        return [0] * B if exact_int else np.zeros(B, T)
+    pol._check_method(method, total)
+    if backend is not None and method in ("auto", "dp") and total <= pol.DP_HARD_MAX:
+        idxs = np.stack([_expanded_indices(rp, total) for rp in rpts])
+        P = _gather_pairs_batch(T, A, idxs, total)
+        return _dp_device(T, P, total, prec, max_batch, exact_int)
+    # Per-pattern choice, as the reference's loop over hafnian_repeated(A, rpts[b]; nthreads=1)
+    # (:1355-1358), then one device call per strategy.
+    out = [None] * B
+    dp_idx, sv_idx, sv_ax, sv_reps, sv_g = [], [], [], [], []
+    for b, rp in enumerate(rpts):
+        x, er = pol.matched_reps(rp)
+        sel, sg = pol._choose_method(total, er, 1)
+        chosen = sel if method == "auto" else method
+        if chosen != "sieve":
+            dp_idx.append(b)
+        else:
+            sv_idx.append(b)
+            sv_ax.append(_permuted(T, A, x))
+            sv_reps.append(er)
+            sv_g.append(sg if glynn is None else glynn)
+    if dp_idx:
+        idxs = np.stack([_expanded_indices(rpts[b], total) for b in dp_idx])
+        vals = _dp_device(T, _gather_pairs_batch(T, A, idxs, total), total, prec, max_batch, exact_int)
+        for k, b in enumerate(dp_idx):
+            out[b] = vals[k]
+    if sv_idx:
+        if exact_int:
+            raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
+        vals = _sieve_device_batch(T, sv_ax, sv_reps, sv_g)
+        for k, b in enumerate(sv_idx):
+            out[b] = vals[k]
+    return out if exact_int else np.array(out, dtype=T)
+
+
+def reduction(A, rpt) -> np.ndarray:
+    """A with row/column i repeated rpt[i] times (src/hafnian.jl:1369-1374)."""
+    A = np.asarray(A)
+    if _checksquare(A) != len(rpt):
+        raise DimensionMismatch("rpt must have one entry per row of A")
+    idx = _expanded_indices(rpt, int(sum(rpt)))
+    return A[np.ix_(idx, idx)]
+
+
+def sieve(Ax, edge_reps, *, glynn: bool = False):
+    """The device sieve on a pre-permuted matrix: _calc_hafnian(Ax, edge_reps; glynn)
+    (src/hafnian.jl:684), the seam the reference has no device hook for."""
+    Ax = np.asarray(Ax)
+    T = _haf_dtype(Ax)
+    return _sieve_one(T, Ax, list(edge_reps), glynn)
