@@ -92,6 +92,7 @@ class SieveWorkload:
         self.reps = np.ones(E, dtype=np.int64)
         self.flops = R.sieve_flops([1] * E, self.glynn, cplx)
         self.dtype = 1 if cplx else 0
+        self.prec = 1  # EGG_PREC_FMA: the register-resident kernels (the API default for the sieve)
         self.name = (f"config2{'b' if cplx else 'a'}: N={N} {'ComplexF64 N(0,1/(2N)) parts' if cplx else 'Float64 U[-1,1]/sqrt(N)'}, "
                      f"hafnian(A; method=:sieve) = {'Glynn' if self.glynn else 'inclusion-exclusion'}, "
                      f"{2 ** (E - 1) if self.glynn else 2 ** E} terms")
@@ -103,13 +104,13 @@ class SieveWorkload:
 
     def step_device(self, stream_ptr):
         L = self.egg.lib()
-        rc = L.egg_sieve_device(self.dtype, self.dAx.data_ptr(), self.E, self.reps.ctypes.data, int(self.glynn),
-                                self.dout.data_ptr(), stream_ptr)
+        rc = L.egg_sieve_device(self.dtype, self.prec, self.dAx.data_ptr(), self.E, self.reps.ctypes.data,
+                                int(self.glynn), self.dout.data_ptr(), stream_ptr)
         if rc:
             raise RuntimeError(L.egg_last_error().decode())
 
     def step_e2e(self):
-        return self.egg.hafnian(self.A, method="sieve", glynn=self.glynn, check_symmetric=False)
+        return self.egg.hafnian(self.A, method="sieve", glynn=self.glynn, check_symmetric=False, prec="fma")
 
     launches_per_step = 2  # sieve kernel + fixed-order reduction kernel
     kernel = "sieve"
@@ -248,7 +249,10 @@ def run_ours(args):
         raise SystemExit(L.egg_last_error().decode())
     wl = make_workload(args.workload, egg, W, rank)
     wl.setup_device(torch, dev)
-    stream = torch.cuda.current_stream(dev)
+    torch.cuda.synchronize(dev)
+    # A dedicated stream: the legacy default stream's handle is NULL, which the C ABI reads as
+    # "use the library's own stream", and events on one stream do not time work on another.
+    stream = torch.cuda.Stream(dev)
     sp = stream.cuda_stream
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
@@ -270,7 +274,8 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     evs = []
     for _ in range(args.steps):
-        flush.fill_(1.0)
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)

@@ -42,10 +42,12 @@ extern "C" {
 #define EGG_I64 4   /* Int64 entries; DP states and results are Int128 (two int64 words, low first) */
 
 /* ---- DP precision modes ------------------------------------------------------------------ */
-#define EGG_PREC_EXACT 0  /* one thread per state, plan order, no FMA contraction: bit-identical to
-                             the reference's CPU _dp_states! (src/dp.jl:344-363) */
-#define EGG_PREC_FMA 1    /* plan order with fused multiply-add (the reference GPU kernel's rounding,
-                             ext/TheEggmanKernelAbstractionsExt.jl:47-51) */
+#define EGG_PREC_EXACT 0  /* DP: one thread per state, plan order, no FMA contraction: bit-identical to
+                             the reference's CPU _dp_states! (src/dp.jl:344-363).  Sieve: every
+                             term in the reference's loop order and rounding. */
+#define EGG_PREC_FMA 1    /* DP: plan order with fused multiply-add (the reference GPU kernel's
+                             rounding, ext/TheEggmanKernelAbstractionsExt.jl:47-51).  Sieve: the
+                             register-resident fast kernels. */
 #define EGG_PREC_MIXED 2  /* FP32 multiplies, FP64 per-state accumulation, FP32 state storage
                              (F64/C128 inputs only) */
 
@@ -129,19 +131,22 @@ int egg_dp_batch_device(int K, int idx_bytes, int dtype, int prec, const void *P
  * edge_reps the E multiplicities from matched_reps (:142-188).  glynn selects the Glynn
  * (1) or inclusion-exclusion (0) variant.  FP64 per term, double-double accumulation of the
  * signed terms; out receives one value (EGG_F64 or EGG_C128).
+ * prec: EGG_PREC_EXACT evaluates every term in the reference's loop order and rounding (each term
+ * bit-identical to _glynn_term!, :528-602); EGG_PREC_FMA keeps each term's matrix in registers
+ * and uses fused multiply-adds (terms agree to rounding; the fast path).
  * Replaces _calc_hafnian (src/hafnian.jl:684); the reference has no device sieve. */
-int egg_sieve(int dtype, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, void *out);
+int egg_sieve(int dtype, int prec, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, void *out);
 
 /* Same, Ax and out in device memory (edge_reps on the host), enqueued on `stream`. */
-int egg_sieve_device(int dtype, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, void *out,
-                     void *stream);
+int egg_sieve_device(int dtype, int prec, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn,
+                     void *out, void *stream);
 
 /* B independent sieves in one call (the batched form the reference lacks: hafnian_repeated
  * runs its batch as a CPU loop, src/hafnian.jl:1355-1358).  Instance b has E[b] <= Emax edges;
  * its permuted matrix is the leading 2E[b] x 2E[b] block of the 2Emax x 2Emax column-major
  * slab at Ax + b*(2Emax)^2 elements; its multiplicities are edge_reps[b*Emax .. b*Emax+E[b]-1];
  * glynn[b] picks its variant.  out receives B values. */
-int egg_sieve_batch(int dtype, int64_t B, int64_t Emax, const void *Ax, const int64_t *E,
+int egg_sieve_batch(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax, const int64_t *E,
                     const int64_t *edge_reps, const int32_t *glynn, void *out);
 
 #ifdef __cplusplus

@@ -62,4 +62,4 @@ def test_fails_loudly_without_a_device(egg, W):
     out = np.zeros(1)
     A = np.eye(2)
     reps = np.ones(1, np.int64)
-    assert L.egg_sieve(0, A.ctypes.data, 1, reps.ctypes.data, 0, out.ctypes.data) == _native.EGG_ERR_NO_DEVICE
+    assert L.egg_sieve(0, 0, A.ctypes.data, 1, reps.ctypes.data, 0, out.ctypes.data) == _native.EGG_ERR_NO_DEVICE

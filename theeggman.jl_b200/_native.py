@@ -27,7 +27,7 @@ EGG_ERR_PLAN_INVALID = 8
 
 # element types
 EGG_F64, EGG_C128, EGG_F32, EGG_C64, EGG_I64 = 0, 1, 2, 3, 4
-# DP precision modes
+# precision modes (DP: all three; sieve: exact or fma)
 PREC = {"exact": 0, "fma": 1, "mixed": 2}
 
 DTYPE_OF = {
@@ -97,9 +97,9 @@ def lib() -> ctypes.CDLL:
     L.egg_plan_release.argtypes = [i32, i32]
     L.egg_dp_batch.argtypes = [i32, i32, i32, i32, vp, i64, i64, vp]
     L.egg_dp_batch_device.argtypes = [i32, i32, i32, i32, vp, i64, vp, vp]
-    L.egg_sieve.argtypes = [i32, vp, i64, vp, i32, vp]
-    L.egg_sieve_device.argtypes = [i32, vp, i64, vp, i32, vp, vp]
-    L.egg_sieve_batch.argtypes = [i32, i64, i64, vp, vp, vp, vp, vp]
+    L.egg_sieve.argtypes = [i32, i32, vp, i64, vp, i32, vp]
+    L.egg_sieve_device.argtypes = [i32, i32, vp, i64, vp, i32, vp, vp]
+    L.egg_sieve_batch.argtypes = [i32, i32, i64, i64, vp, vp, vp, vp, vp]
     return L
 
 

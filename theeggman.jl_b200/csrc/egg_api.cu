@@ -375,7 +375,7 @@ int egg_dp_batch_device(int K, int idx_bytes, int dtype, int prec, const void *P
     return dp_run(*plan, dtype, prec, P, B, out, st);
 }
 
-int egg_sieve(int dtype, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, void *out)
+int egg_sieve(int dtype, int prec, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, void *out)
 {
     EGG_GUARD();
     if (dtype != EGG_F64 && dtype != EGG_C128) return fail(EGG_ERR_ARGUMENT, "the sieve runs in Float64 or ComplexF64");
@@ -389,24 +389,25 @@ int egg_sieve(int dtype, const void *Ax, int64_t E, const int64_t *edge_reps, in
     rc = ensure_buf(c.scratch[4], 64);
     if (rc) return rc;
     if (abytes) EGG_CUDA_TRY(cudaMemcpyAsync(c.scratch[3].ptr, Ax, abytes, cudaMemcpyHostToDevice, c.stream));
-    rc = sieve_run(dtype, c.scratch[3].ptr, E, edge_reps, glynn, c.scratch[4].ptr, c.stream);
+    rc = sieve_run(dtype, prec, c.scratch[3].ptr, E, edge_reps, glynn, c.scratch[4].ptr, c.stream);
     if (rc) return rc;
     EGG_CUDA_TRY(cudaMemcpyAsync(out, c.scratch[4].ptr, es, cudaMemcpyDeviceToHost, c.stream));
     EGG_CUDA_TRY(cudaStreamSynchronize(c.stream));
     return EGG_OK;
 }
 
-int egg_sieve_device(int dtype, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, void *out, void *stream)
+int egg_sieve_device(int dtype, int prec, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, void *out,
+                     void *stream)
 {
     EGG_GUARD();
     if (dtype != EGG_F64 && dtype != EGG_C128) return fail(EGG_ERR_ARGUMENT, "the sieve runs in Float64 or ComplexF64");
     if (E < 0 || E > 32) return fail(EGG_ERR_TOO_LARGE, "the device sieve supports up to 32 edges (N <= 64)");
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
-    return sieve_run(dtype, Ax, E, edge_reps, glynn, out, st);
+    return sieve_run(dtype, prec, Ax, E, edge_reps, glynn, out, st);
 }
 
-int egg_sieve_batch(int dtype, int64_t B, int64_t Emax, const void *Ax, const int64_t *E, const int64_t *edge_reps,
-                    const int32_t *glynn, void *out)
+int egg_sieve_batch(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax, const int64_t *E,
+                    const int64_t *edge_reps, const int32_t *glynn, void *out)
 {
     EGG_GUARD();
     if (dtype != EGG_F64 && dtype != EGG_C128) return fail(EGG_ERR_ARGUMENT, "the sieve runs in Float64 or ComplexF64");
@@ -423,7 +424,7 @@ int egg_sieve_batch(int dtype, int64_t B, int64_t Emax, const void *Ax, const in
     rc = ensure_buf(c.scratch[4], (size_t)B * es + 64);
     if (rc) return rc;
     if (abytes) EGG_CUDA_TRY(cudaMemcpyAsync(c.scratch[3].ptr, Ax, abytes, cudaMemcpyHostToDevice, c.stream));
-    rc = sieve_batch_run(dtype, B, Emax, c.scratch[3].ptr, E, edge_reps, glynn, c.scratch[4].ptr, c.stream);
+    rc = sieve_batch_run(dtype, prec, B, Emax, c.scratch[3].ptr, E, edge_reps, glynn, c.scratch[4].ptr, c.stream);
     if (rc) return rc;
     EGG_CUDA_TRY(cudaMemcpyAsync(out, c.scratch[4].ptr, (size_t)B * es, cudaMemcpyDeviceToHost, c.stream));
     EGG_CUDA_TRY(cudaStreamSynchronize(c.stream));

@@ -151,9 +151,9 @@ int dp_run(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t B, 
 size_t dp_scratch_bytes(const DevPlan &plan, int dtype, int prec, int64_t B);
 
 // egg_sieve.cu
-int sieve_run(int dtype, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, void *dout,
+int sieve_run(int dtype, int prec, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, void *dout,
               cudaStream_t st);
-int sieve_batch_run(int dtype, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
+int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
                     const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st);
 
 inline size_t dtype_size(int dtype)

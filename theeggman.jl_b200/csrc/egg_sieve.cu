@@ -11,25 +11,9 @@
 // Work layout.  Instance b's terms j = 0..steps-1 are dealt round-robin to that instance's warps
 // (grid.y = instance).  The mixed-radix odometer (edge E least significant, the leading digit
 // clipped to its lower half under Glynn, :655-657) is decoded per term.
-#include "egg_internal.cuh"
+#include "egg_sieve.cuh"
 
 namespace egg {
-
-struct SieveInst {
-    int64_t ax_off;     // element offset of this instance's matrix (ld = lda)
-    int64_t steps;      // number of sieve terms
-    int64_t reps_off;   // offset into the reps array
-    int E, n, glynn, lda;
-};
-
-struct SieveArgs {
-    const void *Ax;
-    const int *reps;
-    const double *binoms;  // (maxrep+1) x (maxrep+1), binoms[a + b*(maxrep+1)] = C(a, b)
-    const SieveInst *inst;
-    dd *partial;           // [B][warps_per_inst][2]
-    int maxrep, warps_per_inst, Emax, nmax;
-};
 
 // Per-warp shared workspace, carved from dynamic shared memory.
 struct WarpWs {
@@ -368,7 +352,8 @@ __device__ void sieve_warp_exact(const SieveArgs &a, const SieveInst &in, WarpWs
         prefac = __shfl_sync(0xffffffffu, prefac, 0);
         __syncwarp();
         const int m = 2 * mE;
-        if (m == 0) continue;  // empty submatrix contributes zero (:566-567)
+        if (m == 0) continue;           // empty submatrix contributes zero (:566-567)
+        if (m <= a.skip_le) continue;   // evaluated by the fast kernels
         const int ld = w.ldm;
         // M = A_S X D (:582-593).
         if (!CPLX) {
@@ -434,18 +419,26 @@ __global__ void __launch_bounds__(256) sieve_exact_kernel(SieveArgs a, int warps
     }
 }
 
-// Sums each instance's per-warp partials in a fixed tree, applies the Glynn rescaling 2^-(n-1)
-// (:737) and writes the result.  One block of 256 threads per instance.
+// Sums each instance's per-warp partials (one array per kernel that evaluated some of its terms) in a fixed tree, applies the Glynn rescaling 2^-(n-1) (:737) and writes the result.
+// One block of 256 threads per instance.
+struct PartialSet {
+    const dd *p[6];  // exact kernel, then up to five register-tile size classes
+    int w[6];
+};
+
 template <bool CPLX>
-__global__ void sieve_reduce_kernel(const dd *partial, int warps_per_inst, const SieveInst *inst, void *out)
+__global__ void sieve_reduce_kernel(PartialSet ps, const SieveInst *inst, void *out)
 {
     __shared__ dd sre[256], sim[256];
     const int b = blockIdx.x, t = threadIdx.x;
     dd r{0.0, 0.0}, i{0.0, 0.0};
-    const dd *p = partial + (size_t)b * warps_per_inst * 2;
-    for (int w = t; w < warps_per_inst; w += 256) {
-        dd_add(r, p[2 * w]);
-        dd_add(i, p[2 * w + 1]);
+    for (int a = 0; a < 6; ++a) {
+        if (!ps.p[a]) continue;
+        const dd *p = ps.p[a] + (size_t)b * ps.w[a] * 2;
+        for (int w = t; w < ps.w[a]; w += 256) {
+            dd_add(r, p[2 * w]);
+            dd_add(i, p[2 * w + 1]);
+        }
     }
     sre[t] = r;
     sim[t] = i;
@@ -493,15 +486,21 @@ static int64_t term_count(const int64_t *reps, int64_t E, int glynn)
     return E == 0 ? 0 : steps;
 }
 
-int sieve_batch_run(int dtype, int64_t B, int64_t Emax, const void *dAx, const int64_t *E, const int64_t *edge_reps,
-                    const int32_t *glynn, void *dout, cudaStream_t st)
+static int64_t align256(int64_t x) { return (x + 255) & ~(int64_t)255; }
+
+int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
+                    const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st)
 {
     Context &c = ctx();
     const int cplx = dtype == EGG_C128;
+    if (prec != EGG_PREC_EXACT && prec != EGG_PREC_FMA) return fail(EGG_ERR_ARGUMENT, "the sieve takes EGG_PREC_EXACT or EGG_PREC_FMA");
+    if (B > 65535) return fail(EGG_ERR_ARGUMENT, "batch too large for one launch (max 65535)");
     std::vector<SieveInst> inst((size_t)B);
     std::vector<int> reps;
+    std::vector<int64_t> strides;
     int maxrep = 0, nmax = 0;
     int64_t maxsteps = 0;
+    int mmin_all = 1 << 30, mmax_all = 0;  // range of term sizes any instance can produce
     const int lda = (int)(2 * Emax);
     for (int64_t b = 0; b < B; ++b) {
         SieveInst &s = inst[(size_t)b];
@@ -511,89 +510,150 @@ int sieve_batch_run(int dtype, int64_t B, int64_t Emax, const void *dAx, const i
         s.ax_off = b * (int64_t)lda * lda;
         s.reps_off = (int64_t)reps.size();
         int64_t n = 0;
+        int fixed = 0;  // edges that never vanish (Glynn with odd multiplicity)
         for (int64_t i = 0; i < s.E; ++i) {
             int64_t r = edge_reps[b * Emax + i];
             if (r < 0 || r > 1000000) return fail(EGG_ERR_ARGUMENT, "edge multiplicities must be non-negative");
             reps.push_back((int)r);
             n += r;
             if (r > maxrep) maxrep = (int)r;
+            if (s.glynn && (r % 2 == 1)) ++fixed;
         }
-        if (n > 64) return fail(EGG_ERR_TOO_LARGE, "the device sieve extracts coefficients up to lambda^64");
+        if (n > 63) return fail(EGG_ERR_TOO_LARGE, "the device sieve extracts coefficients up to lambda^63");
         s.n = (int)n;
         nmax = s.n > nmax ? s.n : nmax;
         s.steps = term_count(edge_reps + b * Emax, s.E, s.glynn);
         if (s.steps < 0) return fail(EGG_ERR_TOO_LARGE, "the sieve's term count overflows Int64");
         maxsteps = s.steps > maxsteps ? s.steps : maxsteps;
+        // mixed-radix place values, edge E-1 least significant
+        std::vector<int64_t> pv((size_t)s.E);
+        int64_t acc = 1;
+        for (int64_t i = s.E - 1; i >= 0; --i) {
+            pv[(size_t)i] = acc;
+            int64_t r = edge_reps[b * Emax + i];
+            acc *= (s.glynn && i == 0) ? (r + 2) / 2 : r + 1;
+        }
+        strides.insert(strides.end(), pv.begin(), pv.end());
+        if (s.steps > 0) {
+            mmin_all = 2 * fixed < mmin_all ? 2 * fixed : mmin_all;
+            mmax_all = 2 * s.E > mmax_all ? 2 * s.E : mmax_all;
+        }
     }
     std::vector<double> binoms((size_t)(maxrep + 1) * (maxrep + 1), 0.0);
     for (int aa = 0; aa <= maxrep; ++aa) {
-        double v = 1.0;  // C(aa, bb) built exactly in doubles for the small multiplicities used here
+        double v = 1.0;  // C(aa, bb), exact for the small multiplicities used here
         for (int bb = 0; bb <= aa; ++bb) {
             binoms[(size_t)aa + (size_t)bb * (maxrep + 1)] = v;
             v = v * (double)(aa - bb) / (double)(bb + 1);
         }
     }
-    // Launch shape: warps per block from the shared workspace size; enough warps per instance to
-    // fill the machine when B is small, capped by the instance's term count.
     const int Ews = (int)(Emax > 0 ? Emax : 1);
-    const size_t wsd = ws_doubles(Ews, nmax, cplx);
-    const size_t per_warp = wsd * sizeof(double);
-    int wpb = (int)((200 * 1024) / per_warp);
-    if (wpb > 8) wpb = 8;
-    if (wpb < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
-    int64_t target_warps = (int64_t)c.num_sms * wpb * 2;  // a couple of blocks per SM overall
-    int64_t per_inst = (target_warps + B - 1) / B;
-    if (per_inst > maxsteps) per_inst = maxsteps;
-    if (per_inst < 1) per_inst = 1;
-    int blocks_x = (int)((per_inst + wpb - 1) / wpb);
-    int warps_per_inst = blocks_x * wpb;
-    if (B > 65535) return fail(EGG_ERR_ARGUMENT, "batch too large for one launch (max 65535)");
 
-    // Device staging: instance table, reps, binoms, partials -- one scratch allocation.
-    size_t off_inst = 0;
-    size_t off_reps = off_inst + ((inst.size() * sizeof(SieveInst) + 255) & ~(size_t)255);
-    size_t off_bin = off_reps + ((reps.size() * sizeof(int) + 256 + 255) & ~(size_t)255);
-    size_t off_part = off_bin + ((binoms.size() * sizeof(double) + 255) & ~(size_t)255);
-    size_t total = off_part + (size_t)B * warps_per_inst * 2 * sizeof(dd);
-    int rc = ensure_buf(c.scratch[5], total);
+    // Which kernels run: in FMA mode, each register-tile size class that some instance's terms can
+    // fall in; the exact kernel takes everything in exact mode, else whatever exceeds the tiles.
+    const int fast_hi = cplx ? 32 : 48;
+    const int nclass = cplx ? kFastClassesCplx : kFastClassesReal;
+    bool run_cls[kFastClassesReal] = {false, false, false, false, false};
+    int ncls_run = 0;
+    if (prec == EGG_PREC_FMA)
+        for (int k = 0; k < nclass; ++k) {
+            run_cls[k] = mmax_all > kFastClasses[k][0] && mmin_all <= kFastClasses[k][1] && mmax_all > 0;
+            ncls_run += run_cls[k];
+        }
+    const bool run_ex = prec == EGG_PREC_EXACT || mmax_all > fast_hi || mmax_all == 0;
+    const int skip_le = prec == EGG_PREC_EXACT ? 0 : fast_hi;
+
+    // Launch shapes.
+    auto per_inst_blocks = [&](int wpb) {
+        int64_t target = (int64_t)c.num_sms * 32;  // resident-warp budget across the machine
+        int64_t per = (target + B - 1) / B;
+        if (per > maxsteps) per = maxsteps;
+        if (per < 1) per = 1;
+        return (int)((per + wpb - 1) / wpb);
+    };
+    const size_t ex_per_warp = ws_doubles(Ews, nmax, cplx) * sizeof(double);
+    int ex_wpb = (int)((200 * 1024) / ex_per_warp);
+    if (ex_wpb > 8) ex_wpb = 8;
+    if (run_ex && ex_wpb < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
+    const int ex_bx = run_ex ? per_inst_blocks(ex_wpb) : 0;
+    const int fwpb = 8;
+    if (fast_smem_bytes(nmax, cplx, fwpb) > 220 * 1024) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
+    const int f_bx = ncls_run ? per_inst_blocks(fwpb) : 0;
+
+    // Device staging: instance table, reps, strides, binoms, partials -- one scratch allocation.
+    int64_t off = 0;
+    const int64_t off_inst = off; off = align256(off + (int64_t)(inst.size() * sizeof(SieveInst)));
+    const int64_t off_reps = off; off = align256(off + (int64_t)((reps.size() + 1) * sizeof(int)));
+    const int64_t off_str = off; off = align256(off + (int64_t)((strides.size() + 1) * sizeof(int64_t)));
+    const int64_t off_bin = off; off = align256(off + (int64_t)(binoms.size() * sizeof(double)));
+    const int64_t off_pex = off; off = align256(off + (run_ex ? B * ex_bx * ex_wpb * 2 * (int64_t)sizeof(dd) : 0));
+    const int64_t off_pf = off; off = align256(off + (int64_t)ncls_run * B * f_bx * fwpb * 2 * (int64_t)sizeof(dd));
+    int rc = ensure_buf(c.scratch[5], (size_t)off + 256);
     if (rc) return rc;
     char *base = (char *)c.scratch[5].ptr;
     EGG_CUDA_TRY(cudaMemcpyAsync(base + off_inst, inst.data(), inst.size() * sizeof(SieveInst), cudaMemcpyHostToDevice, st));
     if (!reps.empty())
         EGG_CUDA_TRY(cudaMemcpyAsync(base + off_reps, reps.data(), reps.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    if (!strides.empty())
+        EGG_CUDA_TRY(cudaMemcpyAsync(base + off_str, strides.data(), strides.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
     EGG_CUDA_TRY(cudaMemcpyAsync(base + off_bin, binoms.data(), binoms.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     SieveArgs a;
     a.Ax = dAx;
     a.reps = (const int *)(base + off_reps);
     a.binoms = (const double *)(base + off_bin);
     a.inst = (const SieveInst *)(base + off_inst);
-    a.partial = (dd *)(base + off_part);
     a.maxrep = maxrep;
-    a.warps_per_inst = warps_per_inst;
     a.Emax = Ews;
     a.nmax = nmax;
-    size_t smem = (size_t)wpb * per_warp;
-    dim3 grid((unsigned)blocks_x, (unsigned)B);
-    if (cplx) {
-        EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        sieve_exact_kernel<true><<<grid, wpb * 32, smem, st>>>(a, wpb);
-        sieve_reduce_kernel<true><<<(unsigned)B, 256, 0, st>>>(a.partial, warps_per_inst, a.inst, dout);
-    } else {
-        EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        sieve_exact_kernel<false><<<grid, wpb * 32, smem, st>>>(a, wpb);
-        sieve_reduce_kernel<false><<<(unsigned)B, 256, 0, st>>>(a.partial, warps_per_inst, a.inst, dout);
+    a.skip_le = skip_le;
+    PartialSet ps;
+    for (int k = 0; k < 6; ++k) {
+        ps.p[k] = nullptr;
+        ps.w[k] = 0;
     }
+    if (ncls_run) {
+        a.warps_per_inst = f_bx * fwpb;
+        a.partial = nullptr;
+        int slot = 1;
+        for (int k = 0; k < nclass; ++k) {
+            if (!run_cls[k]) continue;
+            dd *part = (dd *)(base + off_pf) + (size_t)(slot - 1) * B * a.warps_per_inst * 2;
+            rc = launch_fast(a, (const int64_t *)(base + off_str), (int)B, cplx, k, part, fwpb, f_bx, st);
+            if (rc) return rc;
+            ps.p[slot] = part;
+            ps.w[slot] = a.warps_per_inst;
+            ++slot;
+        }
+    }
+    if (run_ex) {
+        a.warps_per_inst = ex_bx * ex_wpb;
+        a.partial = (dd *)(base + off_pex);
+        size_t smem = (size_t)ex_wpb * ex_per_warp;
+        dim3 grid((unsigned)ex_bx, (unsigned)B);
+        if (cplx) {
+            EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            sieve_exact_kernel<true><<<grid, ex_wpb * 32, smem, st>>>(a, ex_wpb);
+        } else {
+            EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            sieve_exact_kernel<false><<<grid, ex_wpb * 32, smem, st>>>(a, ex_wpb);
+        }
+        ps.p[0] = a.partial;
+        ps.w[0] = a.warps_per_inst;
+    }
+    if (cplx) sieve_reduce_kernel<true><<<(unsigned)B, 256, 0, st>>>(ps, a.inst, dout);
+    else sieve_reduce_kernel<false><<<(unsigned)B, 256, 0, st>>>(ps, a.inst, dout);
     EGG_CUDA_TRY(cudaGetLastError());
     return EGG_OK;
 }
 
-int sieve_run(int dtype, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, void *dout, cudaStream_t st)
+int sieve_run(int dtype, int prec, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, void *dout,
+              cudaStream_t st)
 {
     int32_t g = glynn ? 1 : 0;
     int64_t e = E;
     std::vector<int64_t> reps(edge_reps, edge_reps + E);
     if (reps.empty()) reps.push_back(0);
-    return sieve_batch_run(dtype, 1, E, dAx, &e, reps.data(), &g, dout, st);
+    return sieve_batch_run(dtype, prec, 1, E, dAx, &e, reps.data(), &g, dout, st);
 }
 
 }  // namespace egg

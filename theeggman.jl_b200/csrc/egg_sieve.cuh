@@ -1,0 +1,34 @@
+// egg_sieve.cuh -- structures shared by the exact and the fast sieve kernels.
+#pragma once
+
+#include "egg_internal.cuh"
+
+namespace egg {
+
+struct SieveInst {
+    int64_t ax_off;     // element offset of this instance's matrix (ld = lda)
+    int64_t steps;      // number of sieve terms
+    int64_t reps_off;   // offset into the reps / strides arrays
+    int E, n, glynn, lda;
+};
+
+struct SieveArgs {
+    const void *Ax;
+    const int *reps;
+    const double *binoms;  // (maxrep+1) x (maxrep+1), binoms[a + b*(maxrep+1)] = C(a, b)
+    const SieveInst *inst;
+    dd *partial;           // [B][warps_per_inst][2]
+    int maxrep, warps_per_inst, Emax, nmax;
+    int skip_le;           // the exact kernel leaves terms with m <= skip_le to the fast kernels
+};
+
+// Fast path (egg_sieve_fast.cu): size class `cls` covers terms with kFastClasses[cls][0] < m <=
+// kFastClasses[cls][1]; classes 0-2 exist for real and complex terms, 3-4 (two rows per lane) for
+// real terms only.
+extern const int kFastClasses[][2];
+constexpr int kFastClassesReal = 5, kFastClassesCplx = 3;
+size_t fast_smem_bytes(int nmax, int cplx, int warps);
+int launch_fast(const SieveArgs &a, const int64_t *strides, int B, int cplx, int cls, dd *partial, int wpb,
+                int blocks_x, cudaStream_t st);
+
+}  // namespace egg

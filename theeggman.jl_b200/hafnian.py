@@ -7,8 +7,10 @@ GPU by libeggman_b200 (the subset DP or the sieve), never on the CPU.
 Differences from the reference, all additive:
   * `:unrolled` (straight-line CPU code for degree <= 12, src/unrolled.jl) is served by the device
     DP, which evaluates the same recursion in the same order and so returns the same bits;
-  * `prec` picks the DP's rounding ("exact" = the reference CPU's, "fma" = the reference GPU
-    kernel's, "mixed" = FP32 multiplies with FP64 accumulation);
+  * `prec` picks the rounding: "exact" = the reference CPU's, term by term, for both the DP and
+    the sieve; "fma" = fused multiply-adds (the reference GPU kernel's DP rounding, and the
+    register-resident sieve kernels); "mixed" = FP32 multiplies with FP64 accumulation in the
+    DP.  The default (None) runs the DP exactly and the sieve on the fast kernels;
   * `exact=True` runs integer matrices in Int64/Int128 instead of promoting them to Float64.
 """
 from __future__ import annotations
@@ -203,7 +205,21 @@ def _dp_device(T: np.dtype, P: np.ndarray, K: int, prec: str, max_batch, exact_i
     return out
 
 
-def _sieve_device_batch(T: np.dtype, Axs: list[np.ndarray], reps_list: list[list[int]], glynns: list[bool]) -> np.ndarray:
+def _dp_prec(prec) -> str:
+    """DP rounding: the reference CPU's (exact) unless asked otherwise."""
+    return "exact" if prec is None else prec
+
+
+def _sieve_prec(prec) -> int:
+    """Sieve kernel: reference loop order for prec='exact', the register-resident FMA kernels
+    otherwise (the default)."""
+    if prec not in (None, "exact", "fma", "mixed"):
+        raise ArgumentError("prec must be one of None, 'exact', 'fma', 'mixed'")
+    return nat.PREC["exact"] if prec == "exact" else nat.PREC["fma"]
+
+
+def _sieve_device_batch(T: np.dtype, Axs: list[np.ndarray], reps_list: list[list[int]], glynns: list[bool],
+                        prec=None) -> np.ndarray:
     """One egg_sieve_batch call over instances of possibly different edge counts."""
     B = len(Axs)
     cplx = np.dtype(T).kind == "c"
@@ -222,12 +238,12 @@ def _sieve_device_batch(T: np.dtype, Axs: list[np.ndarray], reps_list: list[list
     g = np.array([1 if x else 0 for x in glynns], dtype=np.int32)
     out = np.zeros(B, CT)
     with _lock:
-        nat.check(nat.lib().egg_sieve_batch(nat.EGG_C128 if cplx else nat.EGG_F64, B, Emax, nat.ptr(slab), nat.ptr(E),
-                                            nat.ptr(reps), nat.ptr(g), nat.ptr(out)))
+        nat.check(nat.lib().egg_sieve_batch(nat.EGG_C128 if cplx else nat.EGG_F64, _sieve_prec(prec), B, Emax, nat.ptr(slab),
+                                            nat.ptr(E), nat.ptr(reps), nat.ptr(g), nat.ptr(out)))
     return out.astype(T, copy=False)
 
 
-def _sieve_one(T: np.dtype, Ax: np.ndarray, edge_reps: list[int], glynn: bool):
+def _sieve_one(T: np.dtype, Ax: np.ndarray, edge_reps: list[int], glynn: bool, prec=None):
     """The device sieve in place of _calc_hafnian(Ax, edge_reps; glynn) (src/hafnian.jl:684-738).
     The sieve runs in FP64 (complex: ComplexF64); the result is returned in T."""
     cplx = np.dtype(T).kind == "c"
@@ -237,8 +253,8 @@ def _sieve_one(T: np.dtype, Ax: np.ndarray, edge_reps: list[int], glynn: bool):
     reps = np.ascontiguousarray(edge_reps if E else [0], dtype=np.int64)
     out = np.zeros(1, CT)
     with _lock:
-        nat.check(nat.lib().egg_sieve(nat.EGG_C128 if cplx else nat.EGG_F64, nat.ptr(A) if E else None, E, nat.ptr(reps),
-                                      1 if glynn else 0, nat.ptr(out)))
+        nat.check(nat.lib().egg_sieve(nat.EGG_C128 if cplx else nat.EGG_F64, _sieve_prec(prec), nat.ptr(A) if E else None, E,
+                                      nat.ptr(reps), 1 if glynn else 0, nat.ptr(out)))
     return np.dtype(T).type(out[0])
 
 
@@ -270,7 +286,7 @@ def _is_batch(A) -> bool:
 
 def hafnian(A, *, nthreads: int | None = None, glynn: bool | None = None, method: str = "auto",
             check_symmetric: bool = True, backend=None, max_batch: int | None = None,
-            prec: str = "exact", exact: bool = False):
+            prec: str | None = None, exact: bool = False):
     """Hafnian of the square symmetric matrix A (src/hafnian.jl:1111-1147), or of each matrix of a
     batch (a list, or a (B, N, N) array; src/hafnian.jl:1263-1301).
 
@@ -301,14 +317,14 @@ def hafnian(A, *, nthreads: int | None = None, glynn: bool | None = None, method
         raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
     if chosen in ("unrolled", "dp"):
         P = _gather_pairs_batch(T, A, np.arange(N, dtype=np.int64)[None, :], N)
-        v = _dp_device(T, P, N, prec, None, exact_int)[0]
+        v = _dp_device(T, P, N, _dp_prec(prec), None, exact_int)[0]
         return v if exact_int else T.type(v)
-    return _sieve_one(T, _permuted(T, A, _distinct_x(E)), [1] * E, use_glynn)
+    return _sieve_one(T, _permuted(T, A, _distinct_x(E)), [1] * E, use_glynn, prec)
 
 
 def hafnian_repeated(A, rpt, *, nthreads: int | None = None, glynn: bool | None = None, method: str = "auto",
                      check_symmetric: bool = True, backend=None, max_batch: int | None = None,
-                     prec: str = "exact", exact: bool = False):
+                     prec: str | None = None, exact: bool = False):
     """Hafnian of A with row/column i repeated rpt[i] times, without forming that matrix
     (src/hafnian.jl:1194-1222); with a list of patterns, one hafnian per pattern
     (src/hafnian.jl:1317-1359).  The diagonal of A matters when some rpt[i] >= 2."""
@@ -341,11 +357,11 @@ def hafnian_repeated(A, rpt, *, nthreads: int | None = None, glynn: bool | None 
     if chosen != "sieve":
         idx = _expanded_indices(rpt, total)
         P = _gather_pairs_batch(T, A, idx[None, :], total)
-        v = _dp_device(T, P, total, prec, None, exact_int)[0]
+        v = _dp_device(T, P, total, _dp_prec(prec), None, exact_int)[0]
         return v if exact_int else T.type(v)
     if exact_int:
         raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
-    return _sieve_one(T, _permuted(T, A, x), edge_reps, use_glynn)
+    return _sieve_one(T, _permuted(T, A, x), edge_reps, use_glynn, prec)
 
 
 def _hafnian_batch(As, *, nthreads, glynn, method, check_symmetric, backend, max_batch, prec, exact):
@@ -379,13 +395,13 @@ def _hafnian_batch(As, *, nthreads, glynn, method, check_symmetric, backend, max
     if chosen in ("unrolled", "dp"):
         idxs = np.tile(np.arange(N, dtype=np.int64), (B, 1))
         P = _gather_pairs_batch(T, stack, idxs, N)
-        return _dp_device(T, P, N, prec, max_batch, exact_int)
+        return _dp_device(T, P, N, _dp_prec(prec), max_batch, exact_int)
     if exact_int:
         raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
     sel_glynn = pol._choose_method_distinct(N, N // 2, 1 if backend is None else nthreads)[1]
     use_glynn = sel_glynn if glynn is None else glynn
     x = _distinct_x(N // 2)
-    return _sieve_device_batch(T, [_permuted(T, m, x) for m in mats], [[1] * (N // 2)] * B, [use_glynn] * B)
+    return _sieve_device_batch(T, [_permuted(T, m, x) for m in mats], [[1] * (N // 2)] * B, [use_glynn] * B, prec)
 
 
 def _hafnian_repeated_batch(A, rpts, *, nthreads, glynn, method, check_symmetric, backend, max_batch, prec, exact):
@@ -416,7 +432,7 @@ def _hafnian_repeated_batch(A, rpts, *, nthreads, glynn, method, check_symmetric
     if backend is not None and method in ("auto", "dp") and total <= pol.DP_HARD_MAX:
         idxs = np.stack([_expanded_indices(rp, total) for rp in rpts])
         P = _gather_pairs_batch(T, A, idxs, total)
-        return _dp_device(T, P, total, prec, max_batch, exact_int)
+        return _dp_device(T, P, total, _dp_prec(prec), max_batch, exact_int)
     # Per-pattern choice, as the reference's loop over hafnian_repeated(A, rpts[b]; nthreads=1)
     # (:1355-1358), then one device call per strategy.
     out = [None] * B
@@ -434,13 +450,13 @@ def _hafnian_repeated_batch(A, rpts, *, nthreads, glynn, method, check_symmetric
             sv_g.append(sg if glynn is None else glynn)
     if dp_idx:
         idxs = np.stack([_expanded_indices(rpts[b], total) for b in dp_idx])
-        vals = _dp_device(T, _gather_pairs_batch(T, A, idxs, total), total, prec, max_batch, exact_int)
+        vals = _dp_device(T, _gather_pairs_batch(T, A, idxs, total), total, _dp_prec(prec), max_batch, exact_int)
         for k, b in enumerate(dp_idx):
             out[b] = vals[k]
     if sv_idx:
         if exact_int:
             raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
-        vals = _sieve_device_batch(T, sv_ax, sv_reps, sv_g)
+        vals = _sieve_device_batch(T, sv_ax, sv_reps, sv_g, prec)
         for k, b in enumerate(sv_idx):
             out[b] = vals[k]
     return out if exact_int else np.array(out, dtype=T)
@@ -455,9 +471,10 @@ def reduction(A, rpt) -> np.ndarray:
     return A[np.ix_(idx, idx)]
 
 
-def sieve(Ax, edge_reps, *, glynn: bool = False):
+def sieve(Ax, edge_reps, *, glynn: bool = False, prec: str | None = None):
     """The device sieve on a pre-permuted matrix: _calc_hafnian(Ax, edge_reps; glynn)
-    (src/hafnian.jl:684), the seam the reference has no device hook for."""
+    (src/hafnian.jl:684), the seam the reference has no device hook for.  prec='exact' evaluates
+    every term in the reference's order and rounding; the default uses the fast kernels."""
     Ax = np.asarray(Ax)
     T = _haf_dtype(Ax)
-    return _sieve_one(T, Ax, list(edge_reps), glynn)
+    return _sieve_one(T, Ax, list(edge_reps), glynn, prec)
