@@ -141,6 +141,19 @@ int egg_sieve(int dtype, int prec, const void *Ax, int64_t E, const int64_t *edg
 int egg_sieve_device(int dtype, int prec, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn,
                      void *out, void *stream);
 
+/* The same sieve as egg_sieve_device, for callers that cannot let the library allocate device
+ * memory: a process whose GPU memory is owned by another allocator (a framework that reserves the
+ * device up front), or a loop that must not allocate once running.  Ax and out are the caller's
+ * device buffers; the sieve's scratch (its instance tables and per-warp partial sums) lives in a
+ * fixed 4 MiB array compiled into the library, present on every GPU that loads it until the
+ * process exits.  Nothing is allocated or freed.  A sieve needing more scratch than that (edge
+ * counts up to 32 fit) is refused with EGG_ERR_TOO_LARGE.  The first call on a device looks up
+ * the array's device address, so make it before any stream capture.  All calls share the array:
+ * calls whose device work overlaps race on it.  There is no counterpart of this entry point in the
+ * reference. */
+int egg_sieve_device_noalloc(int dtype, int prec, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn,
+                             void *out, void *stream);
+
 /* B independent sieves in one call (the batched form the reference lacks: hafnian_repeated
  * runs its batch as a CPU loop, src/hafnian.jl:1355-1358).  Instance b has E[b] <= Emax edges;
  * its permuted matrix is the leading 2E[b] x 2E[b] block of the 2Emax x 2Emax column-major

@@ -151,10 +151,18 @@ int dp_run(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t B, 
 size_t dp_scratch_bytes(const DevPlan &plan, int dtype, int prec, int64_t B);
 
 // egg_sieve.cu
+// A caller-provided device region for the sieve's tables and partial sums (used instead of the
+// library's growable buffer when given), with the SM count to shape the launches.
+struct FixedScratch {
+    void *ptr;
+    size_t bytes;
+    int num_sms;
+};
 int sieve_run(int dtype, int prec, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, void *dout,
               cudaStream_t st);
 int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
-                    const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st);
+                    const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st,
+                    const FixedScratch *fixed = nullptr);
 
 inline size_t dtype_size(int dtype)
 {

@@ -489,9 +489,11 @@ static int64_t term_count(const int64_t *reps, int64_t E, int glynn)
 static int64_t align256(int64_t x) { return (x + 255) & ~(int64_t)255; }
 
 int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
-                    const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st)
+                    const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st,
+                    const FixedScratch *fixed)
 {
     Context &c = ctx();
+    const int num_sms = fixed ? fixed->num_sms : c.num_sms;
     const int cplx = dtype == EGG_C128;
     if (prec != EGG_PREC_EXACT && prec != EGG_PREC_FMA) return fail(EGG_ERR_ARGUMENT, "the sieve takes EGG_PREC_EXACT or EGG_PREC_FMA");
     if (B > 65535) return fail(EGG_ERR_ARGUMENT, "batch too large for one launch (max 65535)");
@@ -565,7 +567,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
 
     // Launch shapes.
     auto per_inst_blocks = [&](int wpb) {
-        int64_t target = (int64_t)c.num_sms * 32;  // resident-warp budget across the machine
+        int64_t target = (int64_t)num_sms * 32;  // resident-warp budget across the machine
         int64_t per = (target + B - 1) / B;
         if (per > maxsteps) per = maxsteps;
         if (per < 1) per = 1;
@@ -588,9 +590,19 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     const int64_t off_bin = off; off = align256(off + (int64_t)(binoms.size() * sizeof(double)));
     const int64_t off_pex = off; off = align256(off + (run_ex ? B * ex_bx * ex_wpb * 2 * (int64_t)sizeof(dd) : 0));
     const int64_t off_pf = off; off = align256(off + (int64_t)ncls_run * B * f_bx * fwpb * 2 * (int64_t)sizeof(dd));
-    int rc = ensure_buf(c.scratch[5], (size_t)off + 256);
-    if (rc) return rc;
-    char *base = (char *)c.scratch[5].ptr;
+    char *base;
+    int rc;
+    if (fixed) {
+        if ((size_t)off + 256 > fixed->bytes)
+            return fail(EGG_ERR_TOO_LARGE, "this sieve needs " + std::to_string((size_t)off + 256) +
+                                               " bytes of scratch; the fixed scratch region holds " +
+                                               std::to_string(fixed->bytes));
+        base = (char *)fixed->ptr;
+    } else {
+        rc = ensure_buf(c.scratch[5], (size_t)off + 256);
+        if (rc) return rc;
+        base = (char *)c.scratch[5].ptr;
+    }
     EGG_CUDA_TRY(cudaMemcpyAsync(base + off_inst, inst.data(), inst.size() * sizeof(SieveInst), cudaMemcpyHostToDevice, st));
     if (!reps.empty())
         EGG_CUDA_TRY(cudaMemcpyAsync(base + off_reps, reps.data(), reps.size() * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -653,7 +665,7 @@ int sieve_run(int dtype, int prec, const void *dAx, int64_t E, const int64_t *ed
     int64_t e = E;
     std::vector<int64_t> reps(edge_reps, edge_reps + E);
     if (reps.empty()) reps.push_back(0);
-    return sieve_batch_run(dtype, prec, 1, E, dAx, &e, reps.data(), &g, dout, st);
+    return sieve_batch_run(dtype, prec, 1, E, dAx, &e, reps.data(), &g, dout, st, nullptr);
 }
 
 }  // namespace egg
