@@ -76,6 +76,8 @@ def profile_traffic(name: str):
 class SieveWorkload:
     """One N x N sieve hafnian per step (configuration 2: N = 40, real or complex)."""
 
+    kind = "sieve"
+
     def __init__(self, egg, W, N: int, cplx: bool, glynn, seed: int):
         from theeggman_b200 import policy as pol
         from theeggman_b200 import roofline as R
@@ -93,6 +95,8 @@ class SieveWorkload:
         self.flops = R.sieve_flops([1] * E, self.glynn, cplx)
         self.dtype = 1 if cplx else 0
         self.prec = 1  # EGG_PREC_FMA: the register-resident kernels (the API default for the sieve)
+        self.hafnians_per_step = 1
+        self.dtype_name = "c128" if cplx else "f64"
         self.name = (f"config2{'b' if cplx else 'a'}: N={N} {'ComplexF64 N(0,1/(2N)) parts' if cplx else 'Float64 U[-1,1]/sqrt(N)'}, "
                      f"hafnian(A; method=:sieve) = {'Glynn' if self.glynn else 'inclusion-exclusion'}, "
                      f"{2 ** (E - 1) if self.glynn else 2 ** E} terms")
@@ -112,8 +116,7 @@ class SieveWorkload:
     def step_e2e(self):
         return self.egg.hafnian(self.A, method="sieve", glynn=self.glynn, check_symmetric=False, prec="fma")
 
-    launches_per_step = 2  # sieve kernel + fixed-order reduction kernel
-    kernel = "sieve"
+    launches_per_step = 6  # up to five size-class kernels + the fixed-order reduction
 
     @property
     def h2d_bytes(self):
@@ -123,12 +126,219 @@ class SieveWorkload:
     def d2h_bytes(self):
         return 16 if self.cplx else 8
 
-    def cpu_time(self, nthreads: int):
+    def roofline(self, ms, peaks):
+        from theeggman_b200 import roofline as R
+
+        sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+        peak = R.fp64_nominal_tflops(sm_max)
+        achieved = self.flops / (ms / 1e3) / 1e12
+        return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": f"nominal FP64: 148 SMs x 64 FMA/clk x 2 x {sm_max:.0f} MHz (no FP64 figure in "
+                               "MEASURED_PEAKS.json)",
+                "work": f"{self.flops:.4e} algorithmic flops per hafnian"}
+
+    def cpu_sample(self, nthreads):
         from oracle import oracle as O
 
+        O.calc_hafnian(self.Ax, [1] * self.E, self.glynn, nthreads=nthreads)  # warm the thread pool
         t = time.perf_counter()
         O.calc_hafnian(self.Ax, [1] * self.E, self.glynn, nthreads=nthreads)
-        return time.perf_counter() - t
+        return 1.0 / (time.perf_counter() - t), "one full hafnian of the same workload (every sieve term), all host threads"
+
+
+class DPWorkload:
+    """B hafnians of degree N per step through the subset DP (configurations 1 and 3)."""
+
+    kind = "dp"
+
+    def __init__(self, egg, W, N: int, B: int, kind: str, prec: str, seed: int):
+        from theeggman_b200.hafnian import _gather_pairs_batch
+
+        self.egg, self.N, self.B, self.prec_name = egg, N, B, prec
+        self.code = {"f64": 0, "c128": 1, "i64": 4}[kind]
+        self.prec = {"exact": 0, "fma": 1, "mixed": 2}[prec]
+        T = {"f64": np.float64, "c128": np.complex128, "i64": np.int64}[kind]
+        self.T = np.dtype(T)
+        if kind == "i64":
+            self.mats = [W.er_graph(N, 0.5, seed + b) for b in range(B)]
+        elif kind == "c128":
+            self.mats = [W.dense_complex(N, seed + b, 1.0 / (2 * N)) for b in range(B)]
+        elif N >= 36:
+            self.mats = [W.dense_real(N, seed + b, 0.0, 1.0) for b in range(B)]
+        else:
+            self.mats = [W.dense_real(N, seed + b) for b in range(B)]
+        self.P = _gather_pairs_batch(T, np.stack(self.mats), np.tile(np.arange(N), (B, 1)), N)
+        self.hafnians_per_step = B
+        self.dtype_name = {"f64": "f64", "c128": "c128", "i64": "int64->int128"}[kind]
+        dist = {"f64": "Float64 U[0,1]" if N >= 36 else "Float64 U[-1,1]", "c128": "ComplexF64 N(0,1/(2N)) parts",
+                "i64": "0/1 Erdos-Renyi p=0.5 adjacency, Int128"}[kind]
+        self.name = f"DP N={N} B={B} {dist}, prec={prec}"
+        self.vbytes = {"f64": 8, "c128": 16, "i64": 8}[kind]
+        if prec == "mixed":
+            self.vbytes //= 2  # states and pairs are stored in FP32
+
+    def setup_device(self, torch, dev):
+        from theeggman_b200.hafnian import _dp_plan
+
+        self.key = _dp_plan(self.N)
+        tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.complex128): torch.complex128,
+               np.dtype(np.int64): torch.int64}[self.T]
+        self.dP = torch.from_numpy(np.ascontiguousarray(self.P.T)).to(dev, tdt)
+        self.dout = torch.zeros(2 * self.B, dtype=torch.float64, device=dev)
+
+    def step_device(self, stream_ptr):
+        L = self.egg.lib()
+        rc = L.egg_dp_batch_device(self.key[0], self.key[1], self.code, self.prec, self.dP.data_ptr(), self.B,
+                                   self.dout.data_ptr(), stream_ptr)
+        if rc:
+            raise RuntimeError(L.egg_last_error().decode())
+
+    def step_e2e(self):
+        exact = self.code == 4
+        if self.B == 1:
+            return self.egg.hafnian(self.mats[0], method="dp", check_symmetric=False, prec=self.prec_name, exact=exact)
+        return self.egg.hafnian(self.mats, method="dp", check_symmetric=False, prec=self.prec_name, exact=exact,
+                                backend=self.egg.B200Backend())
+
+    @property
+    def launches_per_step(self):
+        return self.N // 2 + 2
+
+    @property
+    def h2d_bytes(self):
+        return sum(m.nbytes for m in self.mats)
+
+    @property
+    def d2h_bytes(self):
+        return self.B * (16 if self.code in (1, 4) else 8)
+
+    def roofline(self, ms, peaks):
+        from theeggman_b200 import roofline as R
+
+        byts = R.dp_bytes(self.N, self.B, self.vbytes)
+        peak = float(peaks.get("hbm_gbs", 6650.0))
+        achieved = byts / (ms / 1e3) / 1e9
+        return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+                "work": f"{byts:.4e} algorithmic bytes per step (plan once + 2 states + pairs per instance)"}
+
+    def cpu_sample(self, nthreads):
+        from oracle import oracle as O
+        from theeggman_b200 import policy as pol
+
+        if self.N > 32:
+            # A CPU plan at this degree is gigabytes (24 GB of transitions at N = 40): time the
+            # reference loop on the N = 32 plan and scale by the transition counts.
+            Ns = 32
+            A = self.mats[0][:Ns, :Ns].astype(np.float64 if self.code != 4 else np.int64)
+            dt = O.F64 if self.code != 4 else O.I64
+            plan = O.build_plan(Ns, 4)
+            P = O.gather_pairs(A, list(range(1, Ns + 1)), Ns)
+            O.haf_dp_pairs(P, plan, dt, nthreads)
+            t = time.perf_counter()
+            O.haf_dp_pairs(P, plan, dt, nthreads)
+            dtm = time.perf_counter() - t
+            scale = pol._dp_counts(self.N)[1] / pol._dp_counts(Ns)[1]
+            return 1.0 / (dtm * scale), (f"the reference DP loop on the N={Ns} plan ({dtm * 1e3:.1f} ms), scaled by "
+                                         f"the transition count to N={self.N} (x{scale:.1f})")
+        plan = O.build_plan(self.N, 4)
+        nb = min(self.B, 64)
+        dt = {0: O.F64, 1: O.C128, 4: O.I64}[self.code]
+        Psub = np.asfortranarray(self.P[:nb])
+        O.haf_dp_batch(Psub, plan, dt, nthreads)
+        t = time.perf_counter()
+        O.haf_dp_batch(Psub, plan, dt, nthreads)
+        return nb / (time.perf_counter() - t), f"{nb} instances through the reference's batch loop, all host threads"
+
+
+class RepeatedWorkload:
+    """B hafnian_repeated sieves per step (configuration 5)."""
+
+    kind = "sieve"
+
+    def __init__(self, egg, W, which: str, B: int, seed: int):
+        from theeggman_b200 import roofline as R
+        from theeggman_b200 import policy as pol
+
+        self.egg = egg
+        if which == "a":
+            mats, rpts = W.repeated_real(B, 14, seed)
+            self.cplx = False
+        else:
+            mats, rpts = W.repeated_complex(B, 20, 48, seed)
+            self.cplx = True
+        self.mats, self.rpts = mats, rpts
+        self.inst = []
+        flops = 0.0
+        for A, r in zip(mats, rpts):
+            x, er = pol.matched_reps(r)
+            xi = np.array(x) - 1
+            g = pol._choose_method(sum(r), er, 1)[1]
+            self.inst.append((np.ascontiguousarray(A[np.ix_(xi, xi)]), er, g))
+            flops += R.sieve_flops(er, g, self.cplx)
+        self.flops = flops
+        self.B = B
+        self.hafnians_per_step = B
+        self.dtype_name = "c128" if self.cplx else "f64"
+        self.name = (f"config5{which}: {B} x hafnian_repeated(B, rpt), "
+                     + ("14x14 Float64 U[-1,1], rpt=fill(2,14)" if which == "a" else
+                        "20x20 ComplexF64 N(0,1/40) parts, rpt iid U{1..4} trimmed to total <= 48 and even")
+                     + ", mixed-radix sieve, variant by the cost model")
+
+    def setup_device(self, torch, dev):
+        B = self.B
+        Emax = max(len(er) for _, er, _ in self.inst)
+        lda = max(2 * Emax, 1)
+        CT = np.complex128 if self.cplx else np.float64
+        slab = np.zeros((B, lda, lda), dtype=CT)
+        for b, (Ax, er, g) in enumerate(self.inst):
+            m = 2 * len(er)
+            slab[b, :m, :m] = Ax.T
+        self.Emax = Emax
+        self.dslab = torch.from_numpy(slab).to(dev)
+        self.E = np.array([len(er) for _, er, _ in self.inst], dtype=np.int64)
+        self.reps = np.zeros((B, max(Emax, 1)), dtype=np.int64)
+        for b, (_, er, _) in enumerate(self.inst):
+            self.reps[b, : len(er)] = er
+        self.g = np.array([1 if g else 0 for _, _, g in self.inst], dtype=np.int32)
+        self.dout = torch.zeros(2 * B, dtype=torch.float64, device=dev)
+        self.dE = self.E
+
+    def step_device(self, stream_ptr):
+        # The instance tables are host-side and tiny; the matrices stay resident.
+        L = self.egg.lib()
+        rc = L.egg_sieve_batch_device(1 if self.cplx else 0, 1, self.B, self.Emax, self.dslab.data_ptr(),
+                                      self.E.ctypes.data, self.reps.ctypes.data, self.g.ctypes.data,
+                                      self.dout.data_ptr(), stream_ptr)
+        if rc:
+            raise RuntimeError(L.egg_last_error().decode())
+
+    def step_e2e(self):
+        from theeggman_b200.hafnian import _sieve_device_batch
+
+        return _sieve_device_batch(np.dtype(np.complex128 if self.cplx else np.float64), [a for a, _, _ in self.inst],
+                                   [er for _, er, _ in self.inst], [g for _, _, g in self.inst], "fma")
+
+    launches_per_step = 6
+
+    @property
+    def h2d_bytes(self):
+        return int(self.dslab.numel() * self.dslab.element_size()) if hasattr(self, "dslab") else 0
+
+    @property
+    def d2h_bytes(self):
+        return self.B * (16 if self.cplx else 8)
+
+    roofline = SieveWorkload.roofline
+
+    def cpu_sample(self, nthreads):
+        from oracle import oracle as O
+
+        nb = min(self.B, 64)
+        t = time.perf_counter()
+        for Ax, er, g in self.inst[:nb]:
+            O.calc_hafnian(Ax, er, g, nthreads=nthreads)
+        return nb / (time.perf_counter() - t), f"{nb} instances, each with the reference's sieve threading"
 
 
 def make_workload(name: str, egg, W, rank: int):
@@ -138,6 +348,24 @@ def make_workload(name: str, egg, W, rank: int):
         return SieveWorkload(egg, W, 40, True, None, 2025 + rank)
     if name == "sieve40g":
         return SieveWorkload(egg, W, 40, False, True, 2024 + rank)
+    if name == "dp20":
+        return DPWorkload(egg, W, 20, 1, "f64", "exact", 2020 + rank)
+    if name == "dp32":
+        return DPWorkload(egg, W, 32, 1, "f64", "exact", 3232 + rank)
+    if name == "dp36":
+        return DPWorkload(egg, W, 36, 1, "f64", "exact", 3636 + rank)
+    if name == "dp40":
+        return DPWorkload(egg, W, 40, 1, "f64", "exact", 4040 + rank)
+    if name == "dp40mixed":
+        return DPWorkload(egg, W, 40, 1, "f64", "mixed", 4040 + rank)
+    if name == "dp40int":
+        return DPWorkload(egg, W, 40, 1, "i64", "exact", 4041 + rank)
+    if name == "dp20x1024":
+        return DPWorkload(egg, W, 20, 1024, "c128", "exact", 7000 + rank)
+    if name == "rep14":
+        return RepeatedWorkload(egg, W, "a", 1024, 5 + 100 * rank)
+    if name == "rep20c":
+        return RepeatedWorkload(egg, W, "b", 1024, 6 + 100 * rank)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -200,8 +428,8 @@ def dist_env():
 
 def run_reference(args):
     """The reference's algorithm on this host's CPU cores: the oracle's restatement of
-    src/hafnian.jl's sieve with its own threading policy (Julia is not installed, so the Julia
-    package itself cannot run; the oracle is the closest executable form of it)."""
+    src/dp.jl / src/hafnian.jl with the reference's threading policy.  Julia is not installed, so
+    the Julia package itself cannot run; the oracle is the closest executable form of it."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
@@ -214,17 +442,20 @@ def run_reference(args):
     wl = make_workload(args.workload, egg, W, 0)
     cores = O.max_threads()
     for _ in range(args.warmup):
-        wl.cpu_time(cores)
-    times = [wl.cpu_time(cores) for _ in range(args.steps)]
-    total = sum(times)
-    value = args.steps / total
+        wl.cpu_sample(cores)
+    rates = []
+    sample = ""
+    for _ in range(args.steps):
+        r, sample = wl.cpu_sample(cores)
+        rates.append(r)
+    value = statistics.median(rates)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "hafnians/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wl.name, "host": "CPU"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wl.hafnians_per_step / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype_name,
+        "data": "synthetic (seeded SplitMix64)", "config": {"workload": wl.name, "host": "CPU"},
         "cpu_baseline": {"value": value, "unit": "hafnians/s", "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} full hafnians (every sieve term), all host threads"},
+                         "sample": f"median of {args.steps} samples: {sample}"},
         "e2e": {"value": value, "unit": "hafnians/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -291,7 +522,7 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
-    value = world * args.steps / (ms_max / 1e3)
+    value = world * args.steps * wl.hafnians_per_step / (ms_max / 1e3)
 
     # End to end through the public API, host arrays in and out.
     for _ in range(max(1, args.warmup // 2)):
@@ -305,7 +536,7 @@ def run_ours(args):
     te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps / float(te.item())
+    e2e_value = world * args.steps * wl.hafnians_per_step / float(te.item())
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -313,32 +544,22 @@ def run_ours(args):
 
         O.build()
         cores = O.max_threads()
-        wl.cpu_time(cores)  # warm the thread pool
-        ct = wl.cpu_time(cores)
-        cpu = {"value": 1.0 / ct, "unit": "hafnians/s", "cores": cores, "kind": "port",
-               "sample": "one full hafnian of the same workload (every sieve term), all host threads"}
+        rate, sample = wl.cpu_sample(cores)
+        cpu = {"value": rate, "unit": "hafnians/s", "cores": cores, "kind": "port", "sample": sample}
 
     peaks = measured_peaks()
-    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
-    from theeggman_b200 import roofline as R
-
-    peak = R.fp64_nominal_tflops(sm_max)
-    achieved = wl.flops / (ms_max / args.steps / 1e3) / 1e12
-    traffic = profile_traffic(f"{wl.kernel}_{args.workload}.txt")
+    roof = wl.roofline(ms_max / args.steps, peaks)
+    roof["traffic"] = profile_traffic(f"{wl.kind}_{args.workload}.txt")
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "hafnians/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64)",
+            "vs_baseline": None, "dtype": wl.dtype_name, "data": "synthetic (seeded SplitMix64)",
             "config": {"workload": wl.name, "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "e2e": {"value": e2e_value, "unit": "hafnians/s", "h2d_bytes_per_step": wl.h2d_bytes,
-                    "d2h_bytes_per_step": wl.d2h_bytes, "path": "hafnian(A; method=:sieve) from host memory"},
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": f"nominal FP64: 148 SMs x 64 FMA/clk x 2 x {sm_max:.0f} MHz (no FP64 figure "
-                                        "in MEASURED_PEAKS.json)",
-                         "work": f"{wl.flops:.4e} algorithmic flops per hafnian"},
+                    "d2h_bytes_per_step": wl.d2h_bytes, "path": "the public API from host memory"},
+            "roofline": roof,
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": wl.launches_per_step * args.steps,
         }
         print(json.dumps(line))

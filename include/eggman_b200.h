@@ -162,6 +162,11 @@ int egg_sieve_device_noalloc(int dtype, int prec, const void *Ax, int64_t E, con
 int egg_sieve_batch(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax, const int64_t *E,
                     const int64_t *edge_reps, const int32_t *glynn, void *out);
 
+/* Same, with the matrix slab Ax and out in device memory (E, edge_reps, glynn on the host),
+ * enqueued on `stream`. */
+int egg_sieve_batch_device(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax, const int64_t *E,
+                           const int64_t *edge_reps, const int32_t *glynn, void *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -431,4 +431,18 @@ int egg_sieve_batch(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax
     return EGG_OK;
 }
 
+int egg_sieve_batch_device(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax, const int64_t *E,
+                           const int64_t *edge_reps, const int32_t *glynn, void *out, void *stream)
+{
+    EGG_GUARD();
+    if (dtype != EGG_F64 && dtype != EGG_C128) return fail(EGG_ERR_ARGUMENT, "the sieve runs in Float64 or ComplexF64");
+    if (B < 0 || Emax < 0 || Emax > 32) return fail(EGG_ERR_ARGUMENT, "bad batch shape");
+    if (B == 0) return EGG_OK;
+    if (!Ax || !E || !edge_reps || !glynn || !out) return fail(EGG_ERR_ARGUMENT, "null argument");
+    for (int64_t b = 0; b < B; ++b)
+        if (E[b] < 0 || E[b] > Emax) return fail(EGG_ERR_DIMENSION, "instance edge count exceeds Emax");
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+    return sieve_batch_run(dtype, prec, B, Emax, Ax, E, edge_reps, glynn, out, st);
+}
+
 }  // extern "C"

@@ -422,8 +422,8 @@ __global__ void __launch_bounds__(256) sieve_exact_kernel(SieveArgs a, int warps
 // Sums each instance's per-warp partials (one array per kernel that evaluated some of its terms) in a fixed tree, applies the Glynn rescaling 2^-(n-1) (:737) and writes the result.
 // One block of 256 threads per instance.
 struct PartialSet {
-    const dd *p[6];  // exact kernel, then up to five register-tile size classes
-    int w[6];
+    const dd *p[7];  // exact kernel, then up to six register-tile size classes
+    int w[7];
 };
 
 template <bool CPLX>
@@ -432,7 +432,7 @@ __global__ void sieve_reduce_kernel(PartialSet ps, const SieveInst *inst, void *
     __shared__ dd sre[256], sim[256];
     const int b = blockIdx.x, t = threadIdx.x;
     dd r{0.0, 0.0}, i{0.0, 0.0};
-    for (int a = 0; a < 6; ++a) {
+    for (int a = 0; a < 7; ++a) {
         if (!ps.p[a]) continue;
         const dd *p = ps.p[a] + (size_t)b * ps.w[a] * 2;
         for (int w = t; w < ps.w[a]; w += 256) {
@@ -553,17 +553,19 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
 
     // Which kernels run: in FMA mode, each register-tile size class that some instance's terms can
     // fall in; the exact kernel takes everything in exact mode, else whatever exceeds the tiles.
+    // The register tiles handle orders n <= 31 (one lane per coefficient).
+    const bool fast_ok = prec == EGG_PREC_FMA && nmax <= 31;
     const int fast_hi = cplx ? 32 : 48;
     const int nclass = cplx ? kFastClassesCplx : kFastClassesReal;
-    bool run_cls[kFastClassesReal] = {false, false, false, false, false};
+    bool run_cls[kFastClassesReal] = {false, false, false, false, false, false};
     int ncls_run = 0;
-    if (prec == EGG_PREC_FMA)
+    if (fast_ok)
         for (int k = 0; k < nclass; ++k) {
             run_cls[k] = mmax_all > kFastClasses[k][0] && mmin_all <= kFastClasses[k][1] && mmax_all > 0;
             ncls_run += run_cls[k];
         }
-    const bool run_ex = prec == EGG_PREC_EXACT || mmax_all > fast_hi || mmax_all == 0;
-    const int skip_le = prec == EGG_PREC_EXACT ? 0 : fast_hi;
+    const bool run_ex = !fast_ok || mmax_all > fast_hi || mmax_all == 0;
+    const int skip_le = fast_ok ? fast_hi : 0;
 
     // Launch shapes.
     auto per_inst_blocks = [&](int wpb) {
@@ -579,7 +581,9 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     if (run_ex && ex_wpb < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
     const int ex_bx = run_ex ? per_inst_blocks(ex_wpb) : 0;
     const int fwpb = 8;
-    if (fast_smem_bytes(nmax, cplx, fwpb) > 220 * 1024) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
+    for (int k = 0; k < nclass; ++k)
+        if (run_cls[k] && fast_smem_bytes(nmax, cplx, k, fwpb) > 220 * 1024)
+            return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
     const int f_bx = ncls_run ? per_inst_blocks(fwpb) : 0;
 
     // Device staging: instance table, reps, strides, binoms, partials -- one scratch allocation.
@@ -619,7 +623,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.nmax = nmax;
     a.skip_le = skip_le;
     PartialSet ps;
-    for (int k = 0; k < 6; ++k) {
+    for (int k = 0; k < 7; ++k) {
         ps.p[k] = nullptr;
         ps.w[k] = 0;
     }

@@ -23,11 +23,11 @@ struct SieveArgs {
 };
 
 // Fast path (egg_sieve_fast.cu): size class `cls` covers terms with kFastClasses[cls][0] < m <=
-// kFastClasses[cls][1]; classes 0-2 exist for real and complex terms, 3-4 (two rows per lane) for
+// kFastClasses[cls][1]; classes 0-3 exist for real and complex terms, 4-5 (two rows per lane) for
 // real terms only.
 extern const int kFastClasses[][2];
-constexpr int kFastClassesReal = 5, kFastClassesCplx = 3;
-size_t fast_smem_bytes(int nmax, int cplx, int warps);
+constexpr int kFastClassesReal = 6, kFastClassesCplx = 4;
+size_t fast_smem_bytes(int nmax, int cplx, int cls, int warps);
 int launch_fast(const SieveArgs &a, const int64_t *strides, int B, int cplx, int cls, dd *partial, int wpb,
                 int blocks_x, cudaStream_t st);
 

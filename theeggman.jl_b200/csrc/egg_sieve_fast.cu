@@ -10,9 +10,8 @@
 //     (a similarity, so both) swaps two labels.  Physical column j always carries the label of
 //     physical row j, so a lane knows every column's label from the rows' labels.
 //   * The pivot search is one redux.sync.max over a 32-bit key: the high 24 bits of |pivot|'s
-//     magnitude (sign-free double bits) above 7 bits of (127 - label), so ties go to the smallest
-//     logical index as in the reference.  Entries within 2^-13 of each other may pick either; any
-//     near-maximal pivot keeps the multipliers bounded by ~1.
+//     magnitude (sign-free double bits) above the candidate's physical slot.  Entries within 2^-13
+//     of each other may pick either; any near-maximal pivot keeps the multipliers bounded by ~1.
 //   * The current pivot column (logical s-1) is kept in a scalar per row, `pc`.  The row update
 //     M[i, :] -= mult_i * M[piv, :] runs over all slots with mult_i = 0 for rows that are not below
 //     the pivot (so they are left bit-for-bit unchanged); slots of finished columns hold values that
@@ -21,18 +20,23 @@
 //     vector that is mult_i on the live rows' slots and exactly 1 on the pivot slot, which yields
 //     the updated column s directly -- the next step's `pc` -- with no dynamic register index.
 //
-// Each finished Hessenberg column feeds La Budde's recurrence (src/hafnian.jl:454-492) at once,
-// so only the last n+1 rows of the coefficient table are kept (a ring in shared memory), and the
-// [lambda^n] series coefficient (src/hafnian.jl:502-514) is a warp reduction per order.  All
-// arithmetic is FP64 with fused multiply-adds; terms are accumulated in double-double per warp.
+// Each finished Hessenberg column feeds La Budde's recurrence (src/hafnian.jl:454-492) at once:
+// lanes own coefficient orders t and walk the coefficient table (shared memory, one row per order
+// of leading minor) along a diagonal, one address step per term of the depth sum.  The [lambda^n] series coefficient
+// (src/hafnian.jl:502-514) is accumulated push-style: once f_s is known every lane t > s adds its
+// (t+s) q_{t-s} f_s, so each order costs one multiply-add per lane and one broadcast.  All arithmetic
+// is FP64 with fused multiply-adds; terms are accumulated in double-double per warp.
 //
-// Terms whose size exceeds the register tile (complex m > 32) are left to the exact kernel, which
-// sums them into separate partials.
+// Terms whose size exceeds the register tiles (complex m > 32, real m > 48) or whose order n
+// exceeds 31 are left to the exact kernel, which sums them into separate partials.
 #include "egg_sieve.cuh"
 
 namespace egg {
 
 static constexpr unsigned FULL = 0xffffffffu;
+
+// -1 / (2t) for t = 0..63, rounded on the host (entry 0 unused).
+__constant__ double c_neg_inv_2t[64];
 
 // 1/x by Newton-Raphson iteration from the single-precision reciprocal: each step
 // y <- y + y(1 - xy) doubles the number of correct bits (24 -> 48 -> full).  Outside the range
@@ -49,42 +53,33 @@ __device__ __forceinline__ double recip(double x)
     return fma(y, e, y);
 }
 
-__device__ __forceinline__ unsigned pivot_key(double a, int lab)
+// Candidate key: magnitude bits above bit 7, then a set bit 6 (so every candidate beats the
+// non-candidates' 0), then 63 - slot (ties go to the lowest slot).  a >= 0; NaN never wins.
+__device__ __forceinline__ unsigned pivot_key(double a, int slot)
 {
-    // a >= 0 (a magnitude); NaN never wins
     unsigned hi = (unsigned)__double2hiint(a);
     if (a != a) hi = 0;
-    return (hi & ~127u) | (unsigned)(127 - lab);
+    return (hi & ~127u) | 64u | (unsigned)(63 - slot);
 }
 
 // Per-warp shared scratch of the fast path.
 struct FastWs {
     double *prow;  // pivot row, by physical slot [64]
     double *wv;    // column-update weights, by physical slot [64]
-    double *cf;    // La Budde coefficients coef_i, by i [64]
-    double *C;     // ring of n+1 coefficient rows, (n+1) x (n+1)
-    double *f;     // series coefficients [n+1]
+    double *cf;    // La Budde coefficients coef_i, by i [64] (complex: 32 values)
+    double *C;     // coefficient table, rows 0..mhi, row stride nmax+1
+    double *kval;  // multiplicities of the surviving edges after the Glynn substitution [32]
     int *eidx;     // surviving edges, compacted [32]
-    double *kval;  // their multiplicities after the Glynn substitution [32]
 };
 
-// Rows of the La Budde table live in a ring of RR = 2^p >= n+1 rows (row r in slot r & (RR-1)):
-// row k reads rows k-1 .. k-n only.
-__host__ __device__ inline int ring_rows(int nmax)
-{
-    int rr = 1;
-    while (rr < nmax + 1) rr <<= 1;
-    return rr;
-}
-
-__host__ __device__ inline size_t fast_ws_doubles(int nmax, int cplx)
+__host__ __device__ inline size_t fast_ws_doubles(int nmax, int cplx, int mhi)
 {
     const size_t v = cplx ? 2 : 1;  // doubles per value
-    size_t d = 64 * 3 + v * (size_t)ring_rows(nmax) * (nmax + 1) + v * (nmax + 1) + 32 /*kval*/ + 16 /*eidx*/;
+    size_t d = 64 * 3 + v * (size_t)(mhi + 1) * (nmax + 1) + 32 /*kval*/ + 16 /*eidx*/;
     return (d + 1) & ~(size_t)1;  // keep every warp's region 16-byte aligned
 }
 
-__device__ inline FastWs fast_carve(double *base, int nmax, int cplx)
+__device__ inline FastWs fast_carve(double *base, int nmax, int cplx, int mhi)
 {
     const size_t v = cplx ? 2 : 1;
     FastWs w;
@@ -92,143 +87,126 @@ __device__ inline FastWs fast_carve(double *base, int nmax, int cplx)
     w.prow = p; p += 64;
     w.wv = p; p += 64;
     w.cf = p; p += 64;
-    w.C = p; p += v * (size_t)ring_rows(nmax) * (nmax + 1);
-    w.f = p; p += v * (nmax + 1);
+    w.C = p; p += v * (size_t)(mhi + 1) * (nmax + 1);
     w.kval = p; p += 32;
     w.eidx = (int *)p;
     return w;
 }
 
-// ---- La Budde step k (1-based), lanes over t --------------------------------------------------------
-//   C[k][t] = (t <= min(k-1,n) ? C[k-1][t] : 0) - hkk C[k-1][t-1] - sum_{i=ilo}^{k-1} cf[i] C[i-1][t-k+i-1]
-// Row r of C lives in ring slot (r & rm) with row stride cs = n+1.
-__device__ __forceinline__ void labudde_row(double *C, const double *cf, int k, int n, int rm, double hkk, int lane)
+// ---- La Budde row k (1-based); lane t (0..n) owns coefficient t ----------------------------------
+//   C[k][t] = (t <= min(k-1,n) ? C[k-1][t] : 0) - hkk C[k-1][t-1] - sum_{j=1}^{jmax} cf[k-j] C[k-1-j][t-1-j]
+// (j = k - i of the reference's i loop, which runs i = k-1 .. max(1, k-n+1)).  Entries of a row
+// beyond its degree are zero, so lanes past min(k, n) need no special case in the depth sum.  Row r
+// of the table is at r * cs; the depth-j entry this lane reads is one row and one column before the
+// depth-(j-1) one, so its offset steps by -(cs+1).
+__device__ __forceinline__ void labudde_row(double *C, const double *cf, int k, int n, int cs, double hkk, int lane)
 {
-    const int cs = n + 1;
-    const double *Cp = C + (size_t)((k - 1) & rm) * cs;
-    double *Ck = C + (size_t)(k & rm) * cs;
+    const int t = lane;
+    const bool act = t <= n;
+    const double *Cp = C + (size_t)(k - 1) * cs;
     const int tmax = k < n ? k : n, prevmax = (k - 1) < n ? (k - 1) : n;
-    const int ilo = 1 > k - n + 1 ? 1 : k - n + 1;
-    for (int t = lane; t <= n; t += 32) {
-        double v;
+    double v = 0.0;
+    if (act) {
         if (t == 0) v = Cp[0];
         else if (t <= tmax) v = (t <= prevmax ? Cp[t] : 0.0) - hkk * Cp[t - 1];
-        else v = 0.0;
-        if (t >= 1 && t <= tmax) {
-            // term i reads row i-1 at column u = t-k+i-1; as i steps down by one, so do both
-            const int i0 = ilo > k - t + 1 ? ilo : k - t + 1;
-            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-            int i = k - 1;
-            for (; i - 3 >= i0; i -= 4) {
-                const int u = t - k + i - 1;
-                a0 = fma(cf[i], C[(size_t)((i - 1) & rm) * cs + u], a0);
-                a1 = fma(cf[i - 1], C[(size_t)((i - 2) & rm) * cs + u - 1], a1);
-                a2 = fma(cf[i - 2], C[(size_t)((i - 3) & rm) * cs + u - 2], a2);
-                a3 = fma(cf[i - 3], C[(size_t)((i - 4) & rm) * cs + u - 3], a3);
-            }
-            for (; i >= i0; --i) a0 = fma(cf[i], C[(size_t)((i - 1) & rm) * cs + (t - k + i - 1)], a0);
-            v -= (a0 + a1) + (a2 + a3);
-        }
-        Ck[t] = v;
     }
+    const int jmax = (k - 1) < (n - 1) ? (k - 1) : (n - 1);
+    const double *cfk = cf + k;
+    int off = (k - 2) * cs + (t - 2);  // row k-1-j, column t-1-j at j = 1
+    const int step = cs + 1;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+    for (int j = 1; j <= 31; ++j) {
+        if (j > jmax) break;
+        const double c = cfk[-j];
+        const double x = (act && t > j) ? C[off] : 0.0;
+        off -= step;
+        if ((j & 3) == 1) a0 = fma(c, x, a0);
+        else if ((j & 3) == 2) a1 = fma(c, x, a1);
+        else if ((j & 3) == 3) a2 = fma(c, x, a2);
+        else a3 = fma(c, x, a3);
+    }
+    if (act) C[(size_t)k * cs + t] = v - ((a0 + a1) + (a2 + a3));
 }
 
-// [lambda^n] det(I - lambda H)^(-1/2) from q_j = C[m][j]; warp-parallel over j for each order t.
-__device__ double series_coeff(const double *C, int m, int n, int rm, double *f, int lane)
+// [lambda^n] det(I - lambda H)^(-1/2), push-style: lane t accumulates S_t = sum_j (2t-j) q_j f_{t-j}
+// as the f's become known; f_t = -S_t / (2t).  q_j = C[m][j].  All lanes return f_n.
+__device__ __forceinline__ double series_coeff(const double *C, int m, int n, int cs, int lane)
 {
-    const int cs = n + 1;
-    const double *q = C + (size_t)(m & rm) * cs;
-    if (lane == 0) f[0] = 1.0;
-    __syncwarp();
-    double ft = 1.0;
-    for (int t = 1; t <= n; ++t) {
-        const int jm = t < m ? t : m;
-        double s = 0.0;
-        for (int j = 1 + lane; j <= jm; j += 32) s = fma((double)(2 * t - j) * q[j], f[t - j], s);
-        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(FULL, s, off);
-        ft = -s / (double)(2 * t);
-        if (lane == 0) f[t] = ft;
-        __syncwarp();
+    const double *q = C + (size_t)m * cs;
+    double S = 0.0, fs = 1.0;  // fs = f_s, starting at f_0 = 1
+    for (int s = 0; s < n; ++s) {
+        const int j = lane - s;
+        if (j >= 1 && j <= m && lane <= n) S = fma((double)(lane + s) * q[j], fs, S);
+        fs = __shfl_sync(FULL, S, s + 1) * c_neg_inv_2t[s + 1];
     }
-    return ft;
+    return fs;
 }
 
-// Complex versions (values interleaved as cd in the same ring layout).
-__device__ __forceinline__ void labudde_row_c(cd *C, const cd *cf, int k, int n, int rm, cd hkk, int lane)
+__device__ __forceinline__ void labudde_row_c(cd *C, const cd *cf, int k, int n, int cs, cd hkk, int lane)
 {
-    const int cs = n + 1;
-    const cd *Cp = C + (size_t)((k - 1) & rm) * cs;
-    cd *Ck = C + (size_t)(k & rm) * cs;
+    const int t = lane;
+    const bool act = t <= n;
+    const cd *Cp = C + (size_t)(k - 1) * cs;
     const int tmax = k < n ? k : n, prevmax = (k - 1) < n ? (k - 1) : n;
-    const int ilo = 1 > k - n + 1 ? 1 : k - n + 1;
-    for (int t = lane; t <= n; t += 32) {
-        cd v;
+    cd v{0.0, 0.0};
+    if (act) {
         if (t == 0) v = Cp[0];
         else if (t <= tmax) {
-            cd a = t <= prevmax ? Cp[t] : cd{0.0, 0.0};
-            cd b = Cp[t - 1];
-            v.re = a.re - (hkk.re * b.re - hkk.im * b.im);
-            v.im = a.im - (hkk.re * b.im + hkk.im * b.re);
-        } else v = cd{0.0, 0.0};
-        if (t >= 1 && t <= tmax) {
-            int i0 = ilo > k - t + 1 ? ilo : k - t + 1;
-            double sr = 0.0, si = 0.0, tr = 0.0, ti = 0.0;
-            int i = k - 1;
-            for (; i - 1 >= i0; i -= 2) {
-                const int u = t - k + i - 1;
-                const cd c = cf[i], x = C[(size_t)((i - 1) & rm) * cs + u];
-                const cd c2 = cf[i - 1], x2 = C[(size_t)((i - 2) & rm) * cs + u - 1];
-                sr = fma(c.re, x.re, fma(-c.im, x.im, sr));
-                si = fma(c.re, x.im, fma(c.im, x.re, si));
-                tr = fma(c2.re, x2.re, fma(-c2.im, x2.im, tr));
-                ti = fma(c2.re, x2.im, fma(c2.im, x2.re, ti));
-            }
-            if (i >= i0) {
-                const cd c = cf[i], x = C[(size_t)((i - 1) & rm) * cs + (t - k + i - 1)];
-                sr = fma(c.re, x.re, fma(-c.im, x.im, sr));
-                si = fma(c.re, x.im, fma(c.im, x.re, si));
-            }
-            v.re -= sr + tr;
-            v.im -= si + ti;
+            const cd a = t <= prevmax ? Cp[t] : cd{0.0, 0.0};
+            const cd b = Cp[t - 1];
+            v.re = a.re - fma(hkk.re, b.re, -hkk.im * b.im);
+            v.im = a.im - fma(hkk.re, b.im, hkk.im * b.re);
         }
-        Ck[t] = v;
     }
+    const int jmax = (k - 1) < (n - 1) ? (k - 1) : (n - 1);
+    const cd *cfk = cf + k;
+    int off = (k - 2) * cs + (t - 2);
+    const int step = cs + 1;
+    double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
+#pragma unroll
+    for (int j = 1; j <= 31; ++j) {
+        if (j > jmax) break;
+        const cd c = cfk[-j];
+        const cd x = (act && t > j) ? C[off] : cd{0.0, 0.0};
+        off -= step;
+        if (j & 1) {
+            sr0 = fma(c.re, x.re, fma(-c.im, x.im, sr0));
+            si0 = fma(c.re, x.im, fma(c.im, x.re, si0));
+        } else {
+            sr1 = fma(c.re, x.re, fma(-c.im, x.im, sr1));
+            si1 = fma(c.re, x.im, fma(c.im, x.re, si1));
+        }
+    }
+    if (act) C[(size_t)k * cs + t] = cd{v.re - (sr0 + sr1), v.im - (si0 + si1)};
 }
 
-__device__ cd series_coeff_c(const cd *C, int m, int n, int rm, cd *f, int lane)
+__device__ __forceinline__ cd series_coeff_c(const cd *C, int m, int n, int cs, int lane)
 {
-    const int cs = n + 1;
-    const cd *q = C + (size_t)(m & rm) * cs;
-    if (lane == 0) f[0] = cd{1.0, 0.0};
-    __syncwarp();
-    cd ft{1.0, 0.0};
-    for (int t = 1; t <= n; ++t) {
-        const int jm = t < m ? t : m;
-        double sr = 0.0, si = 0.0;
-        for (int j = 1 + lane; j <= jm; j += 32) {
-            const double w = (double)(2 * t - j);
-            const cd a{w * q[j].re, w * q[j].im}, b = f[t - j];
-            sr = fma(a.re, b.re, fma(-a.im, b.im, sr));
-            si = fma(a.re, b.im, fma(a.im, b.re, si));
+    const cd *q = C + (size_t)m * cs;
+    double Sr = 0.0, Si = 0.0, fr = 1.0, fi = 0.0;
+    for (int s = 0; s < n; ++s) {
+        const int j = lane - s;
+        if (j >= 1 && j <= m && lane <= n) {
+            const double w = (double)(lane + s);
+            const double ar = w * q[j].re, ai = w * q[j].im;
+            Sr = fma(ar, fr, fma(-ai, fi, Sr));
+            Si = fma(ar, fi, fma(ai, fr, Si));
         }
-        for (int off = 16; off > 0; off >>= 1) {
-            sr += __shfl_xor_sync(FULL, sr, off);
-            si += __shfl_xor_sync(FULL, si, off);
-        }
-        const double d2 = 1.0 / (double)(2 * t);
-        ft = cd{-sr * d2, -si * d2};
-        if (lane == 0) f[t] = ft;
-        __syncwarp();
+        const double c = c_neg_inv_2t[s + 1];
+        fr = __shfl_sync(FULL, Sr, s + 1) * c;
+        fi = __shfl_sync(FULL, Si, s + 1) * c;
     }
-    return ft;
+    return cd{fr, fi};
 }
 
 // ---- one real term, m <= 32 * RPL, register tile of MW columns ----------------------------------
 template <int MW, int RPL>
-__device__ __noinline__ double term_real(const double *__restrict__ Axs, int lda, int E, int mE, int n, int rm,
-                                         FastWs &w, int lane)
+__device__ __forceinline__ double term_real(const double *__restrict__ Ax, int lda, int E, int mE, int n, int cs,
+                                            const FastWs &ws, int lane)
 {
     const int m = 2 * mE;
+    double *prow = ws.prow, *wv = ws.wv, *cf = ws.cf, *C = ws.C;
     double R[RPL][MW];
     int lab[RPL];
     double pc[RPL], bet[RPL];
@@ -238,71 +216,58 @@ __device__ __noinline__ double term_real(const double *__restrict__ Axs, int lda
         lab[q] = r;
         bet[q] = 0.0;
         const bool live = r < m;
-        const int ra = live ? (r < mE ? w.eidx[r] : w.eidx[r - mE] + E) : 0;
+        const int ra = live ? (r < mE ? ws.eidx[r] : ws.eidx[r - mE] + E) : 0;
 #pragma unroll
         for (int j = 0; j < MW; ++j) {
             double v = 0.0;
             if (live && j < m) {
                 const int b = j < mE ? j : j - mE;
-                const int col = w.eidx[b] + (j < mE ? E : 0);
-                v = w.kval[b] * __ldg(Axs + (size_t)col * lda + ra);
+                const int col = ws.eidx[b] + (j < mE ? E : 0);
+                v = ws.kval[b] * __ldg(Ax + (size_t)col * lda + ra);
             }
             R[q][j] = v;
         }
         pc[q] = R[q][0];
     }
-    // La Budde row 0
-    for (int t = lane; t <= n; t += 32) w.C[t] = t == 0 ? 1.0 : 0.0;
-    double xprev = 0.0;  // subdiagonal entry of the previous step
+    if (lane <= n) C[lane] = lane == 0 ? 1.0 : 0.0;  // La Budde row 0
+    int hslot = 0;       // physical slot of label s-1 (label 0 never moves)
+    double xprev = 0.0;  // subdiagonal entry h_{s,s-1} of the previous step
     for (int s = 1; s <= m - 2; ++s) {
         // -- pivot among rows with s <= label < m
         unsigned key = 0;
 #pragma unroll
         for (int q = 0; q < RPL; ++q)
             if (lab[q] >= s && lab[q] < m) {
-                unsigned k2 = pivot_key(fabs(pc[q]), lab[q]);
+                const unsigned k2 = pivot_key(fabs(pc[q]), lane + 32 * q);
                 key = k2 > key ? k2 : key;
             }
         const unsigned best = __reduce_max_sync(FULL, key);
-        const int plab = 127 - (int)(best & 127u);
-        int mine = -1;
+        const int pslot = 63 - (int)(best & 63u);
+        const int plane = pslot & 31, pq = pslot >> 5;
+        const double pcp = (RPL > 1 && pq == 1) ? pc[RPL - 1] : pc[0];
+        const int labp = (RPL > 1 && pq == 1) ? lab[RPL - 1] : lab[0];
+        const double x = __shfl_sync(FULL, pcp, plane);
+        const int plab = __shfl_sync(FULL, labp, plane);
+        // -- column s-1 is final for rows with label <= s-1 plus the pivot; feed La Budde step k = s
+        {
+            const double hcand = (RPL > 1 && (hslot >> 5) == 1) ? pc[RPL - 1] : pc[0];
+            const double hkk = __shfl_sync(FULL, hcand, hslot & 31);
 #pragma unroll
-        for (int q = 0; q < RPL; ++q)
-            if (lab[q] == plab) mine = q;
-        const unsigned own = __ballot_sync(FULL, mine >= 0);
-        const int plane = __ffs(own) - 1;
-        const int pq = __shfl_sync(FULL, mine, plane);
-        const int pslot = plane + 32 * pq;
-        const double x = __shfl_sync(FULL, (RPL > 1 && mine == RPL - 1) ? pc[RPL - 1] : pc[0], plane);
+            for (int q = 0; q < RPL; ++q) {
+                if (lab[q] <= s - 3) bet[q] *= xprev;
+                else if (lab[q] == s - 2) bet[q] = xprev;
+                if (lab[q] <= s - 2) cf[lab[q] + 1] = pc[q] * bet[q];
+            }
+            __syncwarp();
+            labudde_row(C, cf, s, n, cs, hkk, lane);
+        }
         // -- relabel (similarity swap of logical s and plab)
 #pragma unroll
         for (int q = 0; q < RPL; ++q) {
             if (lab[q] == s) lab[q] = plab;
             else if (lab[q] == plab) lab[q] = s;
         }
-        // -- column s-1 is final for rows with label <= s: feed La Budde step k = s
-        {
-            // beta_{i,s} for i = lab+1: multiply by the subdiagonal h_{s,s-1} = xprev (s >= 2)
-#pragma unroll
-            for (int q = 0; q < RPL; ++q) {
-                if (lab[q] <= s - 3) bet[q] *= xprev;
-                else if (lab[q] == s - 2) bet[q] = xprev;
-                if (lab[q] <= s - 2) w.cf[lab[q] + 1] = pc[q] * bet[q];
-            }
-            double hkk = 0.0;
-#pragma unroll
-            for (int q = 0; q < RPL; ++q)
-                if (lab[q] == s - 1) hkk = pc[q];
-            const unsigned hown = __ballot_sync(FULL, [&] {
-                bool o = false;
-#pragma unroll
-                for (int q = 0; q < RPL; ++q) o |= lab[q] == s - 1;
-                return o;
-            }());
-            hkk = __shfl_sync(FULL, hkk, __ffs(hown) - 1);
-            __syncwarp();
-            labudde_row(w.C, w.cf, s, n, rm, hkk, lane);
-        }
+        hslot = pslot;
         xprev = x;
         if (x == 0.0) {
             // Nothing to eliminate (:231-232): the next pivot column is the physical slot of label s.
@@ -323,22 +288,24 @@ __device__ __noinline__ double term_real(const double *__restrict__ Axs, int lda
         for (int q = 0; q < RPL; ++q) mult[q] = (lab[q] > s && lab[q] < m) ? pc[q] * rx : 0.0;
         if (lane == plane) {
 #pragma unroll
-            for (int j = 0; j < MW; ++j) w.prow[j] = (RPL > 1 && pq == RPL - 1) ? R[RPL - 1][j] : R[0][j];
+            for (int j = 0; j < MW; j += 2)
+                *reinterpret_cast<double2 *>(prow + j) =
+                    (RPL > 1 && pq == 1) ? make_double2(R[RPL - 1][j], R[RPL - 1][j + 1]) : make_double2(R[0][j], R[0][j + 1]);
         }
 #pragma unroll
         for (int q = 0; q < RPL; ++q) {
             const int r = lane + 32 * q;
-            if (r < MW) w.wv[r] = r == pslot ? 1.0 : mult[q];
+            if (r < MW) wv[r] = r == pslot ? 1.0 : mult[q];
         }
         __syncwarp();
         // -- row update: M[i, :] -= mult_i * M[piv, :]
 #pragma unroll
         for (int j = 0; j < MW; j += 2) {
-            const double2 p2 = *reinterpret_cast<const double2 *>(w.prow + j);
+            const double2 p2 = *reinterpret_cast<const double2 *>(prow + j);
 #pragma unroll
             for (int q = 0; q < RPL; ++q) {
                 R[q][j] = fma(-mult[q], p2.x, R[q][j]);
-                if (j + 1 < MW) R[q][j + 1] = fma(-mult[q], p2.y, R[q][j + 1]);
+                R[q][j + 1] = fma(-mult[q], p2.y, R[q][j + 1]);
             }
         }
         // -- column update: pc <- M[:, piv] + sum_i mult_i M[:, i]
@@ -347,14 +314,12 @@ __device__ __noinline__ double term_real(const double *__restrict__ Axs, int lda
             double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
             for (int j = 0; j < MW; j += 4) {
-                const double2 w0 = *reinterpret_cast<const double2 *>(w.wv + j);
+                const double2 w0 = *reinterpret_cast<const double2 *>(wv + j);
+                const double2 w1 = *reinterpret_cast<const double2 *>(wv + j + 2);
                 a0 = fma(w0.x, R[q][j], a0);
-                if (j + 1 < MW) a1 = fma(w0.y, R[q][j + 1], a1);
-                if (j + 2 < MW) {
-                    const double2 w1 = *reinterpret_cast<const double2 *>(w.wv + j + 2);
-                    a2 = fma(w1.x, R[q][j + 2], a2);
-                    if (j + 3 < MW) a3 = fma(w1.y, R[q][j + 3], a3);
-                }
+                a1 = fma(w0.y, R[q][j + 1], a1);
+                a2 = fma(w1.x, R[q][j + 2], a2);
+                a3 = fma(w1.y, R[q][j + 3], a3);
             }
             pc[q] = (a0 + a1) + (a2 + a3);
         }
@@ -362,15 +327,13 @@ __device__ __noinline__ double term_real(const double *__restrict__ Axs, int lda
     }
     // Last two columns: m-2 is `pc`, m-1 is the physical slot carrying label m-1.  Feed La Budde
     // steps k = m-1 and k = m (for m == 2 the loop above did not run and k = 1, 2 remain).
-    int lastslot = 0;
+    int lastslot;
     {
         int mine = -1;
 #pragma unroll
         for (int q = 0; q < RPL; ++q)
-            if (lab[q] == m - 1) mine = q;
-        const unsigned own = __ballot_sync(FULL, mine >= 0);
-        const int ln = __ffs(own) - 1;
-        lastslot = ln + 32 * __shfl_sync(FULL, mine, ln);
+            if (lab[q] == m - 1) mine = lane + 32 * q;
+        lastslot = (int)__reduce_max_sync(FULL, (unsigned)(mine + 1)) - 1;
     }
     double colm1[RPL];
 #pragma unroll
@@ -382,25 +345,13 @@ __device__ __noinline__ double term_real(const double *__restrict__ Axs, int lda
         colm1[q] = v;
     }
     for (int k = (m >= 3 ? m - 1 : 1); k <= m; ++k) {
-        // column k-1 is `pc` for k = m-1 (or k = 1 when m == 2), `colm1` for k = m
-        const bool last = (k == m);
-        double sub = xprev;  // h_{k,k-1}
-        if (k >= 2) {
-            // h_{k,k-1} = H[k-1][k-2]: for k = m-1 that is the last pivot value; for k = m it is the
-            // entry of the row labelled m-1 in column m-2 (= pc of that row).
-            if (k == m) {
-                double v = 0.0;
-#pragma unroll
-                for (int q = 0; q < RPL; ++q)
-                    if (lab[q] == m - 1) v = pc[q];
-                const unsigned o = __ballot_sync(FULL, [&] {
-                    bool b = false;
-#pragma unroll
-                    for (int q = 0; q < RPL; ++q) b |= lab[q] == m - 1;
-                    return b;
-                }());
-                sub = __shfl_sync(FULL, v, __ffs(o) - 1);
-            }
+        const bool last = k == m;
+        // h_{k,k-1}: for k = m-1 the last pivot value; for k = m the entry of the row labelled m-1
+        // in column m-2, i.e. that row's pc.
+        double sub = xprev;
+        if (last && k >= 2) {
+            const double cand = (RPL > 1 && (lastslot >> 5) == 1) ? pc[RPL - 1] : pc[0];
+            sub = __shfl_sync(FULL, cand, lastslot & 31);
         }
         double hkk = 0.0;
 #pragma unroll
@@ -409,46 +360,40 @@ __device__ __noinline__ double term_real(const double *__restrict__ Axs, int lda
             if (k >= 2) {
                 if (lab[q] <= k - 3) bet[q] *= sub;
                 else if (lab[q] == k - 2) bet[q] = sub;
-                if (lab[q] <= k - 2) w.cf[lab[q] + 1] = colv * bet[q];
+                if (lab[q] <= k - 2) cf[lab[q] + 1] = colv * bet[q];
             }
             if (lab[q] == k - 1) hkk = colv;
         }
-        const unsigned hown = __ballot_sync(FULL, [&] {
-            bool o = false;
-#pragma unroll
-            for (int q = 0; q < RPL; ++q) o |= lab[q] == k - 1;
-            return o;
-        }());
-        hkk = __shfl_sync(FULL, hkk, __ffs(hown) - 1);
+        const int hs = last ? lastslot : hslot;
+        hkk = __shfl_sync(FULL, hkk, hs & 31);
         __syncwarp();
-        labudde_row(w.C, w.cf, k, n, rm, hkk, lane);
+        labudde_row(C, cf, k, n, cs, hkk, lane);
         __syncwarp();
     }
-    return series_coeff(w.C, m, n, rm, w.f, lane);
+    return series_coeff(C, m, n, cs, lane);
 }
 
 // ---- one complex term, m <= 32 --------------------------------------------------------------------
 template <int MW>
-__device__ __noinline__ cd term_cplx(const cd *__restrict__ Axs, int lda, int E, int mE, int n, int rm, FastWs &w,
-                                     int lane)
+__device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int E, int mE, int n, int cs,
+                                        const FastWs &ws, int lane)
 {
     const int m = 2 * mE;
     double Rr[MW], Ri[MW];
     int lab = lane;
     const bool live = lane < m;
     {
-        const int ra = live ? (lane < mE ? w.eidx[lane] : w.eidx[lane - mE] + E) : 0;
+        const int ra = live ? (lane < mE ? ws.eidx[lane] : ws.eidx[lane - mE] + E) : 0;
 #pragma unroll
         for (int j = 0; j < MW; ++j) {
             double vr = 0.0, vi = 0.0;
             if (live && j < m) {
                 const int b = j < mE ? j : j - mE;
-                const int col = w.eidx[b] + (j < mE ? E : 0);
-                const double2 z2 = __ldg(reinterpret_cast<const double2 *>(Axs + (size_t)col * lda + ra));
-                const cd z{z2.x, z2.y};
-                const double kb = w.kval[b];
-                vr = kb * z.re;
-                vi = kb * z.im;
+                const int col = ws.eidx[b] + (j < mE ? E : 0);
+                const double2 z = __ldg(reinterpret_cast<const double2 *>(Ax + (size_t)col * lda + ra));
+                const double kb = ws.kval[b];
+                vr = kb * z.x;
+                vi = kb * z.y;
             }
             Rr[j] = vr;
             Ri[j] = vi;
@@ -456,35 +401,34 @@ __device__ __noinline__ cd term_cplx(const cd *__restrict__ Axs, int lda, int E,
     }
     double pcr = Rr[0], pci = Ri[0];
     cd bet{0.0, 0.0};
-    cd *C = (cd *)w.C;
-    cd *cfc = (cd *)w.cf;  // complex coefficients need 2 doubles each: cf and prow regions are adjacent
-    double *prr = w.prow, *pri = w.prow + 32, *wvr = w.wv, *wvi = w.wv + 32;
-    for (int t = lane; t <= n; t += 32) C[t] = t == 0 ? cd{1.0, 0.0} : cd{0.0, 0.0};
+    cd *C = (cd *)ws.C;
+    cd *cfc = (cd *)ws.cf;  // 32 complex coefficients
+    double *prr = ws.prow, *pri = ws.prow + 32, *wvr = ws.wv, *wvi = ws.wv + 32;
+    if (lane <= n) C[lane] = lane == 0 ? cd{1.0, 0.0} : cd{0.0, 0.0};
+    int hslot = 0;
     cd xprev{0.0, 0.0};
-    auto feed = [&](int k, double colr, double coli, cd sub) {
+    auto feed = [&](int k, double colr, double coli, cd sub, int hs) {
         if (k >= 2) {
-            if (lab <= k - 3) bet = cd{bet.re * sub.re - bet.im * sub.im, bet.re * sub.im + bet.im * sub.re};
+            if (lab <= k - 3) bet = cd{fma(bet.re, sub.re, -bet.im * sub.im), fma(bet.re, sub.im, bet.im * sub.re)};
             else if (lab == k - 2) bet = sub;
-            if (lab <= k - 2) cfc[lab + 1] = cd{colr * bet.re - coli * bet.im, colr * bet.im + coli * bet.re};
+            if (lab <= k - 2) cfc[lab + 1] = cd{fma(colr, bet.re, -coli * bet.im), fma(colr, bet.im, coli * bet.re)};
         }
-        const unsigned hown = __ballot_sync(FULL, lab == k - 1);
-        const int hl = __ffs(hown) - 1;
-        cd hkk{__shfl_sync(FULL, colr, hl), __shfl_sync(FULL, coli, hl)};
+        const cd hkk{__shfl_sync(FULL, colr, hs), __shfl_sync(FULL, coli, hs)};
         __syncwarp();
-        labudde_row_c(C, cfc, k, n, rm, hkk, lane);
+        labudde_row_c(C, cfc, k, n, cs, hkk, lane);
         __syncwarp();
     };
     for (int s = 1; s <= m - 2; ++s) {
         unsigned key = 0;
-        if (lab >= s && lab < m) key = pivot_key(fma(pcr, pcr, pci * pci), lab);
+        if (lab >= s && lab < m) key = pivot_key(fma(pcr, pcr, pci * pci), lane);
         const unsigned best = __reduce_max_sync(FULL, key);
-        const int plab = 127 - (int)(best & 127u);
-        const unsigned own = __ballot_sync(FULL, lab == plab);
-        const int plane = __ffs(own) - 1;
+        const int plane = 63 - (int)(best & 63u);
         const double xr = __shfl_sync(FULL, pcr, plane), xi = __shfl_sync(FULL, pci, plane);
+        const int plab = __shfl_sync(FULL, lab, plane);
+        feed(s, pcr, pci, xprev, hslot);
         if (lab == s) lab = plab;
         else if (lab == plab) lab = s;
-        feed(s, pcr, pci, xprev);
+        hslot = plane;
         xprev = cd{xr, xi};
         const double d = fma(xr, xr, xi * xi);
         if (d == 0.0) {
@@ -507,9 +451,9 @@ __device__ __noinline__ cd term_cplx(const cd *__restrict__ Axs, int lda, int E,
         }
         if (lane == plane) {
 #pragma unroll
-            for (int j = 0; j < MW; ++j) {
-                prr[j] = Rr[j];
-                pri[j] = Ri[j];
+            for (int j = 0; j < MW; j += 2) {
+                *reinterpret_cast<double2 *>(prr + j) = make_double2(Rr[j], Rr[j + 1]);
+                *reinterpret_cast<double2 *>(pri + j) = make_double2(Ri[j], Ri[j + 1]);
             }
         }
         if (lane < MW) {
@@ -523,10 +467,8 @@ __device__ __noinline__ cd term_cplx(const cd *__restrict__ Axs, int lda, int E,
             const double2 ai = *reinterpret_cast<const double2 *>(pri + j);
             Rr[j] = fma(-mr, ar.x, fma(mi, ai.x, Rr[j]));
             Ri[j] = fma(-mr, ai.x, fma(-mi, ar.x, Ri[j]));
-            if (j + 1 < MW) {
-                Rr[j + 1] = fma(-mr, ar.y, fma(mi, ai.y, Rr[j + 1]));
-                Ri[j + 1] = fma(-mr, ai.y, fma(-mi, ar.y, Ri[j + 1]));
-            }
+            Rr[j + 1] = fma(-mr, ar.y, fma(mi, ai.y, Rr[j + 1]));
+            Ri[j + 1] = fma(-mr, ai.y, fma(-mi, ar.y, Ri[j + 1]));
         }
         double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
 #pragma unroll
@@ -535,17 +477,14 @@ __device__ __noinline__ cd term_cplx(const cd *__restrict__ Axs, int lda, int E,
             const double2 wi = *reinterpret_cast<const double2 *>(wvi + j);
             sr0 = fma(wr.x, Rr[j], fma(-wi.x, Ri[j], sr0));
             si0 = fma(wr.x, Ri[j], fma(wi.x, Rr[j], si0));
-            if (j + 1 < MW) {
-                sr1 = fma(wr.y, Rr[j + 1], fma(-wi.y, Ri[j + 1], sr1));
-                si1 = fma(wr.y, Ri[j + 1], fma(wi.y, Rr[j + 1], si1));
-            }
+            sr1 = fma(wr.y, Rr[j + 1], fma(-wi.y, Ri[j + 1], sr1));
+            si1 = fma(wr.y, Ri[j + 1], fma(wi.y, Rr[j + 1], si1));
         }
         pcr = sr0 + sr1;
         pci = si0 + si1;
         __syncwarp();
     }
-    const unsigned lown = __ballot_sync(FULL, lab == m - 1);
-    const int lastslot = __ffs(lown) - 1;
+    const int lastslot = (int)__reduce_max_sync(FULL, lab == m - 1 ? (unsigned)(lane + 1) : 0u) - 1;
     double cr = 0.0, ci = 0.0;
 #pragma unroll
     for (int j = 0; j < MW; ++j)
@@ -555,73 +494,29 @@ __device__ __noinline__ cd term_cplx(const cd *__restrict__ Axs, int lda, int E,
         }
     for (int k = (m >= 3 ? m - 1 : 1); k <= m; ++k) {
         cd sub = xprev;
-        if (k == m && k >= 2) {
-            const unsigned o = __ballot_sync(FULL, lab == m - 1);
-            const int l = __ffs(o) - 1;
-            sub = cd{__shfl_sync(FULL, pcr, l), __shfl_sync(FULL, pci, l)};
-        }
-        if (k == m) feed(k, cr, ci, sub);
-        else feed(k, pcr, pci, sub);
+        if (k == m && k >= 2) sub = cd{__shfl_sync(FULL, pcr, lastslot), __shfl_sync(FULL, pci, lastslot)};
+        if (k == m) feed(k, cr, ci, sub, lastslot);
+        else feed(k, pcr, pci, sub, hslot);
     }
-    return series_coeff_c(C, m, n, rm, (cd *)w.f, lane);
+    return series_coeff_c(C, m, n, cs, lane);
 }
 
-// ---- kernel ------------------------------------------------------------------------------------
+// ---- kernels -----------------------------------------------------------------------------------
 
-// Size classes: terms with MLO < m <= MHI (RPL rows per lane).  Each class is its own kernel with
-// its own register budget, so the small tiles run at high occupancy; every class walks all of the
-// instance's terms (the walk costs a few dozen instructions per term) and evaluates its own.
-template <bool CPLX, int RPL, int MLO, int MHI>
+// Size classes: terms with MLO < m <= MHI, each evaluated on one register tile of MHI columns
+// (two rows per lane above 32).  Each class is its own kernel with its own register budget, so the
+// small tiles run at high occupancy and each kernel holds one copy of the term code; every class
+// walks all of the instance's terms (a few dozen instructions per term) and evaluates its own.
+template <bool CPLX, int MHI>
 struct SizeClass {
     // Blocks of 256 threads kept resident per SM, i.e. the register budget per thread
-    // (65536 / (256 * min_blocks)): sized so each class's tiles fit without spilling in the
-    // elimination loops.
-    static constexpr int min_blocks = CPLX ? (MHI <= 16 ? 2 : 1) : (MHI <= 16 ? 3 : (MHI <= 32 ? 2 : 1));
+    // (65536 / (256 * min_blocks)): sized so each class's tile fits without spilling.
+    static constexpr int min_blocks = CPLX ? (MHI <= 16 ? 2 : 1)
+                                           : (MHI <= 8 ? 4 : (MHI <= 16 ? 3 : (MHI <= 32 ? 2 : 1)));
 };
 
-template <bool CPLX, int RPL, int MLO, int MHI>
-__device__ __forceinline__ void eval_term(const void *Ax, int lda, int E, int mE, int n, int rm, FastWs &w, int lane,
-                                          double prefac, dd &acc_re, dd &acc_im)
-{
-    const int mw = (2 * mE + 3) & ~3;  // register tile: the next multiple of 4 (MLO < m <= MHI)
-    if constexpr (!CPLX) {
-        const double *A = (const double *)Ax;
-        double val = 0.0;
-#define EGG_TILE(MWV)                                                                  \
-    if constexpr (MLO < MWV && MWV <= MHI) {                                            \
-        if (mw <= MWV) {                                                                \
-            val = term_real<MWV, (MWV > 32 ? 2 : 1)>(A, lda, E, mE, n, rm, w, lane);    \
-            goto done_real;                                                             \
-        }                                                                               \
-    }
-        EGG_TILE(4) EGG_TILE(8) EGG_TILE(12) EGG_TILE(16) EGG_TILE(20) EGG_TILE(24)
-        EGG_TILE(28) EGG_TILE(32) EGG_TILE(36) EGG_TILE(40) EGG_TILE(44) EGG_TILE(48)
-#undef EGG_TILE
-    done_real:
-        if (lane == 0) dd_add(acc_re, prefac * val);
-    } else {
-        const cd *A = (const cd *)Ax;
-        cd val{0.0, 0.0};
-#define EGG_TILE(MWV)                                                        \
-    if constexpr (MLO < MWV && MWV <= MHI) {                                  \
-        if (mw <= MWV) {                                                      \
-            val = term_cplx<MWV>(A, lda, E, mE, n, rm, w, lane);              \
-            goto done_cplx;                                                   \
-        }                                                                     \
-    }
-        EGG_TILE(4) EGG_TILE(8) EGG_TILE(12) EGG_TILE(16) EGG_TILE(20) EGG_TILE(24) EGG_TILE(28) EGG_TILE(32)
-#undef EGG_TILE
-    done_cplx:
-        if (lane == 0) {
-            dd_add(acc_re, prefac * val.re);
-            dd_add(acc_im, prefac * val.im);
-        }
-    }
-    (void)RPL;
-}
-
-template <bool CPLX, int RPL, int MLO, int MHI>
-__global__ void __launch_bounds__(256, (SizeClass<CPLX, RPL, MLO, MHI>::min_blocks))
+template <bool CPLX, int MLO, int MHI>
+__global__ void __launch_bounds__(256, (SizeClass<CPLX, MHI>::min_blocks))
     sieve_fast_kernel(SieveArgs a, const int64_t *__restrict__ strides, int warps_per_block, dd *partial)
 {
     extern __shared__ double smem[];
@@ -629,8 +524,8 @@ __global__ void __launch_bounds__(256, (SizeClass<CPLX, RPL, MLO, MHI>::min_bloc
     const int b = blockIdx.y;
     const SieveInst in = a.inst[b];
     const int E = in.E, n = in.n;
-    const int rm = ring_rows(a.nmax) - 1;
-    FastWs w = fast_carve(smem + (size_t)wib * fast_ws_doubles(a.nmax, CPLX), a.nmax, CPLX);
+    const int cs = a.nmax + 1;
+    const FastWs w = fast_carve(smem + (size_t)wib * fast_ws_doubles(a.nmax, CPLX, MHI), a.nmax, CPLX, MHI);
     const int wslot = blockIdx.x * warps_per_block + wib;
     const int64_t W = a.warps_per_inst;
     const int64_t chunk = (in.steps + W - 1) / W;
@@ -639,7 +534,7 @@ __global__ void __launch_bounds__(256, (SizeClass<CPLX, RPL, MLO, MHI>::min_bloc
     dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
     const int *reps = a.reps + in.reps_off;
     const int mr1 = a.maxrep + 1;
-    const void *Ax = CPLX ? (const void *)((const cd *)a.Ax + in.ax_off) : (const void *)((const double *)a.Ax + in.ax_off);
+    const bool unit = a.maxrep <= 1;  // all multiplicities 1: every binomial factor is 1
     // Odometer: lane i holds digit i (edge E-1 least significant); digit 0 clipped under Glynn.
     int r = 0, base = 1, digit = 0;
     if (lane < E) {
@@ -661,8 +556,11 @@ __global__ void __launch_bounds__(256, (SizeClass<CPLX, RPL, MLO, MHI>::min_bloc
         const int m = 2 * mE;
         if (m <= MLO || m > MHI) continue;  // another size class (or an empty term, which vanishes)
         const int esum = __reduce_add_sync(FULL, lane < E ? digit : 0);
-        double bp = lane < E ? a.binoms[r + digit * mr1] : 1.0;
-        for (int off = 16; off > 0; off >>= 1) bp *= __shfl_xor_sync(FULL, bp, off);
+        double bp = 1.0;
+        if (!unit) {
+            bp = lane < E ? a.binoms[r + digit * mr1] : 1.0;
+            for (int off = 16; off > 0; off >>= 1) bp *= __shfl_xor_sync(FULL, bp, off);
+        }
         double prefac = ((n - esum) & 1) ? -bp : bp;
         const int k0 = __shfl_sync(FULL, kk, 0);
         if (in.glynn && k0 == 0) prefac *= 0.5;
@@ -672,7 +570,17 @@ __global__ void __launch_bounds__(256, (SizeClass<CPLX, RPL, MLO, MHI>::min_bloc
             w.kval[pos] = (double)kk;
         }
         __syncwarp();
-        eval_term<CPLX, RPL, MLO, MHI>(Ax, in.lda, E, mE, n, rm, w, lane, prefac, acc_re, acc_im);
+        if constexpr (!CPLX) {
+            const double val = term_real<MHI, (MHI > 32 ? 2 : 1)>((const double *)a.Ax + in.ax_off, in.lda, E, mE, n, cs, w,
+                                                                  lane);
+            if (lane == 0) dd_add(acc_re, prefac * val);
+        } else {
+            const cd val = term_cplx<MHI>((const cd *)a.Ax + in.ax_off, in.lda, E, mE, n, cs, w, lane);
+            if (lane == 0) {
+                dd_add(acc_re, prefac * val.re);
+                dd_add(acc_im, prefac * val.im);
+            }
+        }
         __syncwarp();
     }
     if (lane == 0) {
@@ -682,42 +590,56 @@ __global__ void __launch_bounds__(256, (SizeClass<CPLX, RPL, MLO, MHI>::min_bloc
     }
 }
 
-size_t fast_smem_bytes(int nmax, int cplx, int warps)
+size_t fast_smem_bytes(int nmax, int cplx, int cls, int warps)
 {
-    return (size_t)warps * fast_ws_doubles(nmax, cplx) * sizeof(double);
+    return (size_t)warps * fast_ws_doubles(nmax, cplx, kFastClasses[cls][1]) * sizeof(double);
 }
 
-template <bool CPLX, int RPL, int MLO, int MHI>
+template <bool CPLX, int MLO, int MHI>
 static int launch_one(const SieveArgs &a, const int64_t *strides, dim3 grid, int wpb, size_t smem, dd *partial,
                       cudaStream_t st)
 {
-    auto k = sieve_fast_kernel<CPLX, RPL, MLO, MHI>;
+    auto k = sieve_fast_kernel<CPLX, MLO, MHI>;
     EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<grid, wpb * 32, smem, st>>>(a, strides, wpb, partial);
     EGG_CUDA_TRY(cudaGetLastError());
     return EGG_OK;
 }
 
-const int kFastClasses[][2] = {{0, 16}, {16, 24}, {24, 32}, {32, 40}, {40, 48}};
+const int kFastClasses[][2] = {{0, 8}, {8, 16}, {16, 24}, {24, 32}, {32, 40}, {40, 48}};
+
+static int upload_tables(cudaStream_t st)
+{
+    // -1/(2t), computed with IEEE division on the host.
+    static double host_tab[64];
+    if (host_tab[1] == 0.0)
+        for (int t = 1; t < 64; ++t) host_tab[t] = -1.0 / (2.0 * t);
+    EGG_CUDA_TRY(cudaMemcpyToSymbolAsync(c_neg_inv_2t, host_tab, sizeof(host_tab), 0, cudaMemcpyHostToDevice, st));
+    return EGG_OK;
+}
 
 int launch_fast(const SieveArgs &a, const int64_t *strides, int B, int cplx, int cls, dd *partial, int wpb,
                 int blocks_x, cudaStream_t st)
 {
-    const size_t smem = fast_smem_bytes(a.nmax, cplx, wpb);
+    int rc = upload_tables(st);
+    if (rc) return rc;
+    const size_t smem = fast_smem_bytes(a.nmax, cplx, cls, wpb);
     dim3 grid((unsigned)blocks_x, (unsigned)B);
     if (cplx) {
         switch (cls) {
-        case 0: return launch_one<true, 1, 0, 16>(a, strides, grid, wpb, smem, partial, st);
-        case 1: return launch_one<true, 1, 16, 24>(a, strides, grid, wpb, smem, partial, st);
-        case 2: return launch_one<true, 1, 24, 32>(a, strides, grid, wpb, smem, partial, st);
+        case 0: return launch_one<true, 0, 8>(a, strides, grid, wpb, smem, partial, st);
+        case 1: return launch_one<true, 8, 16>(a, strides, grid, wpb, smem, partial, st);
+        case 2: return launch_one<true, 16, 24>(a, strides, grid, wpb, smem, partial, st);
+        case 3: return launch_one<true, 24, 32>(a, strides, grid, wpb, smem, partial, st);
         }
     } else {
         switch (cls) {
-        case 0: return launch_one<false, 1, 0, 16>(a, strides, grid, wpb, smem, partial, st);
-        case 1: return launch_one<false, 1, 16, 24>(a, strides, grid, wpb, smem, partial, st);
-        case 2: return launch_one<false, 1, 24, 32>(a, strides, grid, wpb, smem, partial, st);
-        case 3: return launch_one<false, 2, 32, 40>(a, strides, grid, wpb, smem, partial, st);
-        case 4: return launch_one<false, 2, 40, 48>(a, strides, grid, wpb, smem, partial, st);
+        case 0: return launch_one<false, 0, 8>(a, strides, grid, wpb, smem, partial, st);
+        case 1: return launch_one<false, 8, 16>(a, strides, grid, wpb, smem, partial, st);
+        case 2: return launch_one<false, 16, 24>(a, strides, grid, wpb, smem, partial, st);
+        case 3: return launch_one<false, 24, 32>(a, strides, grid, wpb, smem, partial, st);
+        case 4: return launch_one<false, 32, 40>(a, strides, grid, wpb, smem, partial, st);
+        case 5: return launch_one<false, 40, 48>(a, strides, grid, wpb, smem, partial, st);
         }
     }
     return fail(EGG_ERR_ARGUMENT, "no such sieve size class");
