@@ -59,6 +59,11 @@ const char *egg_version(void);
 /* Message describing the calling thread's most recent failure ("" if none). */
 const char *egg_last_error(void);
 
+/* Kernel launches the library has made since it was loaded, all entry points together (a
+ * diagnostic: read it before and after a call to count that call's launches).  No counterpart in
+ * the reference. */
+int64_t egg_launch_count(void);
+
 /* Select the CUDA device (idempotent; the first call of any other entry point does this with
  * device 0).  Fails with EGG_ERR_NO_DEVICE if there is none. */
 int egg_init(int device);
@@ -85,23 +90,28 @@ int egg_dp_counts(int K, int64_t *nstates, int64_t *ntrans);
  * reference's 1-based starts[nstates+1], trans[ntrans], levels[nlevels].  Idempotent: a
  * resident plan for the key is kept.  The structure is checked on the device (every child in
  * the previous level, every pair index in 1..K(K-1)/2, uniform out-degree per level) and a plan
- * that fails is refused with EGG_ERR_PLAN_INVALID.
+ * that fails is refused with EGG_ERR_PLAN_INVALID.  A plan equal entry for entry to the layout of
+ * _build_dp_plan is then kept in closed form (its array is released and never read again, with
+ * identical results); any other valid plan keeps its array and is evaluated in its own order.
  * Replaces _device_plan(backend, plan), ext/TheEggmanKernelAbstractionsExt.jl:31-42. */
 int egg_plan_upload(int K, int idx_bytes, const void *starts, const void *trans, const void *levels,
                     int64_t nlevels, int64_t nstates, int64_t ntrans);
 
-/* Build the degree-K plan directly in device memory, laid out exactly as _build_dp_plan(K, I)
- * (src/dp.jl:223-304) would, by combinatorial ranking of the level subsets.  Same key and
- * caching as egg_plan_upload; refuses what the reference refuses (src/dp.jl:224-234) with
- * EGG_ERR_TOO_LARGE, and plans that would not fit in free device memory likewise. */
+/* Make the degree-K plan of _build_dp_plan(K, I) (src/dp.jl:223-304) resident in closed form:
+ * its states are the colex-ranked subsets of each level, so the evaluation derives every
+ * transition from the state's rank and no transition array is stored.  Same key and caching as
+ * egg_plan_upload; refuses what the reference refuses (src/dp.jl:224-234) with
+ * EGG_ERR_TOO_LARGE. */
 int egg_plan_build(int K, int idx_bytes);
 
-/* Sizes of a resident plan (EGG_ERR_NO_PLAN if absent). */
+/* Sizes of a resident plan (EGG_ERR_NO_PLAN if absent); device_bytes is 0 for a closed-form
+ * plan. */
 int egg_plan_info(int K, int idx_bytes, int64_t *nstates, int64_t *ntrans, int64_t *nlevels,
                   int64_t *device_bytes);
 
 /* Copy a resident plan back to the host in the reference layout (starts[nstates+1],
- * trans[ntrans], levels[nlevels], element size idx_bytes). */
+ * trans[ntrans], levels[nlevels], element size idx_bytes).  A closed-form plan is written out
+ * through a temporary device array of ntrans * idx_bytes bytes. */
 int egg_plan_download(int K, int idx_bytes, void *starts, void *trans, void *levels);
 
 /* Drop one resident plan. */

@@ -78,6 +78,50 @@ def test_uploaded_plan_is_validated(egg, nat, orc):
     egg.empty_gpu_cache()
 
 
+def _plan_device_bytes(nat, K, ib):
+    import ctypes
+
+    ns, nt, nl, db = (ctypes.c_int64() for _ in range(4))
+    nat.check(nat.lib().egg_plan_info(K, ib, ctypes.byref(ns), ctypes.byref(nt), ctypes.byref(nl), ctypes.byref(db)))
+    return db.value
+
+
+def _reversed_plan(orc, K, ib):
+    """The reference plan with each state's transitions in reverse order: still a valid plan (same
+    children, same pairs), but summed in another order."""
+    ref = orc.build_plan(K, ib)
+    tr = ref.trans.copy()
+    lv = ref.levels
+    for L in range(1, len(lv) - 1):
+        lo, hi = lv[L] - 1, lv[L + 1] - 1
+        t0, t1 = ref.starts[lo] - 1, ref.starts[hi] - 1
+        deg = (t1 - t0) // (hi - lo)
+        tr[t0:t1] = tr[t0:t1].reshape(hi - lo, deg)[:, ::-1].ravel()
+    return orc.Plan(K, ib, ref.nstates, ref.starts, tr, ref.levels)
+
+
+@pytest.mark.parametrize("K", [14, 26])
+def test_uploaded_plans_closed_form_or_explicit(egg, nat, orc, W, K):
+    # The reference layout is recognised and evaluated without its array; any other valid plan
+    # keeps its array and is summed in its own transition order.
+    A = W.dense_real(K, 4400 + K)
+    P = pairs_of(orc, A, K)[None, :]
+    egg.empty_gpu_cache()
+    ref = orc.build_plan(K, 4)
+    egg.upload_plan(K, 4, ref.starts, ref.trans, ref.levels)
+    assert _plan_device_bytes(nat, K, 4) == 0
+    got = run_dp(egg, nat, P, K, nat.EGG_F64)[0]
+    assert got == orc.haf_dp_pairs(P[0], ref, orc.F64)
+    egg.empty_gpu_cache()
+    rev = _reversed_plan(orc, K, 4)
+    egg.upload_plan(K, 4, rev.starts, rev.trans, rev.levels)
+    assert _plan_device_bytes(nat, K, 4) == rev.trans.nbytes
+    got_rev = run_dp(egg, nat, P, K, nat.EGG_F64)[0]
+    assert got_rev == orc.haf_dp_pairs(P[0], rev, orc.F64)
+    assert rel(got_rev, got) < 1e-12
+    egg.empty_gpu_cache()
+
+
 @pytest.mark.parametrize("kind", ["f64", "c128", "f32", "c64"])
 def test_exact_mode_bit_identical(egg, nat, orc, W, kind):
     dt = {"f64": np.float64, "c128": np.complex128, "f32": np.float32, "c64": np.complex64}[kind]
@@ -147,6 +191,21 @@ def test_chunking_and_determinism(egg, nat, orc, W):
     for b in range(7):
         assert run_dp(egg, nat, P[b:b + 1], K, nat.EGG_C128)[0] == full[b]
     assert np.array_equal(run_dp(egg, nat, P, K, nat.EGG_C128), full)
+
+
+@pytest.mark.parametrize("K,B", [(24, 5), (26, 2100)])
+def test_level_kernel_batches(egg, nat, orc, W, K, B):
+    # Degrees past the one-CTA kernel, with a small batch and with more instances than one block's
+    # chunk of (state, instance) pairs: every instance equals its own single-instance evaluation,
+    # and the first few equal the reference loop.
+    rng = np.random.default_rng(K * 1000 + B)
+    npairs = K * (K - 1) // 2
+    P = rng.uniform(-1.0, 1.0, size=(B, npairs))
+    got = run_dp(egg, nat, P, K, nat.EGG_F64)
+    plan = orc.build_plan(K, 4)
+    for b in sorted({0, 1, B // 2, B - 1}):
+        assert got[b] == run_dp(egg, nat, P[b:b + 1], K, nat.EGG_F64)[0], b
+        assert got[b] == orc.haf_dp_pairs(np.ascontiguousarray(P[b]), plan, orc.F64), b
 
 
 def test_cache_accounting(egg, nat, W):

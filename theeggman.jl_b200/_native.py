@@ -43,7 +43,7 @@ EXPORTS = (
     "egg_version", "egg_last_error", "egg_init", "egg_cache_bytes", "egg_cache_clear",
     "egg_dp_batch_bytes", "egg_dp_counts", "egg_plan_upload", "egg_plan_build", "egg_plan_info",
     "egg_plan_download", "egg_plan_release", "egg_dp_batch", "egg_dp_batch_device", "egg_sieve",
-    "egg_sieve_device", "egg_sieve_batch", "egg_sieve_batch_device", "egg_sieve_device_noalloc",
+    "egg_sieve_device", "egg_sieve_batch", "egg_sieve_batch_device", "egg_sieve_device_noalloc", "egg_launch_count",
 )
 
 
@@ -87,6 +87,7 @@ def lib() -> ctypes.CDLL:
     L.egg_last_error.restype = ctypes.c_char_p
     L.egg_init.argtypes = [i32]
     L.egg_cache_bytes.restype = i64
+    L.egg_launch_count.restype = i64
     L.egg_dp_batch_bytes.argtypes = [i32, i32, i64]
     L.egg_dp_batch_bytes.restype = i64
     L.egg_dp_counts.argtypes = [i32, p64, p64]

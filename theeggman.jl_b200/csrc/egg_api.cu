@@ -12,6 +12,7 @@
 namespace egg {
 
 static thread_local std::string t_err;
+std::atomic<long long> g_launches{0};
 
 void set_error(const std::string &msg) { t_err = msg; }
 int fail(int code, const std::string &msg)
@@ -127,6 +128,8 @@ extern "C" {
 const char *egg_version(void) { return "eggman_b200 0.1.0 (sm_100a)"; }
 
 const char *egg_last_error(void) { return t_err.c_str(); }
+
+int64_t egg_launch_count(void) { return (int64_t)g_launches.load(std::memory_order_relaxed); }
 
 int egg_init(int device)
 {
@@ -247,10 +250,18 @@ int egg_plan_upload(int K, int idx_bytes, const void *starts, const void *trans,
         }
     }
     rc = plan_validate_device(p, ctx().stream);
+    bool same = false;
+    if (!rc) rc = plan_is_closed_form(p, ctx().stream, &same);
     if (rc) {
         cudaStreamSynchronize(ctx().stream);
         cudaFree(p.trans);
         return rc;
+    }
+    if (same) {
+        // The uploaded plan is _build_dp_plan's layout: evaluate it in closed form and drop the
+        // array (the results are the same entry for entry; only the memory traffic differs).
+        cudaFree(p.trans);
+        p.trans = nullptr;
     }
     ctx().plans[{K, idx_bytes}] = std::move(p);
     return EGG_OK;
@@ -264,7 +275,7 @@ int egg_plan_build(int K, int idx_bytes)
     if (K % 2 != 0 || K < 2) return fail(EGG_ERR_ARGUMENT, "device plans are built for even degrees >= 2");
     if (find_plan(K, idx_bytes)) return EGG_OK;
     DevPlan p;
-    rc = plan_build_device(K, idx_bytes, p);
+    rc = plan_levels(K, idx_bytes, p);
     if (rc) return rc;
     ctx().plans[{K, idx_bytes}] = std::move(p);
     return EGG_OK;
@@ -299,7 +310,25 @@ int egg_plan_download(int K, int idx_bytes, void *starts, void *trans, void *lev
             for (int64_t s = 0; s < lv.n; ++s) st(starts, lv.lo + s + 1, lv.toff + (s + 1) * lv.deg + 1);
     }
     if (trans && p->ntrans) {
-        EGG_CUDA_TRY(cudaMemcpyAsync(trans, p->trans, (size_t)p->ntrans * idx_bytes, cudaMemcpyDeviceToHost, ctx().stream));
+        const size_t bytes = (size_t)p->ntrans * idx_bytes;
+        if (p->closed_form()) {
+            // Written out on request into a temporary device array.
+            void *tmp = nullptr;
+            cudaError_t e = cudaMalloc(&tmp, bytes);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                return fail(EGG_ERR_TOO_LARGE, "writing out the plan needs " + std::to_string(bytes) + " device bytes: " +
+                                                   cudaGetErrorString(e));
+            }
+            int rc = plan_materialize(*p, tmp, ctx().stream);
+            if (!rc) {
+                e = cudaMemcpy(trans, tmp, bytes, cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess) rc = fail(EGG_ERR_CUDA, std::string("plan download: ") + cudaGetErrorString(e));
+            }
+            cudaFree(tmp);
+            return rc;
+        }
+        EGG_CUDA_TRY(cudaMemcpyAsync(trans, p->trans, bytes, cudaMemcpyDeviceToHost, ctx().stream));
         EGG_CUDA_TRY(cudaStreamSynchronize(ctx().stream));
     }
     return EGG_OK;
@@ -332,13 +361,13 @@ int egg_dp_batch(int K, int idx_bytes, int dtype, int prec, const void *P, int64
     int64_t chunk = (max_batch > 0 && max_batch < B) ? max_batch : B;
     int64_t npairs = (int64_t)K * (K - 1) / 2;
     size_t oes = state_out_size(dtype);
-    if (max_batch <= 0) {
+    const size_t per = dp_scratch_bytes(*plan, dtype, prec, 1) + (size_t)npairs * es * 2 + oes;
+    const size_t held = c.scratch[0].bytes + c.scratch[1].bytes + c.scratch[2].bytes;
+    if (max_batch <= 0 && per * (size_t)B > held && per * (size_t)B > ((size_t)1 << 30)) {
         // The reference leaves chunking to the caller (src/dp.jl:581-582).  Here the free device
-        // memory is known, so an unchunked batch is split to fit half of it.
+        // memory is known, so an unchunked batch of more than 1 GiB is split to fit half of it.
         size_t free_b = 0, total_b = 0;
         EGG_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-        size_t held = c.scratch[0].bytes + c.scratch[1].bytes + c.scratch[2].bytes;
-        size_t per = dp_scratch_bytes(*plan, dtype, prec, 1) + (size_t)npairs * es * 2 + oes;
         int64_t fit = (int64_t)((free_b + held) / 2 / (per ? per : 1));
         if (fit < 1) return fail(EGG_ERR_TOO_LARGE, "one instance's work buffers do not fit in device memory");
         if (chunk > fit) chunk = fit;
@@ -352,7 +381,11 @@ int egg_dp_batch(int K, int idx_bytes, int dtype, int prec, const void *P, int64
         // This chunk's pairs, re-laid with the chunk's own instance count as leading dimension
         // (the host transpose of ext/TheEggmanKernelAbstractionsExt.jl:127-130, done as one
         // strided copy).
-        if (npairs > 0)
+        // An unchunked batch is already in that layout and goes as one contiguous copy: a 2-D
+        // copy of short rows from pageable memory costs one staged transfer per row.
+        if (npairs > 0 && nb == B)
+            EGG_CUDA_TRY(cudaMemcpyAsync(c.scratch[1].ptr, P, (size_t)B * npairs * es, cudaMemcpyHostToDevice, c.stream));
+        else if (npairs > 0)
             EGG_CUDA_TRY(cudaMemcpy2DAsync(c.scratch[1].ptr, nb * es, (const char *)P + b0 * es, B * es, nb * es, npairs,
                                            cudaMemcpyHostToDevice, c.stream));
         rc = dp_run(*plan, dtype, prec, c.scratch[1].ptr, nb, c.scratch[2].ptr, c.stream);

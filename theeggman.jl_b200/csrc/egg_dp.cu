@@ -1,12 +1,17 @@
 // egg_dp.cu -- the subset DP (src/dp.jl:344-363 _dp_states!, :408-442 _haf_dp) on the device.
 //
-// Layout in HBM.  The plan's packed transitions stay resident (one array per (K, layout)).  State
-// values live in two ping-pong buffers, each sized for the largest level: every transition out of a
-// level lands in the level immediately below (two subset sizes down, src/dp.jl:146-148), so level L
-// only ever reads level L-1 and the full `H` of the reference (1.3 GB at K = 40 in FP64) is never
-// materialised.  Within a buffer values are instance-fastest, (state - level_lo) * B + b, the
-// reference device layout (ext/TheEggmanKernelAbstractionsExt.jl:13-20, :56-62) restricted to
-// one level.
+// Layout in HBM.  State values live in two ping-pong buffers, each sized for the largest level:
+// every transition out of a level lands in the level immediately below (two subset sizes down,
+// src/dp.jl:146-148), so level L only ever reads level L-1 and the full `H` of the reference
+// (1.3 GB at K = 40 in FP64) is never materialised.  Within a buffer values are instance-fastest,
+// (state - level_lo) * B + b, the reference device layout (ext/TheEggmanKernelAbstractionsExt.jl:
+// 13-20, :56-62) restricted to one level.
+//
+// Plans.  The plan of _build_dp_plan has a closed form (egg_plan.cu), so a resident plan of that
+// layout is evaluated without its transition array: each thread derives its state's children from
+// the state's rank (dpc_* kernels below).  At K = 40 that removes 22.7 GB of reads per evaluation.
+// An uploaded plan that differs from that layout keeps its array and runs through the dp_* kernels
+// that read it.
 //
 // Arithmetic.  Each state is accumulated by one thread in plan order, as the reference does.
 // EGG_PREC_EXACT rounds every product and sum separately (__dmul_rn/__dadd_rn), which is how Julia
@@ -64,6 +69,9 @@ __device__ __forceinline__ void store(cf &d, cf a) { d = a; }
 __device__ __forceinline__ void store(cf &d, cd a) { d = cf{__double2float_rn(a.re), __double2float_rn(a.im)}; }
 __device__ __forceinline__ void store(__int128 &d, __int128 a) { d = a; }
 
+// Transitions whose loads a thread issues together before accumulating them in order.
+static constexpr int kBatch = 8;
+
 // One level: states [0, n) of the level, out-degree deg, transitions from toff.  Hprev holds
 // level L-1 (child numbers are 1-based global, child_lo1 = first state of L-1, 1-based).
 template <class Op, class I, class PT, class HT, class AT, bool B1>
@@ -84,13 +92,287 @@ __global__ void __launch_bounds__(256) dp_level_kernel(const I *__restrict__ tra
         }
         const I *tr = trans + toff + s * deg;
         AT acc = zero_of<AT>();
-        for (int k = 0; k < deg; ++k) {
-            I t = __ldg(tr + k);
-            int64_t pi = (int64_t)(t & mask) - 1;
-            int64_t ci = (int64_t)(t >> bits) - child_lo1;
-            acc = madd(Op{}, acc, P[pi * B + b], Hprev[ci * B + b]);
+        for (int k0 = 0; k0 < deg; k0 += kBatch) {
+            I tv[kBatch];
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u)
+                if (k0 + u < deg) tv[u] = __ldg(tr + k0 + u);
+            PT pv[kBatch];
+            HT hv[kBatch];
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u)
+                if (k0 + u < deg) {
+                    const int64_t pi = (int64_t)(tv[u] & mask) - 1;
+                    const int64_t ci = (int64_t)(tv[u] >> bits) - child_lo1;
+                    pv[u] = P[pi * B + b];
+                    hv[u] = Hprev[ci * B + b];
+                }
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u)
+                if (k0 + u < deg) acc = madd(Op{}, acc, pv[u], hv[u]);
         }
         store(Hcur[s * B + b], acc);
+    }
+}
+
+// Whole instances in one launch, for degrees whose two largest adjacent levels fit in shared
+// memory (N <= 22 in FP64): one CTA per instance (grid-strided over the batch), the level loop
+// inside the kernel with a barrier between levels, both level buffers and the instance's pairs in
+// shared memory, the plan streamed from global memory (it is L2-resident at these sizes, 0.36 MB
+// at N = 20).  Same per-state arithmetic and order as dp_level_kernel.
+static constexpr int kSmallMaxDeg = 23;  // out-degree |S|-1 of the largest level handled (N <= 24)
+
+struct SmallLevels {
+    int64_t toff[33];
+    int n[33];
+    int deg[33];
+    int nlev;
+};
+
+template <class Op, class I, class PT, class HT, class AT>
+__global__ void __launch_bounds__(512) dp_small_kernel(const I *__restrict__ trans, SmallLevels lv, const PT *__restrict__ P,
+                                                       HT *__restrict__ out, int64_t B, int npairs, int maxlev, int bits)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    HT *H0 = reinterpret_cast<HT *>(smem_raw);
+    HT *H1 = H0 + maxlev;
+    PT *Ps = reinterpret_cast<PT *>(H1 + maxlev);
+    const I mask = ((I)1 << bits) - 1;
+    for (int64_t b = blockIdx.x; b < B; b += gridDim.x) {
+        for (int q = threadIdx.x; q < npairs; q += blockDim.x) Ps[q] = P[(int64_t)q * B + b];
+        if (threadIdx.x == 0) H0[0] = one_of<HT>();
+        __syncthreads();
+        int64_t child_lo1 = 1;  // first state of the previous level, 1-based
+        int64_t lo1 = 2;        // first state of the current level, 1-based
+        for (int L = 1; L < lv.nlev; ++L) {
+            const HT *prev = (L & 1) ? H0 : H1;
+            HT *cur = (L & 1) ? H1 : H0;
+            const int n = lv.n[L], deg = lv.deg[L];
+            const I *tl = trans + lv.toff[L];
+            for (int s = threadIdx.x; s < n; s += blockDim.x) {
+                // Issue all of this state's transition loads before using any (one L2 round trip),
+                // then accumulate in plan order.
+                const I *tr = tl + (int64_t)s * deg;
+                I tv[kSmallMaxDeg];
+#pragma unroll
+                for (int k = 0; k < kSmallMaxDeg; ++k)
+                    if (k < deg) tv[k] = __ldg(tr + k);
+                AT acc = zero_of<AT>();
+#pragma unroll
+                for (int k = 0; k < kSmallMaxDeg; ++k)
+                    if (k < deg) acc = madd(Op{}, acc, Ps[(int)(tv[k] & mask) - 1], prev[(int64_t)(tv[k] >> bits) - child_lo1]);
+                store(cur[s], acc);
+            }
+            __syncthreads();
+            child_lo1 = lo1;
+            lo1 += n;
+        }
+        if (threadIdx.x == 0) out[b] = ((lv.nlev - 1) & 1) ? H1[0] : H0[0];
+        __syncthreads();
+    }
+}
+
+// ---- closed-form plans ---------------------------------------------------------------------------
+//
+// A plan with the layout of _build_dp_plan (src/dp.jl:223-304) needs no transition array.  Level c
+// (popcount c) is every c-subset of the top U = K - m0 positions (m0 = (K - c) / 2), numbered in
+// colex order, which is increasing mask order.  A state S with shifted elements e1 < ... < ec has
+// out-degree c - 1; its j-th transition (j = 2..c, the order of the plan) pairs e1 with ej and
+// lands on S - {e1, ej}, whose rank in the level below is
+//     pre_j + suf_j,  pre_j = sum_{x=2}^{j-1} C(e_x - 1, x - 1),  suf_j = sum_{x=j+1}^{c} C(e_x - 1, x - 2).
+// Both sums are carried along the walk, so a transition costs two table lookups in shared memory
+// instead of an 8-byte load from HBM.  The arithmetic per state is that of the plan kernels, in
+// the same order, so results are identical.
+
+template <class M> __device__ __forceinline__ int low_bit(M v);
+template <> __device__ __forceinline__ int low_bit<uint32_t>(uint32_t v) { return __ffs((int)v) - 1; }
+template <> __device__ __forceinline__ int low_bit<uint64_t>(uint64_t v) { return __ffsll((long long)v) - 1; }
+
+// The colex-successor of a c-subset mask (the next larger integer with the same popcount).
+template <class M> __device__ __forceinline__ M colex_next(M v)
+{
+    const M t = v | (v - 1);
+    return (t + 1) | (((~t & (M)(0 - ~t)) - 1) >> (low_bit<M>(v) + 1));
+}
+
+// The c-subset of [0, U) with colex rank R; T[x * ld + k] = C(x, k) (saturated at 2^32 - 1, which
+// stays above every rank compared against it).
+template <class M>
+__device__ __forceinline__ M colex_unrank(const uint32_t *T, int ld, int U, int c, uint32_t R)
+{
+    M m = 0;
+    int x = U - 1;
+    for (int i = c; i >= 1; --i) {
+        uint32_t v;
+        while ((v = T[x * ld + i]) > R) --x;
+        m |= (M)1 << x;
+        R -= v;
+        --x;
+    }
+    return m;
+}
+
+// One state's value: sum over its transitions, in plan order, of P[pair] * H[child] (instance b
+// of B, instance-fastest; B1 when B == 1).  Hprev == nullptr stands for the level of the empty set
+// (value 1).  The loads of kBatch transitions are issued before any of them is used, so a state
+// waits for one memory round trip per batch rather than one per transition; the accumulation
+// order is unchanged.
+
+template <class Op, class M, class PT, class HT, class AT, bool B1>
+__device__ __forceinline__ AT walk_state(M m, const uint32_t *T, int ld, int c, int K, int m0, const PT *P,
+                                         const HT *Hprev, int64_t B, int64_t b)
+{
+    const int e1 = low_bit<M>(m);
+    M rest = m & (m - 1);
+    uint32_t suf = 0;
+    {
+        M r2 = rest & (rest - 1);
+        for (int x = 3; x <= c; ++x) {
+            const int e = low_bit<M>(r2);
+            r2 &= r2 - 1;
+            suf += T[(e - 1) * ld + (x - 2)];
+        }
+    }
+    // 0-based _pair_index(e1 + m0 + 1, ej + m0 + 1, K) - 1 = pb + ej (src/unrolled.jl:60).
+    const int ib = e1 + m0 + 1;
+    const int pb = (ib - 1) * K - (ib * (ib + 1)) / 2 + m0;
+    uint32_t pre = 0;
+    int ej = low_bit<M>(rest);
+    rest &= rest - 1;
+    AT acc = zero_of<AT>();
+    for (int x0 = 2; x0 <= c; x0 += kBatch) {
+        HT hv[kBatch];
+        PT pv[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int x = x0 + u;
+            if (x <= c) {
+                const uint32_t child = pre + suf;
+                if (B1) {
+                    hv[u] = Hprev ? Hprev[child] : one_of<HT>();
+                    pv[u] = P[pb + ej];
+                } else {
+                    hv[u] = Hprev ? Hprev[(int64_t)child * B + b] : one_of<HT>();
+                    pv[u] = P[(int64_t)(pb + ej) * B + b];
+                }
+                pre += T[(ej - 1) * ld + (x - 1)];
+                if (x < c) {
+                    const int en = low_bit<M>(rest);
+                    rest &= rest - 1;
+                    suf -= T[(en - 1) * ld + (x - 1)];
+                    ej = en;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u)
+            if (x0 + u <= c) acc = madd(Op{}, acc, pv[u], hv[u]);
+    }
+    return acc;
+}
+
+// One level of a closed-form plan.  Each block takes chunks of run * 256 consecutive states
+// (run <= kRun, smaller for small levels so that every SM gets blocks): first every thread writes
+// the masks of `run` consecutive states into shared memory (one unrank, then colex successors),
+// then the threads walk the chunk's (state, instance) pairs with consecutive threads on
+// consecutive pairs, so a warp's child loads fall on a few neighbouring sectors.
+static constexpr int kRun = 8;
+static constexpr int kLevelThreads = 256;
+
+template <class M, class PT>
+static size_t level_smem(int K, int c, int64_t B)
+{
+    const int m0 = (K - c) / 2, U = K - m0;
+    size_t bytes = (size_t)kRun * kLevelThreads * sizeof(M) + (((size_t)U * (c + 1) * 4 + 15) / 16) * 16;
+    if (B == 1) bytes += (size_t)K * (K - 1) / 2 * sizeof(PT);
+    return bytes;
+}
+
+template <class Op, class M, class PT, class HT, class AT, bool B1>
+__global__ void __launch_bounds__(kLevelThreads) dpc_level_kernel(const uint32_t *__restrict__ binom, const PT *__restrict__ P,
+                                                                  const HT *__restrict__ Hprev, HT *__restrict__ Hcur,
+                                                                  int K, int c, int64_t n, int64_t B, int run)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int m0 = (K - c) / 2, U = K - m0, ld = c + 1;
+    M *masks = reinterpret_cast<M *>(smem_raw);
+    uint32_t *T = reinterpret_cast<uint32_t *>(masks + kRun * kLevelThreads);
+    PT *Ps = reinterpret_cast<PT *>(smem_raw + (size_t)kRun * kLevelThreads * sizeof(M) + (((size_t)U * ld * 4 + 15) / 16) * 16);
+    for (int i = threadIdx.x; i < U * ld; i += kLevelThreads) T[i] = binom[(i / ld) * 65 + (i % ld)];
+    const int npairs = K * (K - 1) / 2;
+    if (B1)
+        for (int q = threadIdx.x; q < npairs; q += kLevelThreads) Ps[q] = P[q];
+    __syncthreads();
+    const PT *Pp = B1 ? Ps : P;
+    // States per chunk: run * 256 for one instance, fewer for a batch (about that many pairs).
+    const int64_t chunk = B1 ? (int64_t)run * kLevelThreads
+                             : (B >= (int64_t)run * kLevelThreads ? 1 : ((int64_t)run * kLevelThreads) / B);
+    for (int64_t s0 = blockIdx.x * chunk; s0 < n; s0 += (int64_t)gridDim.x * chunk) {
+        const int cnt = (int)(n - s0 < chunk ? n - s0 : chunk);
+        const int r0 = threadIdx.x * run;
+        if (r0 < cnt) {
+            M m = colex_unrank<M>(T, ld, U, c, (uint32_t)(s0 + r0));
+            masks[r0] = m;
+            for (int r = 1; r < run && r0 + r < cnt; ++r) {
+                m = colex_next<M>(m);
+                masks[r0 + r] = m;
+            }
+        }
+        __syncthreads();
+        const int64_t items = (int64_t)cnt * B;
+        for (int64_t i = threadIdx.x; i < items; i += kLevelThreads) {
+            int sl;
+            int64_t b;
+            if (B1) {
+                sl = (int)i;
+                b = 0;
+            } else {
+                sl = (int)(i / B);
+                b = i - (int64_t)sl * B;
+            }
+            const AT acc = walk_state<Op, M, PT, HT, AT, B1>(masks[sl], T, ld, c, K, m0, Pp, Hprev, B, b);
+            store(Hcur[(s0 + sl) * B + b], acc);
+        }
+        __syncthreads();
+    }
+}
+
+// Whole instances of a closed-form plan in one launch (degrees whose two largest levels fit in
+// shared memory): one CTA per instance, the level loop inside the kernel.  Each thread takes a
+// run of consecutive states of a level (one unrank, then successors) and walks each in turn.
+template <class Op, class PT, class HT, class AT, int MAXT>
+__global__ void __launch_bounds__(MAXT) dpc_small_kernel(const uint32_t *__restrict__ binom, const PT *__restrict__ P,
+                                                        HT *__restrict__ out, int64_t B, int K, int maxlev)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    HT *H0 = reinterpret_cast<HT *>(smem_raw);
+    HT *H1 = H0 + maxlev;
+    PT *Ps = reinterpret_cast<PT *>(H1 + maxlev);
+    const int npairs = K * (K - 1) / 2;
+    const int ld = K + 1;
+    uint32_t *T = reinterpret_cast<uint32_t *>(smem_raw + (((size_t)2 * maxlev * sizeof(HT) + (size_t)npairs * sizeof(PT) + 15) / 16) * 16);
+    for (int i = threadIdx.x; i < ld * ld; i += blockDim.x) T[i] = binom[(i / ld) * 65 + (i % ld)];
+    for (int64_t b = blockIdx.x; b < B; b += gridDim.x) {
+        for (int q = threadIdx.x; q < npairs; q += blockDim.x) Ps[q] = P[(int64_t)q * B + b];
+        __syncthreads();
+        for (int c = 2; c <= K; c += 2) {
+            const HT *prev = c == 2 ? nullptr : (((c / 2) & 1) ? H0 : H1);
+            HT *cur = ((c / 2) & 1) ? H1 : H0;
+            const int m0 = (K - c) / 2, U = K - m0;
+            const int n = (int)T[U * ld + c];
+            const int per = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+            const int r0 = threadIdx.x * per;
+            if (r0 < n) {
+                uint32_t m = colex_unrank<uint32_t>(T, ld, U, c, (uint32_t)r0);
+                for (int r = 0; r < per && r0 + r < n; ++r) {
+                    if (r) m = colex_next<uint32_t>(m);
+                    store(cur[r0 + r], walk_state<Op, uint32_t, PT, HT, AT, true>(m, T, ld, c, K, m0, Ps, prev, 1, 0));
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[b] = ((K / 2) & 1) ? H1[0] : H0[0];
+        __syncthreads();
     }
 }
 
@@ -150,10 +432,134 @@ size_t dp_scratch_bytes(const DevPlan &plan, int dtype, int prec, int64_t B)
     return 2 * (size_t)max_level(plan) * (size_t)B * hs;
 }
 
+// Shared memory the whole-instance kernel needs for this plan (0 if it does not fit).
+template <class PT, class HT>
+static size_t small_smem(const DevPlan &plan)
+{
+    if (plan.levels.size() > 33 || plan.K - 1 > kSmallMaxDeg) return 0;
+    int64_t maxlev = 1;
+    for (const Level &lv : plan.levels) maxlev = lv.n > maxlev ? lv.n : maxlev;
+    const int64_t npairs = (int64_t)plan.K * (plan.K - 1) / 2;
+    size_t bytes = 2 * (size_t)maxlev * sizeof(HT) + (size_t)npairs * sizeof(PT) + 64;
+    return bytes <= 160 * 1024 ? bytes : 0;
+}
+
+template <class Op, class I, class PT, class HT, class AT>
+static int run_small(const DevPlan &plan, const PT *P, HT *out, int64_t B, size_t smem, cudaStream_t st)
+{
+    SmallLevels lv;
+    lv.nlev = (int)plan.levels.size();
+    int64_t maxlev = 1;
+    for (int L = 0; L < lv.nlev; ++L) {
+        lv.toff[L] = plan.levels[L].toff;
+        lv.n[L] = (int)plan.levels[L].n;
+        lv.deg[L] = plan.levels[L].deg;
+        maxlev = plan.levels[L].n > maxlev ? plan.levels[L].n : maxlev;
+    }
+    auto k = dp_small_kernel<Op, I, PT, HT, AT>;
+    EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int64_t grid = B;
+    const int64_t cap = (int64_t)ctx().num_sms * 8;
+    if (grid > cap) grid = cap;
+    const int threads = B == 1 ? 512 : (maxlev >= 1024 ? 256 : 128);
+    k<<<(unsigned)grid, threads, smem, st>>>((const I *)plan.trans, lv, P, out, B, plan.K * (plan.K - 1) / 2, (int)maxlev,
+                                               pair_bits(plan.idx_bytes));
+    count_launch();
+    EGG_CUDA_TRY(cudaGetLastError());
+    return EGG_OK;
+}
+
+// Shared memory dpc_small_kernel needs for a closed-form plan (0 if it does not fit).
+template <class PT, class HT>
+static size_t closed_small_smem(const DevPlan &plan)
+{
+    if (plan.K > 24) return 0;
+    const int64_t maxlev = max_level(plan);
+    const int64_t npairs = (int64_t)plan.K * (plan.K - 1) / 2;
+    size_t bytes = (((size_t)2 * maxlev * sizeof(HT) + (size_t)npairs * sizeof(PT) + 15) / 16) * 16 +
+                   (size_t)(plan.K + 1) * (plan.K + 1) * 4;
+    return bytes <= 160 * 1024 ? bytes : 0;
+}
+
+template <class Op, class M, class PT, class HT, class AT>
+static int launch_closed_level(const uint32_t *bt, const PT *P, const HT *prev, HT *cur, int K, int c, int64_t n, int64_t B,
+                               cudaStream_t st)
+{
+    auto k = B == 1 ? dpc_level_kernel<Op, M, PT, HT, AT, true> : dpc_level_kernel<Op, M, PT, HT, AT, false>;
+    static bool attr_set = false;  // per instantiation; the library's lock serialises callers
+    if (!attr_set) {
+        EGG_CUDA_TRY(cudaFuncSetAttribute(dpc_level_kernel<Op, M, PT, HT, AT, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        EGG_CUDA_TRY(cudaFuncSetAttribute(dpc_level_kernel<Op, M, PT, HT, AT, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        attr_set = true;
+    }
+    const size_t sm = level_smem<M, PT>(K, c, B);
+    // The longest run (fewest unranks) that still gives every SM several blocks.
+    const int64_t want = (int64_t)ctx().num_sms * 4;
+    int run = kRun;
+    while (run > 1) {
+        const int64_t ch = B >= (int64_t)run * kLevelThreads ? 1 : ((int64_t)run * kLevelThreads) / B;
+        if ((n + ch - 1) / ch >= want) break;
+        run /= 2;
+    }
+    const int64_t chunk = B >= (int64_t)run * kLevelThreads ? 1 : ((int64_t)run * kLevelThreads) / B;
+    int64_t blocks = (n + chunk - 1) / chunk;
+    const int64_t cap = (int64_t)ctx().num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    k<<<(unsigned)blocks, kLevelThreads, sm, st>>>(bt, P, prev, cur, K, c, n, B, run);
+    count_launch();
+    return EGG_OK;
+}
+
+// A closed-form plan: one launch for small degrees, else one launch per level with the last level
+// written straight into `out` when the state type is the output type.
+template <class Op, class PT, class HT, class AT>
+static int run_closed(const DevPlan &plan, const PT *P, HT *h0, HT *h1, HT *out, bool out_direct, int64_t B,
+                      cudaStream_t st)
+{
+    int rc = EGG_OK;
+    const uint32_t *bt = binom32_device(st, &rc);
+    if (!bt) return rc;
+    const int K = plan.K;
+    const size_t small = out_direct ? closed_small_smem<PT, HT>(plan) : 0;
+    if (small) {
+        // One instance: as many threads as keep the state type's registers unspilled.
+        constexpr int kMaxT = sizeof(HT) <= 8 ? 1024 : 512;
+        auto k = dpc_small_kernel<Op, PT, HT, AT, kMaxT>;
+        EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small));
+        int64_t grid = B;
+        const int64_t cap = (int64_t)ctx().num_sms * 8;
+        if (grid > cap) grid = cap;
+        const int threads = B == 1 ? kMaxT : (max_level(plan) >= 1024 ? 256 : 128);
+        k<<<(unsigned)grid, threads, small, st>>>(bt, P, out, B, K, (int)max_level(plan));
+        count_launch();
+        EGG_CUDA_TRY(cudaGetLastError());
+        return EGG_OK;
+    }
+    for (int64_t L = 0; L < (int64_t)plan.levels.size(); ++L)
+        if (plan.levels[L].n >= ((int64_t)1 << 31))
+            return fail(EGG_ERR_TOO_LARGE, "a level of the degree-" + std::to_string(K) + " plan has 2^31 states or more");
+    const HT *prev = nullptr;  // the empty set's level: value 1
+    const int nlev = (int)plan.levels.size();
+    for (int L = 1; L < nlev; ++L) {
+        const int c = 2 * L;
+        HT *cur = (L == nlev - 1 && out_direct) ? out : ((L & 1) ? h1 : h0);
+        const int U = K - (K - c) / 2;
+        rc = U <= 32 ? launch_closed_level<Op, uint32_t, PT, HT, AT>(bt, P, prev, cur, K, c, plan.levels[L].n, B, st)
+                     : launch_closed_level<Op, uint64_t, PT, HT, AT>(bt, P, prev, cur, K, c, plan.levels[L].n, B, st);
+        if (rc) return rc;
+        prev = cur;
+    }
+    EGG_CUDA_TRY(cudaGetLastError());
+    return EGG_OK;
+}
+
 template <class Op, class I, class PT, class HT, class AT>
 static int run_levels(const DevPlan &plan, const PT *P, HT *H0, HT *H1, int64_t B, cudaStream_t st)
 {
     fill_one_kernel<HT><<<grid_for(B, 256), 256, 0, st>>>(H0, B);
+    count_launch((long long)plan.levels.size());  // the fill and one launch per level below
     const int bits = pair_bits(plan.idx_bytes);
     for (size_t L = 1; L < plan.levels.size(); ++L) {
         const Level &lv = plan.levels[L];
@@ -191,44 +597,64 @@ static int dp_dispatch(const DevPlan &plan, int dtype, int prec, const void *dP,
         if (rc) return rc;
         float *P32 = (float *)c.scratch[5].ptr;
         to_f32_kernel<<<grid_for(nvals, 256), 256, 0, st>>>((const double *)dP, P32, nvals);
-        if (dtype == EGG_F64)
+        count_launch();
+        if (plan.closed_form()) {
+            if (dtype == EGG_F64)
+                rc = run_closed<MixedOp, float, float, double>(plan, P32, (float *)h0, (float *)h1, nullptr, false, B, st);
+            else
+                rc = run_closed<MixedOp, cf, cf, cd>(plan, (const cf *)P32, (cf *)h0, (cf *)h1, nullptr, false, B, st);
+        } else if (dtype == EGG_F64) {
             rc = run_levels<MixedOp, I, float, float, double>(plan, P32, (float *)h0, (float *)h1, B, st);
-        else
+        } else {
             rc = run_levels<MixedOp, I, cf, cf, cd>(plan, (const cf *)P32, (cf *)h0, (cf *)h1, B, st);
+        }
         if (rc) return rc;
         to_f64_kernel<<<grid_for(B, 256), 256, 0, st>>>((const float *)res, (double *)dout,
                                                          B * (dtype == EGG_C128 ? 2 : 1));
+        count_launch();
         EGG_CUDA_TRY(cudaGetLastError());
         return EGG_OK;
     }
     const bool fma_mode = prec == EGG_PREC_FMA;
     if (prec != EGG_PREC_EXACT && prec != EGG_PREC_FMA && prec != EGG_PREC_MIXED)
         return fail(EGG_ERR_ARGUMENT, "unknown precision mode");
+    // Degrees whose levels fit in shared memory run whole instances in one launch.
+#define EGG_SMALL_OR_LEVELS(OPX, PT, HT, AT)                                                                   \
+    do {                                                                                                      \
+        const size_t sm = plan.closed_form() ? 0 : small_smem<PT, HT>(plan);                                  \
+        if (plan.closed_form()) {                                                                             \
+            rc = run_closed<OPX, PT, HT, AT>(plan, (const PT *)dP, (HT *)h0, (HT *)h1, (HT *)dout, true, B, st); \
+        } else if (sm) {                                                                                      \
+            rc = run_small<OPX, I, PT, HT, AT>(plan, (const PT *)dP, (HT *)dout, B, sm, st);                  \
+        } else {                                                                                              \
+            rc = run_levels<OPX, I, PT, HT, AT>(plan, (const PT *)dP, (HT *)h0, (HT *)h1, B, st);             \
+            if (!rc) {                                                                                        \
+                copy_out_kernel<HT><<<grid_for(B, 256), 256, 0, st>>>((const HT *)res, (HT *)dout, B);        \
+                count_launch();                                                                               \
+            }                                                                                                 \
+        }                                                                                                     \
+    } while (0)
     switch (dtype) {
     case EGG_F64:
-        rc = fma_mode ? run_levels<FmaOp, I, double, double, double>(plan, (const double *)dP, (double *)h0, (double *)h1, B, st)
-                      : run_levels<ExactOp, I, double, double, double>(plan, (const double *)dP, (double *)h0, (double *)h1, B, st);
-        if (!rc) copy_out_kernel<double><<<grid_for(B, 256), 256, 0, st>>>((const double *)res, (double *)dout, B);
+        if (fma_mode) EGG_SMALL_OR_LEVELS(FmaOp, double, double, double);
+        else EGG_SMALL_OR_LEVELS(ExactOp, double, double, double);
         break;
     case EGG_C128:
-        rc = fma_mode ? run_levels<FmaOp, I, cd, cd, cd>(plan, (const cd *)dP, (cd *)h0, (cd *)h1, B, st)
-                      : run_levels<ExactOp, I, cd, cd, cd>(plan, (const cd *)dP, (cd *)h0, (cd *)h1, B, st);
-        if (!rc) copy_out_kernel<cd><<<grid_for(B, 256), 256, 0, st>>>((const cd *)res, (cd *)dout, B);
+        if (fma_mode) EGG_SMALL_OR_LEVELS(FmaOp, cd, cd, cd);
+        else EGG_SMALL_OR_LEVELS(ExactOp, cd, cd, cd);
         break;
     case EGG_F32:
-        rc = fma_mode ? run_levels<FmaOp, I, float, float, float>(plan, (const float *)dP, (float *)h0, (float *)h1, B, st)
-                      : run_levels<ExactOp, I, float, float, float>(plan, (const float *)dP, (float *)h0, (float *)h1, B, st);
-        if (!rc) copy_out_kernel<float><<<grid_for(B, 256), 256, 0, st>>>((const float *)res, (float *)dout, B);
+        if (fma_mode) EGG_SMALL_OR_LEVELS(FmaOp, float, float, float);
+        else EGG_SMALL_OR_LEVELS(ExactOp, float, float, float);
         break;
     case EGG_C64:
-        rc = fma_mode ? run_levels<FmaOp, I, cf, cf, cf>(plan, (const cf *)dP, (cf *)h0, (cf *)h1, B, st)
-                      : run_levels<ExactOp, I, cf, cf, cf>(plan, (const cf *)dP, (cf *)h0, (cf *)h1, B, st);
-        if (!rc) copy_out_kernel<cf><<<grid_for(B, 256), 256, 0, st>>>((const cf *)res, (cf *)dout, B);
+        if (fma_mode) EGG_SMALL_OR_LEVELS(FmaOp, cf, cf, cf);
+        else EGG_SMALL_OR_LEVELS(ExactOp, cf, cf, cf);
         break;
     case EGG_I64:
-        rc = run_levels<IntOp, I, int64_t, __int128, __int128>(plan, (const int64_t *)dP, (__int128 *)h0, (__int128 *)h1, B, st);
-        if (!rc) copy_out_kernel<__int128><<<grid_for(B, 256), 256, 0, st>>>((const __int128 *)res, (__int128 *)dout, B);
+        EGG_SMALL_OR_LEVELS(IntOp, int64_t, __int128, __int128);
         break;
+#undef EGG_SMALL_OR_LEVELS
     default:
         return fail(EGG_ERR_ARGUMENT, "unknown dtype");
     }

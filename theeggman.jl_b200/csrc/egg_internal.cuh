@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -108,13 +109,17 @@ struct Level {
     int deg;
 };
 
+// A plan is either closed-form (`trans` null: the layout _build_dp_plan produces, evaluated without
+// reading any transition array) or explicit (an uploaded `trans` that passed the structure check
+// but differs from that layout, evaluated by reading it).
 struct DevPlan {
     int K = 0, idx_bytes = 0;
     int64_t nstates = 0, ntrans = 0;
-    void *trans = nullptr;        // device, ntrans entries of idx_bytes
+    void *trans = nullptr;        // device, ntrans entries of idx_bytes; null for a closed-form plan
     std::vector<Level> levels;    // levels[0] is the empty set
     std::vector<int64_t> level_starts;  // the reference's 1-based `levels` vector
-    int64_t bytes() const { return ntrans * (int64_t)idx_bytes; }
+    bool closed_form() const { return trans == nullptr; }
+    int64_t bytes() const { return trans ? ntrans * (int64_t)idx_bytes : 0; }
 };
 
 struct DevBuf {
@@ -133,6 +138,11 @@ struct Context {
 
 Context &ctx();
 int ensure_init();
+
+// Kernel launches the library has made since it was loaded (reported by egg_launch_count).
+extern std::atomic<long long> g_launches;
+inline void count_launch(long long n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
 int ensure_buf(DevBuf &b, size_t bytes);
 DevPlan *find_plan(int K, int idx_bytes);
 
@@ -143,8 +153,16 @@ inline int pair_bits(int idx_bytes) { return idx_bytes == 4 ? 9 : 12; }
 // ---- entry points implemented per file ----------------------------------------------------------
 
 // egg_plan.cu
-int plan_build_device(int K, int idx_bytes, DevPlan &out);
+// Level table of the degree-K plan (no device memory: the plan is closed-form).
+int plan_levels(int K, int idx_bytes, DevPlan &out);
+// Write the closed-form plan's packed transitions into dst (ntrans entries of idx_bytes).
+int plan_materialize(const DevPlan &p, void *dst, cudaStream_t st);
+// Whether an explicit plan's transitions equal the closed-form layout, entry for entry.
+int plan_is_closed_form(const DevPlan &p, cudaStream_t st, bool *same);
 int plan_validate_device(const DevPlan &p, cudaStream_t st);
+// Saturated 32-bit binomial table C(n, k), n, k <= 64, row-major with row length 65, in device
+// memory (uploaded once; no allocation).
+const uint32_t *binom32_device(cudaStream_t st, int *rc);
 
 // egg_dp.cu
 int dp_run(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t B, void *dout, cudaStream_t st);

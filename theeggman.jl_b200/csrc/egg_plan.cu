@@ -4,7 +4,8 @@
 // every reachable mask by (popcount, mask), a Dict from mask to state number, and a CSR walk.
 // At K = 40 that is 2.84e9 transitions (22.7 GB as Int64) and needs about twice that in host RAM.
 //
-// Here the same layout is produced directly in HBM.  The reachable subsets have a closed form:
+// Here that layout is never stored: its closed form is enough to evaluate it (egg_dp.cu), to write
+// it out on request and to recognise it in an uploaded array.  The reachable subsets are:
 // S is reachable iff, with r = K - |S| removed, its minimum bit (0-based) is >= ceil(r/2)
 // (src/dp.jl:16-27: p - 1 <= r <= 2(p - 1)).  So the level of popcount c is exactly the set of all
 // c-subsets of the top U = K - ceil((K-c)/2) bit positions, and sorting by mask value within a level
@@ -24,15 +25,18 @@ static __device__ __forceinline__ int64_t pair_index(int64_t i, int64_t j, int64
 // Binomial table C(n, k) for n, k <= 64 (C(64, 32) < 2^63), staged per block in shared memory.
 __constant__ int64_t c_binom_dummy;  // keeps the constant bank initialised on every build
 
-template <class I>
+// Writes level c's transitions (CHECK = false) or counts the entries of `trans` that differ from
+// them (CHECK = true).
+template <class I, bool CHECK>
 __global__ void __launch_bounds__(256) plan_level_kernel(I *__restrict__ trans, const int64_t *__restrict__ binom_g,
                                                          int K, int c, int m0, int64_t n, int64_t toff,
-                                                         int64_t child_lo1, int bits)
+                                                         int64_t child_lo1, int bits, unsigned long long *diff)
 {
     __shared__ int64_t binom[65 * 65];
     for (int i = threadIdx.x; i < 65 * 65; i += blockDim.x) binom[i] = binom_g[i];
     __syncthreads();
     const int U = K - m0;  // level elements are the shifted positions 0..U-1
+    unsigned long long ndiff = 0;
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
         // Unrank s (colex) into c shifted elements e[1] < ... < e[c].
         int e[65];
@@ -57,10 +61,13 @@ __global__ void __launch_bounds__(256) plan_level_kernel(I *__restrict__ trans, 
         for (int j = 2; j <= c; ++j) {
             int64_t child = child_lo1 + pre + suf[j];
             int64_t jb = (int64_t)e[j] + m0 + 1;
-            out[j - 2] = (I)((child << bits) | pair_index(ib, jb, K));
+            const I v = (I)((child << bits) | pair_index(ib, jb, K));
+            if (CHECK) ndiff += out[j - 2] != v;
+            else out[j - 2] = v;
             pre += binom[(e[j] - 1) * 65 + (j - 1)];
         }
     }
+    if (CHECK && ndiff) atomicAdd(diff, ndiff);
 }
 
 static void host_binom(std::vector<int64_t> &t)
@@ -75,15 +82,15 @@ static void host_binom(std::vector<int64_t> &t)
     }
 }
 
-int plan_build_device(int K, int idx_bytes, DevPlan &p)
+int plan_levels(int K, int idx_bytes, DevPlan &p)
 {
-    Context &cx = ctx();
     int64_t ns, nt;
     dp_counts(K, ns, nt);
     p.K = K;
     p.idx_bytes = idx_bytes;
     p.nstates = ns;
     p.ntrans = nt;
+    p.trans = nullptr;
     std::vector<int64_t> binom;
     host_binom(binom);
     // Levels: popcount c = 0, 2, ..., K.
@@ -105,51 +112,89 @@ int plan_build_device(int K, int idx_bytes, DevPlan &p)
     }
     p.level_starts.push_back(lo + 1);
     if (lo != ns || toff != nt) return fail(EGG_ERR_PLAN_INVALID, "closed-form level sizes disagree with _dp_counts");
-    size_t bytes = (size_t)nt * idx_bytes;
-    size_t free_b = 0, total_b = 0;
-    EGG_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-    if (bytes + ((size_t)1 << 28) > free_b)
-        return fail(EGG_ERR_TOO_LARGE, "a degree-" + std::to_string(K) + " plan needs " + std::to_string(bytes) +
-                                           " device bytes; " + std::to_string(free_b) + " are free");
-    cudaError_t e = cudaMalloc(&p.trans, bytes ? bytes : 16);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(EGG_ERR_TOO_LARGE, std::string("plan allocation failed: ") + cudaGetErrorString(e));
-    }
+    return EGG_OK;
+}
+
+// Runs plan_level_kernel over every level of p into (CHECK = false) or against (CHECK = true) dst.
+template <bool CHECK>
+static int run_plan_kernels(const DevPlan &p, void *dst, cudaStream_t st, unsigned long long *ddiff)
+{
+    Context &cx = ctx();
+    std::vector<int64_t> binom;
+    host_binom(binom);
     int64_t *dbinom = nullptr;
-    e = cudaMalloc(&dbinom, binom.size() * sizeof(int64_t));
-    if (e != cudaSuccess) {
-        cudaFree(p.trans);
-        p.trans = nullptr;
-        return fail(EGG_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    }
-    int rc = EGG_OK;
-    e = cudaMemcpyAsync(dbinom, binom.data(), binom.size() * sizeof(int64_t), cudaMemcpyHostToDevice, cx.stream);
-    int bits = pair_bits(idx_bytes);
+    EGG_CUDA_TRY(cudaMalloc(&dbinom, binom.size() * sizeof(int64_t)));
+    cudaError_t e = cudaMemcpyAsync(dbinom, binom.data(), binom.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+    const int bits = pair_bits(p.idx_bytes);
     for (size_t L = 1; e == cudaSuccess && L < p.levels.size(); ++L) {
         const Level &lv = p.levels[L];
-        int c = 2 * (int)L;
-        int m0 = (K - c + 1) / 2;
+        const int c = 2 * (int)L;
+        const int m0 = (p.K - c + 1) / 2;
         int64_t blocks = (lv.n + 255) / 256;
-        int64_t cap = (int64_t)cx.num_sms * 16;
+        const int64_t cap = (int64_t)cx.num_sms * 16;
         if (blocks > cap) blocks = cap;
-        int64_t child_lo1 = p.levels[L - 1].lo + 1;
-        if (idx_bytes == 4)
-            plan_level_kernel<int32_t><<<(unsigned)blocks, 256, 0, cx.stream>>>((int32_t *)p.trans, dbinom, K, c, m0, lv.n,
-                                                                              lv.toff, child_lo1, bits);
+        const int64_t child_lo1 = p.levels[L - 1].lo + 1;
+        if (p.idx_bytes == 4)
+            plan_level_kernel<int32_t, CHECK><<<(unsigned)blocks, 256, 0, st>>>((int32_t *)dst, dbinom, p.K, c, m0, lv.n,
+                                                                               lv.toff, child_lo1, bits, ddiff);
         else
-            plan_level_kernel<int64_t><<<(unsigned)blocks, 256, 0, cx.stream>>>((int64_t *)p.trans, dbinom, K, c, m0, lv.n,
-                                                                              lv.toff, child_lo1, bits);
+            plan_level_kernel<int64_t, CHECK><<<(unsigned)blocks, 256, 0, st>>>((int64_t *)dst, dbinom, p.K, c, m0, lv.n,
+                                                                               lv.toff, child_lo1, bits, ddiff);
+        count_launch();
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(cx.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(dbinom);
-    if (e != cudaSuccess) {
-        cudaFree(p.trans);
-        p.trans = nullptr;
-        rc = fail(EGG_ERR_CUDA, std::string("plan build: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(EGG_ERR_CUDA, std::string("plan kernels: ") + cudaGetErrorString(e));
+    return EGG_OK;
+}
+
+int plan_materialize(const DevPlan &p, void *dst, cudaStream_t st) { return run_plan_kernels<false>(p, dst, st, nullptr); }
+
+int plan_is_closed_form(const DevPlan &p, cudaStream_t st, bool *same)
+{
+    *same = false;
+    if (!p.trans) return fail(EGG_ERR_ARGUMENT, "plan has no transition array to compare");
+    unsigned long long *ddiff = nullptr;
+    EGG_CUDA_TRY(cudaMalloc(&ddiff, sizeof(unsigned long long)));
+    cudaError_t e = cudaMemsetAsync(ddiff, 0, sizeof(unsigned long long), st);
+    int rc = e == cudaSuccess ? run_plan_kernels<true>(p, p.trans, st, ddiff)
+                              : fail(EGG_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+    unsigned long long diff = 1;
+    if (!rc) {
+        e = cudaMemcpy(&diff, ddiff, sizeof(diff), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(EGG_ERR_CUDA, std::string("plan compare: ") + cudaGetErrorString(e));
     }
+    cudaFree(ddiff);
+    if (!rc) *same = diff == 0;
     return rc;
+}
+
+// ---- the binomial table the closed-form DP kernels read ----------------------------------------
+
+static __device__ uint32_t g_binom32[65 * 65];
+static std::mutex g_binom32_mu;
+static const uint32_t *g_binom32_addr = nullptr;
+
+const uint32_t *binom32_device(cudaStream_t st, int *rc)
+{
+    std::lock_guard<std::mutex> lk(g_binom32_mu);
+    *rc = EGG_OK;
+    if (g_binom32_addr) return g_binom32_addr;
+    std::vector<int64_t> b;
+    host_binom(b);
+    static uint32_t h[65 * 65];
+    for (int i = 0; i < 65 * 65; ++i) h[i] = b[i] > (int64_t)UINT32_MAX ? UINT32_MAX : (uint32_t)b[i];
+    void *addr = nullptr;
+    cudaError_t e = cudaMemcpyToSymbolAsync(g_binom32, h, sizeof(h), 0, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaGetSymbolAddress(&addr, g_binom32);
+    if (e != cudaSuccess || !addr) {
+        *rc = fail(EGG_ERR_CUDA, std::string("binomial table upload: ") + cudaGetErrorString(e));
+        return nullptr;
+    }
+    g_binom32_addr = (const uint32_t *)addr;
+    return g_binom32_addr;
 }
 
 // Structure check for a plan that came from the host: every transition of level L must name a
@@ -191,6 +236,7 @@ int plan_validate_device(const DevPlan &p, cudaStream_t st)
         else
             plan_check_kernel<int64_t><<<(unsigned)blocks, 256, 0, st>>>((const int64_t *)p.trans, lv.toff, cnt, clo, chi,
                                                                        npairs, bits, dbad);
+        count_launch();
         e = cudaGetLastError();
     }
     unsigned long long bad = 0;

@@ -653,11 +653,13 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             sieve_exact_kernel<false><<<grid, ex_wpb * 32, smem, st>>>(a, ex_wpb);
         }
+        count_launch();
         ps.p[0] = a.partial;
         ps.w[0] = a.warps_per_inst;
     }
     if (cplx) sieve_reduce_kernel<true><<<(unsigned)B, 256, 0, st>>>(ps, a.inst, dout);
     else sieve_reduce_kernel<false><<<(unsigned)B, 256, 0, st>>>(ps, a.inst, dout);
+    count_launch();
     EGG_CUDA_TRY(cudaGetLastError());
     return EGG_OK;
 }

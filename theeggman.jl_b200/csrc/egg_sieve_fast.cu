@@ -602,6 +602,7 @@ static int launch_one(const SieveArgs &a, const int64_t *strides, dim3 grid, int
     auto k = sieve_fast_kernel<CPLX, MLO, MHI>;
     EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<grid, wpb * 32, smem, st>>>(a, strides, wpb, partial);
+    count_launch();
     EGG_CUDA_TRY(cudaGetLastError());
     return EGG_OK;
 }
