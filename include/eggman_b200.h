@@ -177,6 +177,27 @@ int egg_sieve_batch(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax
 int egg_sieve_batch_device(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax, const int64_t *E,
                            const int64_t *edge_reps, const int32_t *glynn, void *out, void *stream);
 
+/* ---- mixed-degree batches -------------------------------------------------------------- */
+
+/* Hafnians of B principal submatrices of one parent: instance b is A[r, r] with
+ * r = rows[offsets[b] .. offsets[b+1]), 0-based indices into the n x n column-major parent A
+ * (dtype EGG_F64, EGG_C128, or EGG_I64 for exact Int128 results; repeated indices act as repeated
+ * rows, as in hafnian_repeated).  Degrees may differ from instance to instance: the instances are
+ * binned by degree, their pair vectors gathered on the device and each bin runs the subset DP of
+ * its degree, so each result equals hafnian(A[r, r]; method = :dp) in the same precision mode.
+ * Odd |r| gives 0 and empty r gives 1.  offsets has B + 1 entries, offsets[0] = 0; out receives
+ * B values (EGG_I64: B Int128 values).  Row indices outside [0, n) are refused.
+ * No counterpart in the reference, whose batch form takes one degree per call
+ * (hafnian(As), src/hafnian.jl:1263-1301). */
+int egg_dp_mix(int dtype, int prec, const void *A, int64_t n, int64_t B, const int64_t *offsets, const int32_t *rows,
+               void *out);
+
+/* Same, with A, rows and out in device memory (offsets on the host, where the binning runs),
+ * enqueued on `stream`.  Row indices outside [0, n) are not read; those pairs are NaN (0 for
+ * integers).  No counterpart in the reference. */
+int egg_dp_mix_device(int dtype, int prec, const void *A, int64_t n, int64_t B, const int64_t *offsets, const int32_t *rows,
+                      void *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

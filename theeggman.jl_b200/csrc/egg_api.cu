@@ -104,6 +104,22 @@ using namespace egg;
         if (rc_) return rc_;                                \
     } while (0)
 
+static int check_layout(int K, int idx_bytes);
+
+DevPlan *egg::dp_plan_for(int K, int *rc)
+{
+    const int ib = K <= 32 ? 4 : 8;  // _dp_index_type: Int32 through DP_MAX = 32 (src/dp.jl:180)
+    DevPlan *p = find_plan(K, ib);
+    if (p) return p;
+    *rc = check_layout(K, ib);
+    if (*rc) return nullptr;
+    DevPlan np;
+    *rc = plan_levels(K, ib, np);
+    if (*rc) return nullptr;
+    ctx().plans[{K, ib}] = std::move(np);
+    return find_plan(K, ib);
+}
+
 static int check_layout(int K, int idx_bytes)
 {
     // The reference's refusals, src/dp.jl:224-234.
@@ -476,6 +492,51 @@ int egg_sieve_batch_device(int dtype, int prec, int64_t B, int64_t Emax, const v
         if (E[b] < 0 || E[b] > Emax) return fail(EGG_ERR_DIMENSION, "instance edge count exceeds Emax");
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
     return sieve_batch_run(dtype, prec, B, Emax, Ax, E, edge_reps, glynn, out, st);
+}
+
+int egg_dp_mix(int dtype, int prec, const void *A, int64_t n, int64_t B, const int64_t *offsets, const int32_t *rows,
+               void *out)
+{
+    EGG_GUARD();
+    if (B < 0 || n < 0) return fail(EGG_ERR_ARGUMENT, "negative size");
+    if (B == 0) return EGG_OK;
+    if (!offsets || !out || (n > 0 && !A)) return fail(EGG_ERR_ARGUMENT, "null argument");
+    if (offsets[0] != 0) return fail(EGG_ERR_ARGUMENT, "offsets[0] must be 0");
+    const int64_t nrows = offsets[B];
+    if (nrows < 0) return fail(EGG_ERR_ARGUMENT, "row-set boundaries must not decrease");
+    if (nrows > 0 && !rows) return fail(EGG_ERR_ARGUMENT, "null rows");
+    for (int64_t i = 0; i < nrows; ++i)
+        if (rows[i] < 0 || rows[i] >= n)
+            return fail(EGG_ERR_ARGUMENT, "row index " + std::to_string(rows[i]) + " outside the " + std::to_string(n) +
+                                              " x " + std::to_string(n) + " parent");
+    const size_t es = dtype_size(dtype);
+    if (!es) return fail(EGG_ERR_ARGUMENT, "unknown dtype");
+    const size_t oes = dtype == EGG_I64 ? 16 : es;
+    Context &c = ctx();
+    const size_t abytes = (size_t)n * n * es, offr = (abytes + 255) / 256 * 256;
+    const size_t offo = offr + ((size_t)nrows * 4 + 255) / 256 * 256;
+    int rc = ensure_buf(c.scratch[7], offo + (size_t)B * oes);
+    if (rc) return rc;
+    char *base = (char *)c.scratch[7].ptr;
+    if (abytes) EGG_CUDA_TRY(cudaMemcpyAsync(base, A, abytes, cudaMemcpyHostToDevice, c.stream));
+    if (nrows) EGG_CUDA_TRY(cudaMemcpyAsync(base + offr, rows, (size_t)nrows * 4, cudaMemcpyHostToDevice, c.stream));
+    rc = mix_run(dtype, prec, base, n, B, offsets, (const int32_t *)(base + offr), base + offo, c.stream);
+    if (rc) return rc;
+    EGG_CUDA_TRY(cudaMemcpyAsync(out, base + offo, (size_t)B * oes, cudaMemcpyDeviceToHost, c.stream));
+    EGG_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    return EGG_OK;
+}
+
+int egg_dp_mix_device(int dtype, int prec, const void *A, int64_t n, int64_t B, const int64_t *offsets, const int32_t *rows,
+                      void *out, void *stream)
+{
+    EGG_GUARD();
+    if (B < 0 || n < 0) return fail(EGG_ERR_ARGUMENT, "negative size");
+    if (B == 0) return EGG_OK;
+    if (!offsets || !out || (n > 0 && !A) || (offsets[B] > 0 && !rows)) return fail(EGG_ERR_ARGUMENT, "null argument");
+    if (offsets[0] != 0) return fail(EGG_ERR_ARGUMENT, "offsets[0] must be 0");
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+    return mix_run(dtype, prec, A, n, B, offsets, rows, out, st);
 }
 
 }  // extern "C"

@@ -18,59 +18,9 @@
 // evaluates the CPU loop, so results are bit-identical to the reference's _haf_dp.  EGG_PREC_FMA
 // contracts each multiply-add as the reference's GPU kernel does.  EGG_PREC_MIXED multiplies in
 // FP32 and accumulates each state in FP64.  Integer inputs run exactly in Int128.
-#include "egg_internal.cuh"
+#include "egg_dp_common.cuh"
 
 namespace egg {
-
-struct ExactOp {};
-struct FmaOp {};
-struct MixedOp {};
-struct IntOp {};
-
-template <class A> __device__ __forceinline__ A zero_of();
-template <> __device__ __forceinline__ double zero_of<double>() { return 0.0; }
-template <> __device__ __forceinline__ float zero_of<float>() { return 0.0f; }
-template <> __device__ __forceinline__ cd zero_of<cd>() { return cd{0.0, 0.0}; }
-template <> __device__ __forceinline__ cf zero_of<cf>() { return cf{0.0f, 0.0f}; }
-template <> __device__ __forceinline__ __int128 zero_of<__int128>() { return 0; }
-
-template <class A> __device__ __forceinline__ A one_of();
-template <> __device__ __forceinline__ double one_of<double>() { return 1.0; }
-template <> __device__ __forceinline__ float one_of<float>() { return 1.0f; }
-template <> __device__ __forceinline__ cd one_of<cd>() { return cd{1.0, 0.0}; }
-template <> __device__ __forceinline__ cf one_of<cf>() { return cf{1.0f, 0.0f}; }
-template <> __device__ __forceinline__ __int128 one_of<__int128>() { return 1; }
-
-// madd(op, acc, p, h) = acc + p*h in the op's rounding.
-__device__ __forceinline__ double madd(ExactOp, double a, double p, double h) { return x_madd(a, p, h); }
-__device__ __forceinline__ float madd(ExactOp, float a, float p, float h) { return x_madd(a, p, h); }
-__device__ __forceinline__ cd madd(ExactOp, cd a, cd p, cd h) { return x_madd(a, p, h); }
-__device__ __forceinline__ cf madd(ExactOp, cf a, cf p, cf h) { return x_madd(a, p, h); }
-__device__ __forceinline__ double madd(FmaOp, double a, double p, double h) { return f_madd(a, p, h); }
-__device__ __forceinline__ float madd(FmaOp, float a, float p, float h) { return f_madd(a, p, h); }
-__device__ __forceinline__ cd madd(FmaOp, cd a, cd p, cd h) { return f_madd(a, p, h); }
-__device__ __forceinline__ cf madd(FmaOp, cf a, cf p, cf h) { return f_madd(a, p, h); }
-__device__ __forceinline__ double madd(MixedOp, double a, float p, float h) { return __dadd_rn(a, (double)__fmul_rn(p, h)); }
-__device__ __forceinline__ cd madd(MixedOp, cd a, cf p, cf h)
-{
-    cf t = x_cmul(p, h);
-    a.re = __dadd_rn(a.re, (double)t.re);
-    a.im = __dadd_rn(a.im, (double)t.im);
-    return a;
-}
-__device__ __forceinline__ __int128 madd(IntOp, __int128 a, int64_t p, __int128 h) { return a + (__int128)p * h; }
-
-// Storage conversions from the accumulator.
-__device__ __forceinline__ void store(double &d, double a) { d = a; }
-__device__ __forceinline__ void store(float &d, float a) { d = a; }
-__device__ __forceinline__ void store(float &d, double a) { d = __double2float_rn(a); }
-__device__ __forceinline__ void store(cd &d, cd a) { d = a; }
-__device__ __forceinline__ void store(cf &d, cf a) { d = a; }
-__device__ __forceinline__ void store(cf &d, cd a) { d = cf{__double2float_rn(a.re), __double2float_rn(a.im)}; }
-__device__ __forceinline__ void store(__int128 &d, __int128 a) { d = a; }
-
-// Transitions whose loads a thread issues together before accumulating them in order.
-static constexpr int kBatch = 8;
 
 // One level: states [0, n) of the level, out-degree deg, transitions from toff.  Hprev holds
 // level L-1 (child numbers are 1-based global, child_lo1 = first state of L-1, 1-based).
@@ -180,114 +130,132 @@ __global__ void __launch_bounds__(512) dp_small_kernel(const I *__restrict__ tra
 // out-degree c - 1; its j-th transition (j = 2..c, the order of the plan) pairs e1 with ej and
 // lands on S - {e1, ej}, whose rank in the level below is
 //     pre_j + suf_j,  pre_j = sum_{x=2}^{j-1} C(e_x - 1, x - 1),  suf_j = sum_{x=j+1}^{c} C(e_x - 1, x - 2).
-// Both sums are carried along the walk, so a transition costs two table lookups in shared memory
-// instead of an 8-byte load from HBM.  The arithmetic per state is that of the plan kernels, in
-// the same order, so results are identical.
+// Both sums are carried along the walk.  A table entry holds C(x, k) and C(x, k + 1) side by side,
+// so stepping to the next element takes one 8-byte shared-memory load: its C(e - 1, j - 1) leaves
+// suf now and its C(e - 1, j) joins pre one step later.  The arithmetic per state is that of the
+// plan kernels, in the same order, so results are identical.
 
-template <class M> __device__ __forceinline__ int low_bit(M v);
-template <> __device__ __forceinline__ int low_bit<uint32_t>(uint32_t v) { return __ffs((int)v) - 1; }
-template <> __device__ __forceinline__ int low_bit<uint64_t>(uint64_t v) { return __ffsll((long long)v) - 1; }
-
-// The colex-successor of a c-subset mask (the next larger integer with the same popcount).
-template <class M> __device__ __forceinline__ M colex_next(M v)
+// One step of the walk: load the child value and pair value for element ej, then advance
+// pre/suf/ej to the next element (if this is not the last step).
+template <class M, class PT, class HT, bool B1>
+__device__ __forceinline__ void walk_step(int x, int c, M &rest, uint32_t &pre, uint32_t &suf, uint32_t &padd, int &ej,
+                                          const uint2 *TP, int ld, int pb, const PT *P, const HT *Hprev, int64_t B,
+                                          int64_t b, HT &h, PT &p)
 {
-    const M t = v | (v - 1);
-    return (t + 1) | (((~t & (M)(0 - ~t)) - 1) >> (low_bit<M>(v) + 1));
-}
-
-// The c-subset of [0, U) with colex rank R; T[x * ld + k] = C(x, k) (saturated at 2^32 - 1, which
-// stays above every rank compared against it).
-template <class M>
-__device__ __forceinline__ M colex_unrank(const uint32_t *T, int ld, int U, int c, uint32_t R)
-{
-    M m = 0;
-    int x = U - 1;
-    for (int i = c; i >= 1; --i) {
-        uint32_t v;
-        while ((v = T[x * ld + i]) > R) --x;
-        m |= (M)1 << x;
-        R -= v;
-        --x;
+    const uint32_t child = pre + suf;
+    if (B1) {
+        h = Hprev[child];
+        p = P[pb + ej];
+    } else {
+        h = Hprev[(int64_t)child * B + b];
+        p = P[(int64_t)(pb + ej) * B + b];
     }
-    return m;
+    pre += padd;
+    if (x < c) {
+        const int en = low_bit<M>(rest);
+        rest &= rest - 1;
+        const uint2 t = TP[(en - 1) * ld + (x - 1)];
+        suf -= t.x;
+        padd = t.y;
+        ej = en;
+    }
 }
 
-// One state's value: sum over its transitions, in plan order, of P[pair] * H[child] (instance b
-// of B, instance-fastest; B1 when B == 1).  Hprev == nullptr stands for the level of the empty set
-// (value 1).  The loads of kBatch transitions are issued before any of them is used, so a state
-// waits for one memory round trip per batch rather than one per transition; the accumulation
-// order is unchanged.
-
+// One state's value (c >= 4): the sum over its transitions, in plan order, of P[pair] * H[child]
+// (instance b of B, instance-fastest; B1 when B == 1).  The loads of kBatch transitions are issued
+// before any of them is used, so a state waits for one memory round trip per batch rather than one
+// per transition; the accumulation order is unchanged.
 template <class Op, class M, class PT, class HT, class AT, bool B1>
-__device__ __forceinline__ AT walk_state(M m, const uint32_t *T, int ld, int c, int K, int m0, const PT *P,
+__device__ __forceinline__ AT walk_state(M m, const uint2 *TP, int ld, int c, int K, int m0, const PT *P,
                                          const HT *Hprev, int64_t B, int64_t b)
 {
     const int e1 = low_bit<M>(m);
     M rest = m & (m - 1);
-    uint32_t suf = 0;
+    const int e2 = low_bit<M>(rest);
+    rest &= rest - 1;  // e3..ec
+    uint32_t suf = 0;  // suf_2 = sum_{x=3}^{c} C(e_x - 1, x - 2)
     {
-        M r2 = rest & (rest - 1);
-        for (int x = 3; x <= c; ++x) {
-            const int e = low_bit<M>(r2);
-            r2 &= r2 - 1;
-            suf += T[(e - 1) * ld + (x - 2)];
+        M r = rest;
+        int x = 3;
+        for (; x + 3 <= c; x += 4) {
+            const int ea = low_bit<M>(r);
+            r &= r - 1;
+            const int eb = low_bit<M>(r);
+            r &= r - 1;
+            const int ecc = low_bit<M>(r);
+            r &= r - 1;
+            const int ed = low_bit<M>(r);
+            r &= r - 1;
+            suf += TP[(ea - 1) * ld + (x - 2)].x + TP[(eb - 1) * ld + (x - 1)].x + TP[(ecc - 1) * ld + x].x +
+                   TP[(ed - 1) * ld + (x + 1)].x;
+        }
+        for (; x <= c; ++x) {
+            const int e = low_bit<M>(r);
+            r &= r - 1;
+            suf += TP[(e - 1) * ld + (x - 2)].x;
         }
     }
     // 0-based _pair_index(e1 + m0 + 1, ej + m0 + 1, K) - 1 = pb + ej (src/unrolled.jl:60).
     const int ib = e1 + m0 + 1;
     const int pb = (ib - 1) * K - (ib * (ib + 1)) / 2 + m0;
     uint32_t pre = 0;
-    int ej = low_bit<M>(rest);
-    rest &= rest - 1;
+    uint32_t padd = TP[(e2 - 1) * ld].y;  // C(e2 - 1, 1): joins pre after the first step
+    int ej = e2;
     AT acc = zero_of<AT>();
-    for (int x0 = 2; x0 <= c; x0 += kBatch) {
+    int x = 2;
+    for (; x + kBatch - 1 <= c; x += kBatch) {
         HT hv[kBatch];
         PT pv[kBatch];
 #pragma unroll
-        for (int u = 0; u < kBatch; ++u) {
-            const int x = x0 + u;
-            if (x <= c) {
-                const uint32_t child = pre + suf;
-                if (B1) {
-                    hv[u] = Hprev ? Hprev[child] : one_of<HT>();
-                    pv[u] = P[pb + ej];
-                } else {
-                    hv[u] = Hprev ? Hprev[(int64_t)child * B + b] : one_of<HT>();
-                    pv[u] = P[(int64_t)(pb + ej) * B + b];
-                }
-                pre += T[(ej - 1) * ld + (x - 1)];
-                if (x < c) {
-                    const int en = low_bit<M>(rest);
-                    rest &= rest - 1;
-                    suf -= T[(en - 1) * ld + (x - 1)];
-                    ej = en;
-                }
-            }
-        }
+        for (int u = 0; u < kBatch; ++u)
+            walk_step<M, PT, HT, B1>(x + u, c, rest, pre, suf, padd, ej, TP, ld, pb, P, Hprev, B, b, hv[u], pv[u]);
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) acc = madd(Op{}, acc, pv[u], hv[u]);
+    }
+    if (x <= c) {
+        HT hv[kBatch];
+        PT pv[kBatch];
 #pragma unroll
         for (int u = 0; u < kBatch; ++u)
-            if (x0 + u <= c) acc = madd(Op{}, acc, pv[u], hv[u]);
+            if (x + u <= c)
+                walk_step<M, PT, HT, B1>(x + u, c, rest, pre, suf, padd, ej, TP, ld, pb, P, Hprev, B, b, hv[u], pv[u]);
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u)
+            if (x + u <= c) acc = madd(Op{}, acc, pv[u], hv[u]);
     }
     return acc;
 }
 
-// One level of a closed-form plan.  Each block takes chunks of run * 256 consecutive states
-// (run <= kRun, smaller for small levels so that every SM gets blocks): first every thread writes
-// the masks of `run` consecutive states into shared memory (one unrank, then colex successors),
-// then the threads walk the chunk's (state, instance) pairs with consecutive threads on
-// consecutive pairs, so a warp's child loads fall on a few neighbouring sectors.
-static constexpr int kRun = 8;
-static constexpr int kLevelThreads = 256;
-
-template <class M, class PT>
-static size_t level_smem(int K, int c, int64_t B)
+// Level c = 2: state s = {e1 < e2} (colex rank C(e2, 2) + e1) has the single transition to the
+// empty set, whose value is 1.
+template <class Op, class PT, class HT, class AT>
+__device__ __forceinline__ HT first_level_value(int64_t s, int K, const PT *P, int64_t B, int64_t b)
 {
-    const int m0 = (K - c) / 2, U = K - m0;
-    size_t bytes = (size_t)kRun * kLevelThreads * sizeof(M) + (((size_t)U * (c + 1) * 4 + 15) / 16) * 16;
-    if (B == 1) bytes += (size_t)K * (K - 1) / 2 * sizeof(PT);
-    return bytes;
+    const int m0 = (K - 2) / 2;
+    int e2 = (int)((1.0 + sqrt(1.0 + 8.0 * (double)s)) * 0.5);
+    while ((int64_t)e2 * (e2 - 1) / 2 > s) --e2;
+    while ((int64_t)(e2 + 1) * e2 / 2 <= s) ++e2;
+    const int e1 = (int)(s - (int64_t)e2 * (e2 - 1) / 2);
+    const int ib = e1 + m0 + 1;
+    const int q = (ib - 1) * K - (ib * (ib + 1)) / 2 + m0 + e2;
+    HT out;
+    store(out, madd(Op{}, zero_of<AT>(), P[(int64_t)q * B + b], one_of<HT>()));
+    return out;
 }
 
+template <class Op, class PT, class HT, class AT>
+__global__ void __launch_bounds__(256) dpc_first_kernel(const PT *__restrict__ P, HT *__restrict__ Hcur, int K, int64_t n,
+                                                        int64_t B)
+{
+    const int64_t total = n * B;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = g / B, b = g - s * B;
+        Hcur[g] = first_level_value<Op, PT, HT, AT>(s, K, P, B, b);
+    }
+}
+
+// One level (c >= 4) of a closed-form plan, for levels without a fixed-popcount kernel
+// (egg_dp_fixed.cuh): the same two phases with the popcount a runtime value.
 template <class Op, class M, class PT, class HT, class AT, bool B1>
 __global__ void __launch_bounds__(kLevelThreads) dpc_level_kernel(const uint32_t *__restrict__ binom, const PT *__restrict__ P,
                                                                   const HT *__restrict__ Hprev, HT *__restrict__ Hcur,
@@ -296,9 +264,9 @@ __global__ void __launch_bounds__(kLevelThreads) dpc_level_kernel(const uint32_t
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int m0 = (K - c) / 2, U = K - m0, ld = c + 1;
     M *masks = reinterpret_cast<M *>(smem_raw);
-    uint32_t *T = reinterpret_cast<uint32_t *>(masks + kRun * kLevelThreads);
-    PT *Ps = reinterpret_cast<PT *>(smem_raw + (size_t)kRun * kLevelThreads * sizeof(M) + (((size_t)U * ld * 4 + 15) / 16) * 16);
-    for (int i = threadIdx.x; i < U * ld; i += kLevelThreads) T[i] = binom[(i / ld) * 65 + (i % ld)];
+    uint2 *TP = reinterpret_cast<uint2 *>(smem_raw + (size_t)kRun * kLevelThreads * sizeof(M));
+    PT *Ps = reinterpret_cast<PT *>(smem_raw + level_pairs_offset<M>(U, ld));
+    fill_pair_table(TP, binom, U, ld, threadIdx.x, kLevelThreads);
     const int npairs = K * (K - 1) / 2;
     if (B1)
         for (int q = threadIdx.x; q < npairs; q += kLevelThreads) Ps[q] = P[q];
@@ -311,7 +279,7 @@ __global__ void __launch_bounds__(kLevelThreads) dpc_level_kernel(const uint32_t
         const int cnt = (int)(n - s0 < chunk ? n - s0 : chunk);
         const int r0 = threadIdx.x * run;
         if (r0 < cnt) {
-            M m = colex_unrank<M>(T, ld, U, c, (uint32_t)(s0 + r0));
+            M m = colex_unrank<M>(TP, ld, U, c, (uint32_t)(s0 + r0));
             masks[r0] = m;
             for (int r = 1; r < run && r0 + r < cnt; ++r) {
                 m = colex_next<M>(m);
@@ -330,7 +298,7 @@ __global__ void __launch_bounds__(kLevelThreads) dpc_level_kernel(const uint32_t
                 sl = (int)(i / B);
                 b = i - (int64_t)sl * B;
             }
-            const AT acc = walk_state<Op, M, PT, HT, AT, B1>(masks[sl], T, ld, c, K, m0, Pp, Hprev, B, b);
+            const AT acc = walk_state<Op, M, PT, HT, AT, B1>(masks[sl], TP, ld, c, K, m0, Pp, Hprev, B, b);
             store(Hcur[(s0 + sl) * B + b], acc);
         }
         __syncthreads();
@@ -342,7 +310,7 @@ __global__ void __launch_bounds__(kLevelThreads) dpc_level_kernel(const uint32_t
 // run of consecutive states of a level (one unrank, then successors) and walks each in turn.
 template <class Op, class PT, class HT, class AT, int MAXT>
 __global__ void __launch_bounds__(MAXT) dpc_small_kernel(const uint32_t *__restrict__ binom, const PT *__restrict__ P,
-                                                        HT *__restrict__ out, int64_t B, int K, int maxlev)
+                                                         HT *__restrict__ out, int64_t B, int K, int maxlev)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     HT *H0 = reinterpret_cast<HT *>(smem_raw);
@@ -350,23 +318,28 @@ __global__ void __launch_bounds__(MAXT) dpc_small_kernel(const uint32_t *__restr
     PT *Ps = reinterpret_cast<PT *>(H1 + maxlev);
     const int npairs = K * (K - 1) / 2;
     const int ld = K + 1;
-    uint32_t *T = reinterpret_cast<uint32_t *>(smem_raw + (((size_t)2 * maxlev * sizeof(HT) + (size_t)npairs * sizeof(PT) + 15) / 16) * 16);
-    for (int i = threadIdx.x; i < ld * ld; i += blockDim.x) T[i] = binom[(i / ld) * 65 + (i % ld)];
+    uint2 *TP = reinterpret_cast<uint2 *>(smem_raw + (((size_t)2 * maxlev * sizeof(HT) + (size_t)npairs * sizeof(PT) + 15) / 16) * 16);
+    fill_pair_table(TP, binom, ld, ld, threadIdx.x, blockDim.x);
     for (int64_t b = blockIdx.x; b < B; b += gridDim.x) {
         for (int q = threadIdx.x; q < npairs; q += blockDim.x) Ps[q] = P[(int64_t)q * B + b];
         __syncthreads();
-        for (int c = 2; c <= K; c += 2) {
-            const HT *prev = c == 2 ? nullptr : (((c / 2) & 1) ? H0 : H1);
+        {
+            const int n = (K / 2 + 1) * (K / 2) / 2;  // level c = 2
+            for (int s = threadIdx.x; s < n; s += blockDim.x) H1[s] = first_level_value<Op, PT, HT, AT>(s, K, Ps, 1, 0);
+        }
+        __syncthreads();
+        for (int c = 4; c <= K; c += 2) {
+            const HT *prev = ((c / 2) & 1) ? H0 : H1;
             HT *cur = ((c / 2) & 1) ? H1 : H0;
             const int m0 = (K - c) / 2, U = K - m0;
-            const int n = (int)T[U * ld + c];
+            const int n = (int)TP[U * ld + c].x;
             const int per = (n + (int)blockDim.x - 1) / (int)blockDim.x;
             const int r0 = threadIdx.x * per;
             if (r0 < n) {
-                uint32_t m = colex_unrank<uint32_t>(T, ld, U, c, (uint32_t)r0);
+                uint32_t m = colex_unrank<uint32_t>(TP, ld, U, c, (uint32_t)r0);
                 for (int r = 0; r < per && r0 + r < n; ++r) {
                     if (r) m = colex_next<uint32_t>(m);
-                    store(cur[r0 + r], walk_state<Op, uint32_t, PT, HT, AT, true>(m, T, ld, c, K, m0, Ps, prev, 1, 0));
+                    store(cur[r0 + r], walk_state<Op, uint32_t, PT, HT, AT, true>(m, TP, ld, c, K, m0, Ps, prev, 1, 0));
                 }
             }
             __syncthreads();
@@ -477,7 +450,7 @@ static size_t closed_small_smem(const DevPlan &plan)
     const int64_t maxlev = max_level(plan);
     const int64_t npairs = (int64_t)plan.K * (plan.K - 1) / 2;
     size_t bytes = (((size_t)2 * maxlev * sizeof(HT) + (size_t)npairs * sizeof(PT) + 15) / 16) * 16 +
-                   (size_t)(plan.K + 1) * (plan.K + 1) * 4;
+                   (size_t)(plan.K + 1) * (plan.K + 1) * sizeof(uint2);
     return bytes <= 160 * 1024 ? bytes : 0;
 }
 
@@ -507,6 +480,9 @@ static int launch_closed_level(const uint32_t *bt, const PT *P, const HT *prev, 
     int64_t blocks = (n + chunk - 1) / chunk;
     const int64_t cap = (int64_t)ctx().num_sms * 8;
     if (blocks > cap) blocks = cap;
+    if constexpr (has_fixed<Op, PT>::value) {
+        if (B == 1 && fixed_level<Op, PT, HT, AT>(bt, P, prev, cur, K, c, n, run, (int)blocks, st)) return EGG_OK;
+    }
     k<<<(unsigned)blocks, kLevelThreads, sm, st>>>(bt, P, prev, cur, K, c, n, B, run);
     count_launch();
     return EGG_OK;
@@ -540,9 +516,14 @@ static int run_closed(const DevPlan &plan, const PT *P, HT *h0, HT *h1, HT *out,
     for (int64_t L = 0; L < (int64_t)plan.levels.size(); ++L)
         if (plan.levels[L].n >= ((int64_t)1 << 31))
             return fail(EGG_ERR_TOO_LARGE, "a level of the degree-" + std::to_string(K) + " plan has 2^31 states or more");
-    const HT *prev = nullptr;  // the empty set's level: value 1
     const int nlev = (int)plan.levels.size();
-    for (int L = 1; L < nlev; ++L) {
+    HT *prev = (1 == nlev - 1 && out_direct) ? out : h1;  // level c = 2 lands in h1 (odd level)
+    {
+        const int64_t total = plan.levels[1].n * B;
+        dpc_first_kernel<Op, PT, HT, AT><<<grid_for(total, 256), 256, 0, st>>>(P, prev, K, plan.levels[1].n, B);
+        count_launch();
+    }
+    for (int L = 2; L < nlev; ++L) {
         const int c = 2 * L;
         HT *cur = (L == nlev - 1 && out_direct) ? out : ((L & 1) ? h1 : h0);
         const int U = K - (K - c) / 2;

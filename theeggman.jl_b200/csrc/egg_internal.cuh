@@ -132,7 +132,8 @@ struct Context {
     cudaStream_t stream = nullptr;
     int num_sms = 0;
     std::map<std::pair<int, int>, DevPlan> plans;
-    DevBuf scratch[6];   // H, P, out, misc...: grown on demand, never shrunk
+    DevBuf scratch[8];   // H, P, out, sieve matrix, sieve out, misc, mixed-degree batch + its staging:
+                         // grown on demand, never shrunk
     std::recursive_mutex mu;
 };
 
@@ -165,8 +166,17 @@ int plan_validate_device(const DevPlan &p, cudaStream_t st);
 const uint32_t *binom32_device(cudaStream_t st, int *rc);
 
 // egg_dp.cu
+// The resident plan for degree K in the layout the reference picks for it (Int32 up to K = 32),
+// made resident (closed form) if absent.
+DevPlan *dp_plan_for(int K, int *rc);
 int dp_run(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t B, void *dout, cudaStream_t st);
 size_t dp_scratch_bytes(const DevPlan &plan, int dtype, int prec, int64_t B);
+
+// egg_mix.cu
+// Hafnians of the principal submatrices A[r, r], r = rows[offsets[b]..offsets[b+1]), of the n x n
+// column-major parent A: A, rows and out in device memory, offsets on the host.
+int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int64_t *offsets, const int32_t *drows,
+            void *dout, cudaStream_t st);
 
 // egg_sieve.cu
 // A caller-provided device region for the sieve's tables and partial sums (used instead of the

@@ -462,6 +462,59 @@ def _hafnian_repeated_batch(A, rpts, *, nthreads, glynn, method, check_symmetric
     return out if exact_int else np.array(out, dtype=T)
 
 
+def _mix_layout(rows_list) -> tuple[np.ndarray, np.ndarray]:
+    """(offsets[B + 1] int64, concatenated rows int32) of a list of 0-based row-index sequences."""
+    sizes = np.fromiter((len(r) for r in rows_list), dtype=np.int64, count=len(rows_list))
+    offsets = np.zeros(len(rows_list) + 1, dtype=np.int64)
+    np.cumsum(sizes, out=offsets[1:])
+    flat = (np.concatenate([np.asarray(r, dtype=np.int64) for r in rows_list]) if offsets[-1]
+            else np.zeros(0, dtype=np.int64))
+    return offsets, np.ascontiguousarray(flat, dtype=np.int32)
+
+
+def hafnian_submatrices(A, rows_list, *, check_symmetric: bool = True, prec: str | None = None,
+                        exact: bool = False):
+    """Hafnians of the principal submatrices A[r, r] of one parent, one per 0-based row-index
+    sequence r in `rows_list`, in one device call whatever the mix of sizes.
+
+    Each result equals ``hafnian(A[np.ix_(r, r)], method="dp", prec=prec)`` (repeated indices act
+    as repeated rows, as in hafnian_repeated); odd sizes give 0 and empty ones 1.  Float64,
+    ComplexF64 or, with ``exact=True``, integer parents (Int128 results as Python ints).  The
+    reference has no counterpart: its batch form takes one size per call
+    (src/hafnian.jl:1263-1301).
+    """
+    A = np.asarray(A)
+    n = _checksquare(A)
+    if check_symmetric:
+        _check_symmetric(A)
+    exact_int = exact and A.dtype.kind in "iub"
+    if exact_int:
+        T, code = np.dtype(np.int64), nat.EGG_I64
+    else:
+        T = _haf_dtype(A)
+        T = np.dtype(np.complex128) if T.kind == "c" else np.dtype(np.float64)
+        code = nat.DTYPE_OF[T]
+    B = len(rows_list)
+    if B == 0:
+        return [] if exact_int else np.zeros(0, dtype=T)
+    offsets, flat = _mix_layout(rows_list)
+    Af = np.asfortranarray(A.astype(T, copy=False))
+    out = np.zeros(2 * B, np.uint64) if exact_int else np.zeros(B, T)
+    prec_name = _dp_prec(prec)
+    if prec_name not in nat.PREC:
+        raise ArgumentError(f"prec must be one of {tuple(nat.PREC)}")
+    with _lock:
+        nat.check(nat.lib().egg_dp_mix(code, nat.PREC[prec_name], nat.ptr(Af), n, B, nat.ptr(offsets),
+                                       nat.ptr(flat) if len(flat) else None, nat.ptr(out)))
+    if exact_int:
+        vals = []
+        for b in range(B):
+            v = int(out[2 * b]) | (int(out[2 * b + 1]) << 64)
+            vals.append(v - (1 << 128) if v >= (1 << 127) else v)
+        return vals
+    return out
+
+
 def reduction(A, rpt) -> np.ndarray:
     """A with row/column i repeated rpt[i] times (src/hafnian.jl:1369-1374)."""
     A = np.asarray(A)
