@@ -57,6 +57,11 @@ def measured_peaks() -> dict:
         return {}
 
 
+# The committed ncu summary (kernel and workload) whose DRAM traffic figure belongs to a workload.
+PROFILE_OF = {"sieve40": "sieve_fast_kernel_sieve40.md", "dp40": "dpc_fixed_kernel_dp40.md",
+              "dp32": "dpc_fixed_kernel_dp32.md"}
+
+
 def profile_traffic(name: str):
     """DRAM bytes per launch from a committed ncu summary (a line `dram_bytes_per_launch: X`)."""
     p = os.path.join(ROOT, "profiles", name)
@@ -208,14 +213,7 @@ class DPWorkload:
         return self.B * (16 if self.code in (1, 4) else 8)
 
     def roofline(self, ms, peaks):
-        from theeggman_b200 import roofline as R
-
-        byts = R.dp_bytes(self.N, self.B, self.vbytes)
-        peak = float(peaks.get("hbm_gbs", 6650.0))
-        achieved = byts / (ms / 1e3) / 1e9
-        return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
-                "work": f"{byts:.4e} algorithmic bytes per step (plan once + 2 states + pairs per instance)"}
+        return dp_roofline([(self.N, self.B)], self.vbytes, ms, peaks)
 
     def cpu_sample(self, nthreads):
         from oracle import oracle as O
@@ -244,6 +242,127 @@ class DPWorkload:
         t = time.perf_counter()
         O.haf_dp_batch(Psub, plan, dt, nthreads)
         return nb / (time.perf_counter() - t), f"{nb} instances through the reference's batch loop, all host threads"
+
+
+def dp_roofline(bins, vbytes, ms, peaks):
+    """HBM roofline of closed-form DP levels over (degree, instances) bins: compulsory bytes (each
+    state written once and read once, plus the pairs; no transition array exists to stream), with
+    the child-load bytes beside them."""
+    from theeggman_b200 import roofline as R
+
+    byts = sum(R.dp_bytes_closed(K, B, vbytes) for K, B in bins)
+    gath = sum(R.dp_gather_bytes(K, B, vbytes) for K, B in bins)
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = byts / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s",
+            "work": f"{byts:.4e} compulsory bytes per step (every state written once and read once, plus the pairs; "
+                    "closed-form plan, so no transition array is read)",
+            "child_load_bytes_per_step": gath, "child_load_GBps": gath / (ms / 1e3) / 1e9}
+
+
+class MixWorkload:
+    """Configuration 4: B hafnians of principal submatrices of one 64 x 64 complex GBS parent, each
+    of an even degree uniform in {8, ..., 32} with distinct rows, all in one call per step
+    (egg_dp_mix_device; `seq` instead makes one single-instance DP call per hafnian, the
+    one-at-a-time GPU path the batched form is compared with)."""
+
+    kind = "dp"
+
+    def __init__(self, egg, W, B: int, prec: str, seq: bool, seed: int):
+        from theeggman_b200.hafnian import _mix_layout
+
+        self.egg, self.B, self.prec_name, self.seq = egg, B, prec, seq
+        self.prec = {"exact": 0, "fma": 1, "mixed": 2}[prec]
+        self.A, self.idxs = W.gbs_mix(B, 64, range(8, 33, 2), seed)
+        self.offsets, self.flat = _mix_layout(self.idxs)
+        self.hafnians_per_step = B
+        self.dtype_name = "c128"
+        self.vbytes = 8 if prec == "mixed" else 16
+        degs = np.bincount([len(r) for r in self.idxs], minlength=65)
+        self.bins = [(K, int(degs[K])) for K in range(2, 65, 2) if degs[K]]
+        self.name = (f"config4: {B} hafnians of A[r, r], A = U diag(tanh r) U^T 64x64 complex (U Haar), |r| even "
+                     f"uniform in 8..32, distinct rows; prec={prec}; "
+                     + ("one single-instance DP call per hafnian" if seq else "one egg_dp_mix call per step"))
+
+    def setup_device(self, torch, dev):
+        from theeggman_b200.hafnian import _dp_plan, _gather_pairs_batch
+
+        self.dA = torch.from_numpy(np.ascontiguousarray(self.A.T)).to(dev, torch.complex128)
+        self.drows = torch.from_numpy(self.flat.astype(np.int32)).to(dev)
+        self.dout = torch.zeros(self.B, dtype=torch.complex128, device=dev)
+        if self.seq:
+            self.keys = {K: _dp_plan(K) for K, _ in self.bins}
+            self.dPs = [torch.from_numpy(np.ascontiguousarray(
+                _gather_pairs_batch(np.dtype(np.complex128), self.A, np.asarray(r)[None, :], len(r))[0])).to(dev)
+                for r in self.idxs]
+
+    def step_device(self, stream_ptr):
+        L = self.egg.lib()
+        if self.seq:
+            for b, r in enumerate(self.idxs):
+                K = len(r)
+                key = self.keys[K]
+                rc = L.egg_dp_batch_device(key[0], key[1], 1, self.prec, self.dPs[b].data_ptr(), 1,
+                                           self.dout.data_ptr() + 16 * b, stream_ptr)
+                if rc:
+                    raise RuntimeError(L.egg_last_error().decode())
+            return
+        rc = L.egg_dp_mix_device(1, self.prec, self.dA.data_ptr(), 64, self.B, self.offsets.ctypes.data,
+                                 self.drows.data_ptr(), self.dout.data_ptr(), stream_ptr)
+        if rc:
+            raise RuntimeError(L.egg_last_error().decode())
+
+    def step_e2e(self):
+        if self.seq:
+            return [self.egg.hafnian(self.A[np.ix_(r, r)], method="dp", check_symmetric=False, prec=self.prec_name)
+                    for r in self.idxs]
+        return self.egg.hafnian_submatrices(self.A, self.idxs, check_symmetric=False, prec=self.prec_name)
+
+    @property
+    def h2d_bytes(self):
+        if self.seq:  # each call copies its instance's pairs
+            return sum(16 * len(r) * (len(r) - 1) // 2 for r in self.idxs)
+        return self.A.nbytes + self.flat.nbytes + self.offsets.nbytes + 4 * self.B  # parent, rows, bounds, order
+
+    @property
+    def d2h_bytes(self):
+        return 16 * self.B
+
+    def roofline(self, ms, peaks):
+        return dp_roofline(self.bins, self.vbytes, ms, peaks)
+
+    def extra_config(self):
+        """The per-degree evaluation the library's tuner chose (degrees <= 22 run whole-instance)."""
+        import ctypes
+
+        if self.seq:
+            return {}
+        L = self.egg.lib()
+        tiles = {}
+        for K, _ in self.bins:
+            b, g = ctypes.c_int(), ctypes.c_int64()
+            if K > 22 and L.egg_dp_mix_tuning(K, 1, self.prec, ctypes.byref(b), ctypes.byref(g)) == 0:
+                tiles[str(K)] = f"{'batched' if b.value else 'grouped'} x{g.value}"
+        return {"tuned_tiles": tiles}
+
+    def cpu_sample(self, nthreads):
+        from oracle import oracle as O
+
+        # The reference loop over the mix, timed on up to 4 instances per degree and scaled by the
+        # degree counts.
+        total = 0.0
+        for K, cnt in self.bins:
+            rs = [r for r in self.idxs if len(r) == K][:4]
+            plan = O.build_plan(K, 4)
+            P = O.gather_pairs(self.A, [int(i) + 1 for i in rs[0]], K)
+            O.haf_dp_pairs(P, plan, O.C128, nthreads)
+            t = time.perf_counter()
+            for r in rs:
+                O.haf_dp_pairs(O.gather_pairs(self.A, [int(i) + 1 for i in r], K), plan, O.C128, nthreads)
+            total += (time.perf_counter() - t) / len(rs) * cnt
+        return self.B / total, ("the reference DP on up to 4 instances per degree, scaled by the degree counts "
+                                f"({len(self.bins)} degrees), all host threads")
 
 
 class RepeatedWorkload:
@@ -356,6 +475,12 @@ def make_workload(name: str, egg, W, rank: int):
         return DPWorkload(egg, W, 40, 1, "i64", "exact", 4041 + rank)
     if name == "dp20x1024":
         return DPWorkload(egg, W, 20, 1024, "c128", "exact", 7000 + rank)
+    if name == "mix4096":
+        return MixWorkload(egg, W, 4096, "exact", False, 4 + 100 * rank)
+    if name == "mix4096mixed":
+        return MixWorkload(egg, W, 4096, "mixed", False, 4 + 100 * rank)
+    if name == "mix4096seq":
+        return MixWorkload(egg, W, 4096, "exact", True, 4 + 100 * rank)
     if name == "rep14":
         return RepeatedWorkload(egg, W, "a", 1024, 5 + 100 * rank)
     if name == "rep20c":
@@ -545,14 +670,15 @@ def run_ours(args):
 
     peaks = measured_peaks()
     roof = wl.roofline(ms_max / args.steps, peaks)
-    roof["traffic"] = profile_traffic(f"{wl.kind}_{args.workload}.txt")
+    roof["traffic"] = profile_traffic(PROFILE_OF.get(args.workload, ""))
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "hafnians/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": wl.dtype_name, "data": "synthetic (seeded SplitMix64)",
             "config": {"workload": wl.name, "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       **(wl.extra_config() if hasattr(wl, "extra_config") else {})},
             "e2e": {"value": e2e_value, "unit": "hafnians/s", "h2d_bytes_per_step": wl.h2d_bytes,
                     "d2h_bytes_per_step": wl.d2h_bytes, "path": "the public API from host memory"},
             "roofline": roof,

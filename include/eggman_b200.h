@@ -198,6 +198,19 @@ int egg_dp_mix(int dtype, int prec, const void *A, int64_t n, int64_t B, const i
 int egg_dp_mix_device(int dtype, int prec, const void *A, int64_t n, int64_t B, const int64_t *offsets, const int32_t *rows,
                       void *out, void *stream);
 
+/* How the mixed-degree batch evaluates degree K in this dtype and precision mode, as chosen by
+ * timing the candidates on the first batch that had more than one instance of that degree:
+ * batched = 1 runs groups of `group` instances instance-fastest (one thread per state and
+ * instance); batched = 0 runs `group` single-instance evaluations side by side.  Degrees up to 22
+ * always run as one whole-instance launch per batch and are not tuned.  EGG_ERR_NO_PLAN if K has
+ * not been tuned yet.  No counterpart in the reference. */
+int egg_dp_mix_tuning(int K, int dtype, int prec, int *batched, int64_t *group);
+
+/* Pin the evaluation of degree K (> 22) for this dtype and mode instead of timing candidates:
+ * for callers that tuned offline, and for tests that must cover both evaluations.  Results do
+ * not depend on the choice.  No counterpart in the reference. */
+int egg_dp_mix_set_tuning(int K, int dtype, int prec, int batched, int64_t group);
+
 #ifdef __cplusplus
 }
 #endif

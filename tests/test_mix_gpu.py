@@ -1,0 +1,118 @@
+"""Mixed-degree batches (egg_dp_mix, hafnian_submatrices) against per-instance DP calls and the
+oracle: every result must equal hafnian(A[r, r]; method=:dp) of the same precision mode."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def nat(egg):
+    from theeggman_b200 import _native
+
+    assert _native.lib().egg_init(0) == 0, "no CUDA device"
+    return _native
+
+
+def _sub(A, r):
+    r = np.asarray(r, dtype=np.int64)
+    return A[np.ix_(r, r)]
+
+
+def _mix(W, B, n, sizes, seed):
+    rng = np.random.default_rng(seed)
+    return [rng.choice(n, size=int(rng.choice(sizes)), replace=False) for _ in range(B)]
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_mix_equals_single_calls(egg, W, orc, cplx):
+    n = 40
+    A = W.gbs_parent(n, 11) if cplx else W.dense_real(n, 12)
+    rows = _mix(W, 60, n, [0, 1, 2, 3, 4, 6, 8, 11, 12, 16, 20, 22, 24, 26], 5)
+    got = egg.hafnian_submatrices(A, rows, check_symmetric=False)
+    for b, r in enumerate(rows):
+        k = len(r)
+        if k == 0:
+            assert got[b] == 1
+        elif k % 2:
+            assert got[b] == 0
+        else:
+            assert got[b] == egg.hafnian(_sub(A, r), method="dp", check_symmetric=False), (b, k)
+    # the oracle on a few instances (bit-identical in the exact mode)
+    plan_cache = {}
+    for b, r in enumerate(rows[:12]):
+        k = len(r)
+        if k < 2 or k % 2:
+            continue
+        plan = plan_cache.setdefault(k, orc.build_plan(k, 4))
+        P = orc.gather_pairs(np.asarray(A), [int(i) + 1 for i in r], k)
+        assert got[b] == orc.haf_dp_pairs(P, plan, orc.C128 if cplx else orc.F64), (b, k)
+
+
+def test_mix_repeated_rows_and_modes(egg, W):
+    n = 24
+    A = W.gbs_parent(n, 21)
+    rows = [[0, 0, 1, 2], [3, 3, 3, 3, 5, 6], list(range(20)), [7, 8], [1, 2, 3, 4, 5, 6, 7, 8, 9, 10]]
+    got = egg.hafnian_submatrices(A, rows, check_symmetric=False)
+    for b, r in enumerate(rows):
+        assert got[b] == egg.hafnian(_sub(A, r), method="dp", check_symmetric=False)
+    fma = egg.hafnian_submatrices(A, rows, check_symmetric=False, prec="fma")
+    mixed = egg.hafnian_submatrices(A, rows, check_symmetric=False, prec="mixed")
+    for b in range(len(rows)):
+        assert abs(fma[b] - got[b]) <= 1e-12 * abs(got[b])
+        assert abs(mixed[b] - got[b]) <= 1e-5 * abs(got[b])
+
+
+def test_mix_integer_parent_exact(egg, W, orc):
+    n = 30
+    G = W.er_graph(n, 0.5, 31)
+    rows = _mix(W, 25, n, [2, 4, 10, 16, 20], 9)
+    got = egg.hafnian_submatrices(G, rows, exact=True, check_symmetric=False)
+    for b, r in enumerate(rows):
+        assert got[b] == orc.dp_int128(_sub(G, r)), b
+
+
+def test_mix_gbs_shape(egg, W):
+    # The configuration-4 generator at a reduced count: degrees 8..32, distinct rows of the
+    # 64 x 64 parent; every result equals its single call.
+    A, idxs = W.gbs_mix(96, 64, range(8, 33, 2), 4)
+    got = egg.hafnian_submatrices(A, idxs, check_symmetric=False)
+    for b in range(0, 96, 7):
+        assert got[b] == egg.hafnian(_sub(A, idxs[b]), method="dp", check_symmetric=False), b
+    again = egg.hafnian_submatrices(A, idxs, check_symmetric=False)
+    assert np.array_equal(got, again)
+
+
+def test_mix_refusals(egg, W):
+    A = W.dense_real(10, 3)
+    with pytest.raises(egg.ArgumentError):
+        egg.hafnian_submatrices(A, [[0, 1], [2, 10]], check_symmetric=False)
+    with pytest.raises(egg.ArgumentError):
+        egg.hafnian_submatrices(A, [[0, -1]], check_symmetric=False)
+    assert len(egg.hafnian_submatrices(A, [], check_symmetric=False)) == 0
+
+
+@pytest.mark.parametrize("prec", ["exact", "fma", "mixed"])
+def test_mix_evaluations_agree(egg, nat, W, prec):
+    # Degrees past the whole-instance kernel, pinned to each evaluation in turn: batched groups of
+    # several sizes and grouped single instances must give the same bits.
+    import ctypes
+
+    n = 40
+    A = W.gbs_parent(n, 41)
+    rng = np.random.default_rng(77)
+    rows = [rng.choice(n, size=k, replace=False) for k in [24, 26, 24, 28, 26, 24, 26, 28, 24, 30, 26, 28, 24]]
+    L = nat.lib()
+    results = []
+    for batched, group in [(1, 64), (1, 2), (0, 1), (0, 3), (0, 16)]:
+        for K in (24, 26, 28, 30):
+            nat.check(L.egg_dp_mix_set_tuning(K, nat.EGG_C128, nat.PREC[prec], batched, group))
+        results.append(egg.hafnian_submatrices(A, rows, check_symmetric=False, prec=prec))
+        b, g = ctypes.c_int(), ctypes.c_int64()
+        nat.check(L.egg_dp_mix_tuning(26, nat.EGG_C128, nat.PREC[prec], ctypes.byref(b), ctypes.byref(g)))
+        assert (b.value, g.value) == (batched, group)
+    for r in results[1:]:
+        assert np.array_equal(r, results[0])
+    if prec == "exact":
+        for b, r in enumerate(rows):
+            assert results[0][b] == egg.hafnian(_sub(A, r), method="dp", check_symmetric=False)

@@ -539,4 +539,15 @@ int egg_dp_mix_device(int dtype, int prec, const void *A, int64_t n, int64_t B, 
     return mix_run(dtype, prec, A, n, B, offsets, rows, out, st);
 }
 
+int egg_dp_mix_set_tuning(int K, int dtype, int prec, int batched, int64_t group)
+{
+    return mix_set_tuning(K, dtype, prec, batched, group);
+}
+
+int egg_dp_mix_tuning(int K, int dtype, int prec, int *batched, int64_t *group)
+{
+    if (!batched || !group) return fail(EGG_ERR_ARGUMENT, "null argument");
+    return mix_tuned(K, dtype, prec, batched, group);
+}
+
 }  // extern "C"

@@ -18,6 +18,8 @@
 // evaluates the CPU loop, so results are bit-identical to the reference's _haf_dp.  EGG_PREC_FMA
 // contracts each multiply-add as the reference's GPU kernel does.  EGG_PREC_MIXED multiplies in
 // FP32 and accumulates each state in FP64.  Integer inputs run exactly in Int128.
+#include <type_traits>
+
 #include "egg_dp_common.cuh"
 
 namespace egg {
@@ -481,7 +483,7 @@ static int launch_closed_level(const uint32_t *bt, const PT *P, const HT *prev, 
     const int64_t cap = (int64_t)ctx().num_sms * 8;
     if (blocks > cap) blocks = cap;
     if constexpr (has_fixed<Op, PT>::value) {
-        if (B == 1 && fixed_level<Op, PT, HT, AT>(bt, P, prev, cur, K, c, n, run, (int)blocks, st)) return EGG_OK;
+        if (B == 1 && fixed_level<Op, PT, HT, AT>(bt, P, prev, cur, K, c, n, run, (int)blocks, 1, 0, 0, 0, st)) return EGG_OK;
     }
     k<<<(unsigned)blocks, kLevelThreads, sm, st>>>(bt, P, prev, cur, K, c, n, B, run);
     count_launch();
@@ -642,6 +644,127 @@ static int dp_dispatch(const DevPlan &plan, int dtype, int prec, const void *dP,
     if (rc) return rc;
     EGG_CUDA_TRY(cudaGetLastError());
     return EGG_OK;
+}
+
+// ---- several single-instance evaluations per launch ------------------------------------------------
+//
+// For a batch of large degree the instance-fastest level kernel keeps B whole levels live, which
+// outgrows L2 (N = 32 complex: 13 MB per instance and level), so every child load reaches HBM.
+// Here G instances stored instance-major run the single-instance fixed-popcount kernels side by
+// side (blockIdx.y = instance): G levels stay L2-resident and each instance keeps the lean walk.
+
+template <class Op, class PT, class HT, class AT>
+__global__ void __launch_bounds__(256) dpc_first_grouped_kernel(const PT *__restrict__ P, HT *__restrict__ Hcur, int K,
+                                                                int64_t n, int64_t ldp, int64_t ldh)
+{
+    const PT *Pi = P + blockIdx.y * ldp;
+    HT *Hi = Hcur + blockIdx.y * ldh;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
+        Hi[s] = first_level_value<Op, PT, HT, AT>(s, K, Pi, 1, 0);
+}
+
+__device__ __forceinline__ void store(double &d, float a) { d = (double)a; }
+__device__ __forceinline__ void store(cd &d, cf a) { d = cd{(double)a.re, (double)a.im}; }
+
+template <class HT, class OT>
+__global__ void copy_strided_kernel(const HT *__restrict__ in, int64_t ld, OT *__restrict__ out, int64_t G)
+{
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < G; g += (int64_t)gridDim.x * blockDim.x)
+        store(out[g], in[g * ld]);
+}
+
+template <class Op, class PT, class HT, class AT, class OT>
+static int run_grouped(const DevPlan &plan, const PT *P, int64_t G, HT *h0, HT *h1, int64_t ldh, OT *out, cudaStream_t st)
+{
+    int rc = EGG_OK;
+    const uint32_t *bt = binom32_device(st, &rc);
+    if (!bt) return rc;
+    const int K = plan.K;
+    const int64_t ldp = (int64_t)K * (K - 1) / 2;
+    const int nlev = (int)plan.levels.size();
+    constexpr bool direct = std::is_same<HT, OT>::value;  // the last level can land in `out`
+    HT *prev = (nlev == 2 && direct) ? (HT *)out : h1;
+    int64_t ldprev = (nlev == 2 && direct) ? 1 : ldh;
+    {
+        const int64_t n = plan.levels[1].n;
+        int64_t bx = (n + 255) / 256;
+        if (bx > 4096) bx = 4096;
+        dpc_first_grouped_kernel<Op, PT, HT, AT><<<dim3((unsigned)bx, (unsigned)G), 256, 0, st>>>(P, prev, K, n, ldp, ldprev);
+        count_launch();
+    }
+    for (int L = 2; L < nlev; ++L) {
+        const int c = 2 * L;
+        const int64_t n = plan.levels[L].n;
+        const bool last = L == nlev - 1;
+        HT *cur = (last && direct) ? (HT *)out : ((L & 1) ? h1 : h0);
+        const int64_t ldcur = (last && direct) ? 1 : ldh;
+        // Run length and blocks per instance as in the single-instance launch, with the G
+        // instances sharing the SMs.
+        const int64_t want = ((int64_t)ctx().num_sms * 4 + G - 1) / G;
+        int run = kRun;
+        while (run > 1 && (n + (int64_t)run * kLevelThreads - 1) / ((int64_t)run * kLevelThreads) < want) run /= 2;
+        int64_t blocks = (n + (int64_t)run * kLevelThreads - 1) / ((int64_t)run * kLevelThreads);
+        const int64_t cap = ((int64_t)ctx().num_sms * 8 + G - 1) / G;
+        if (blocks > cap) blocks = cap;
+        if (!fixed_level<Op, PT, HT, AT>(bt, P, prev, cur, K, c, n, run, (int)blocks, (int)G, ldp, ldprev, ldcur, st))
+            return fail(EGG_ERR_ARGUMENT, "no fixed-popcount kernel for level " + std::to_string(c) + " of degree " +
+                                              std::to_string(K));
+        prev = cur;
+        ldprev = ldcur;
+    }
+    if (!direct) {
+        copy_strided_kernel<HT, OT><<<grid_for(G, 256), 256, 0, st>>>(prev, ldprev, out, G);
+        count_launch();
+    }
+    EGG_CUDA_TRY(cudaGetLastError());
+    return EGG_OK;
+}
+
+bool dp_grouped_ok(int K, int dtype, int prec)
+{
+    if (K < 4 || K > 40) return false;  // every level has a fixed-popcount kernel up to K = 40
+    if (dtype == EGG_I64) return prec == EGG_PREC_EXACT;
+    return dtype == EGG_F64 || dtype == EGG_C128;
+}
+
+int dp_run_grouped(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t G, void *dout, cudaStream_t st)
+{
+    if (!dp_grouped_ok(plan.K, dtype, prec)) return fail(EGG_ERR_ARGUMENT, "no grouped DP for this degree and type");
+    if (!plan.closed_form()) return fail(EGG_ERR_ARGUMENT, "grouped DP needs a closed-form plan");
+    Context &c = ctx();
+    const size_t need = dp_scratch_bytes(plan, dtype, prec, G);
+    int rc = ensure_buf(c.scratch[0], need);
+    if (rc) return rc;
+    const int64_t maxlev = max_level(plan);
+    char *h0 = (char *)c.scratch[0].ptr, *h1 = h0 + need / 2;
+    const int64_t npairs = (int64_t)plan.K * (plan.K - 1) / 2;
+    if (prec == EGG_PREC_MIXED) {
+        const int64_t nvals = npairs * G * (dtype == EGG_C128 ? 2 : 1);
+        rc = ensure_buf(c.scratch[5], (size_t)nvals * sizeof(float));
+        if (rc) return rc;
+        float *P32 = (float *)c.scratch[5].ptr;
+        to_f32_kernel<<<grid_for(nvals, 256), 256, 0, st>>>((const double *)dP, P32, nvals);
+        count_launch();
+        if (dtype == EGG_F64)
+            return run_grouped<MixedOp, float, float, double, double>(plan, P32, G, (float *)h0, (float *)h1, maxlev,
+                                                                      (double *)dout, st);
+        return run_grouped<MixedOp, cf, cf, cd, cd>(plan, (const cf *)P32, G, (cf *)h0, (cf *)h1, maxlev, (cd *)dout, st);
+    }
+    const bool fma_mode = prec == EGG_PREC_FMA;
+    switch (dtype) {
+    case EGG_F64:
+        return fma_mode ? run_grouped<FmaOp, double, double, double, double>(plan, (const double *)dP, G, (double *)h0,
+                                                                               (double *)h1, maxlev, (double *)dout, st)
+                        : run_grouped<ExactOp, double, double, double, double>(plan, (const double *)dP, G, (double *)h0,
+                                                                                 (double *)h1, maxlev, (double *)dout, st);
+    case EGG_C128:
+        return fma_mode ? run_grouped<FmaOp, cd, cd, cd, cd>(plan, (const cd *)dP, G, (cd *)h0, (cd *)h1, maxlev, (cd *)dout, st)
+                        : run_grouped<ExactOp, cd, cd, cd, cd>(plan, (const cd *)dP, G, (cd *)h0, (cd *)h1, maxlev, (cd *)dout, st);
+    case EGG_I64:
+        return run_grouped<IntOp, int64_t, __int128, __int128, __int128>(plan, (const int64_t *)dP, G, (__int128 *)h0,
+                                                                        (__int128 *)h1, maxlev, (__int128 *)dout, st);
+    }
+    return fail(EGG_ERR_ARGUMENT, "unknown dtype");
 }
 
 int dp_run(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t B, void *dout, cudaStream_t st)

@@ -129,10 +129,12 @@ template <> struct has_fixed<IntOp, int64_t> { static constexpr bool value = tru
 template <> struct has_fixed<MixedOp, float> { static constexpr bool value = true; };
 template <> struct has_fixed<MixedOp, cf> { static constexpr bool value = true; };
 
-// Launches level c of a closed-form plan for one instance (B == 1) with a kernel specialised for
-// that popcount.  Returns false (and launches nothing) when no specialisation covers (c, U).
+// Launches level c of a closed-form plan for G independent instances with a kernel specialised
+// for that popcount; instance g's pairs are at P + g * ldp and its level values at prev + g * ldhp
+// (read) and cur + g * ldhc (written).  Returns false (and launches nothing) when no
+// specialisation covers (c, U).
 template <class Op, class PT, class HT, class AT>
 bool fixed_level(const uint32_t *binom, const PT *P, const HT *prev, HT *cur, int K, int c, int64_t n, int run,
-                 int blocks, cudaStream_t st);
+                 int blocks, int G, int64_t ldp, int64_t ldhp, int64_t ldhc, cudaStream_t st);
 
 }  // namespace egg

@@ -66,12 +66,17 @@ __device__ __forceinline__ AT walk_fixed(M m, const uint2 *__restrict__ TP, int 
 }
 
 // Same phases as dpc_level_kernel with B == 1 (masks of `run` consecutive states per thread, then
-// one state per thread and step), with walk_fixed<C>.
+// one state per thread and step), with walk_fixed<C>.  blockIdx.y selects one of several
+// independent instances stored instance-major: pairs at P + y * ldp, the level read at
+// Hprev + y * ldhp and the level written at Hcur + y * ldhc.
 template <int C, class Op, class M, class PT, class HT, class AT>
 __global__ void __launch_bounds__(kLevelThreads) dpc_fixed_kernel(const uint32_t *__restrict__ binom, const PT *__restrict__ P,
                                                                   const HT *__restrict__ Hprev, HT *__restrict__ Hcur, int K,
-                                                                  int64_t n, int run)
+                                                                  int64_t n, int run, int64_t ldp, int64_t ldhp, int64_t ldhc)
 {
+    P += blockIdx.y * ldp;
+    Hprev += blockIdx.y * ldhp;
+    Hcur += blockIdx.y * ldhc;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int ld = C + 1;
     const int m0 = (K - C) / 2, U = K - m0;
@@ -103,7 +108,7 @@ __global__ void __launch_bounds__(kLevelThreads) dpc_fixed_kernel(const uint32_t
 
 template <int C, class Op, class M, class PT, class HT, class AT>
 static bool launch_fixed(const uint32_t *binom, const PT *P, const HT *prev, HT *cur, int K, int64_t n, int run, int blocks,
-                         cudaStream_t st)
+                         int G, int64_t ldp, int64_t ldhp, int64_t ldhc, cudaStream_t st)
 {
     auto k = dpc_fixed_kernel<C, Op, M, PT, HT, AT>;
     static bool attr_set = false;  // per instantiation; callers hold the library's lock
@@ -113,18 +118,18 @@ static bool launch_fixed(const uint32_t *binom, const PT *P, const HT *prev, HT 
     }
     const int U = (K + C) / 2;
     const size_t sm = level_pairs_offset<M>(U, C + 1) + (size_t)K * (K - 1) / 2 * sizeof(PT);
-    k<<<(unsigned)blocks, kLevelThreads, sm, st>>>(binom, P, prev, cur, K, n, run);
+    k<<<dim3((unsigned)blocks, (unsigned)G), kLevelThreads, sm, st>>>(binom, P, prev, cur, K, n, run, ldp, ldhp, ldhc);
     count_launch();
     return true;
 }
 
 #define EGG_FIXED_CASE(CC, MT) \
-    case CC: return launch_fixed<CC, Op, MT, PT, HT, AT>(binom, P, prev, cur, K, n, run, blocks, st);
+    case CC: return launch_fixed<CC, Op, MT, PT, HT, AT>(binom, P, prev, cur, K, n, run, blocks, G, ldp, ldhp, ldhc, st);
 
 // 32-bit masks for levels whose positions fit (U <= 32, c <= 32); 64-bit masks for c = 26..46.
 template <class Op, class PT, class HT, class AT>
 bool fixed_level(const uint32_t *binom, const PT *P, const HT *prev, HT *cur, int K, int c, int64_t n, int run, int blocks,
-                 cudaStream_t st)
+                 int G, int64_t ldp, int64_t ldhp, int64_t ldhc, cudaStream_t st)
 {
     const int U = (K + c) / 2;
     if (U <= 32) {
@@ -150,6 +155,6 @@ bool fixed_level(const uint32_t *binom, const PT *P, const HT *prev, HT *cur, in
 
 #define EGG_INSTANTIATE_FIXED(OP, PT, HT, AT)                                                                         \
     template bool fixed_level<OP, PT, HT, AT>(const uint32_t *, const PT *, const HT *, HT *, int, int, int64_t, int, int, \
-                                              cudaStream_t);
+                                              int, int64_t, int64_t, int64_t, cudaStream_t);
 
 }  // namespace egg

@@ -171,12 +171,21 @@ const uint32_t *binom32_device(cudaStream_t st, int *rc);
 DevPlan *dp_plan_for(int K, int *rc);
 int dp_run(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t B, void *dout, cudaStream_t st);
 size_t dp_scratch_bytes(const DevPlan &plan, int dtype, int prec, int64_t B);
+// G instances of a closed-form plan side by side, each evaluated as a single instance: P is
+// instance-major (instance g's pairs at g * npairs), out receives G values.  Degrees 4..40, for
+// Float64/ComplexF64 (all modes) and Int64 (exact); dp_grouped_ok says which.
+bool dp_grouped_ok(int K, int dtype, int prec);
+int dp_run_grouped(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t G, void *dout, cudaStream_t st);
 
 // egg_mix.cu
 // Hafnians of the principal submatrices A[r, r], r = rows[offsets[b]..offsets[b+1]), of the n x n
 // column-major parent A: A, rows and out in device memory, offsets on the host.
 int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int64_t *offsets, const int32_t *drows,
             void *dout, cudaStream_t st);
+// The evaluation the tuner chose for (K, dtype, prec): batched (1) or grouped single instances (0),
+// and the group size.
+int mix_tuned(int K, int dtype, int prec, int *batched, int64_t *group);
+int mix_set_tuning(int K, int dtype, int prec, int batched, int64_t group);
 
 // egg_sieve.cu
 // A caller-provided device region for the sieve's tables and partial sums (used instead of the

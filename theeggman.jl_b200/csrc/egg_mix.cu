@@ -12,6 +12,9 @@
 //   4. one scatter kernel writes the results back in the caller's order (odd sizes give 0,
 //      empty row sets give 1).
 // Every result is the value hafnian(A[r, r]; method = :dp) gives for the same precision mode.
+#include <map>
+#include <tuple>
+
 #include "egg_internal.cuh"
 
 namespace egg {
@@ -24,6 +27,7 @@ struct MixBin {
     int64_t first;  // position of the bin's first instance in the sorted order
     int64_t poff;   // element offset of the bin's P
     int64_t ebase;  // gather elements before this bin
+    int64_t lay;    // P layout: consecutive groups of `lay` instances, instance-fastest within a group
 };
 
 struct MixBins {
@@ -41,7 +45,9 @@ template <> __device__ __forceinline__ double nan_of<double>() { return __longlo
 template <> __device__ __forceinline__ cd nan_of<cd>() { return cd{nan_of<double>(), nan_of<double>()}; }
 template <> __device__ __forceinline__ int64_t nan_of<int64_t>() { return 0; }
 
-// P_bin[q * count + i] = A[r[qi], r[qj]] for the bin's i-th instance, q = _pair_index(qi+1, qj+1, K) - 1.
+// The bin's pairs, A[r[qi], r[qj]] for q = _pair_index(qi+1, qj+1, K) - 1, in groups of `lay`
+// instances: group g at poff + g * npairs * lay, pair q of its instance i at q * glen + i.  (lay = 1
+// is instance-major; lay >= count is the instance-fastest matrix of _gather_pairs_batch.)
 // Row indices outside [0, n) are not read: the pair gets NaN (0 for integers).
 template <class T>
 __global__ void mix_gather_kernel(const T *__restrict__ A, int64_t n, const int64_t *__restrict__ offsets,
@@ -53,7 +59,12 @@ __global__ void mix_gather_kernel(const T *__restrict__ A, int64_t n, const int6
         while (k + 1 < bins.nb && bins.b[k + 1].ebase <= g) ++k;
         const MixBin &bn = bins.b[k];
         const int64_t e = g - bn.ebase;
-        const int64_t q = e / bn.count, i = e - q * bn.count;
+        // e enumerates (group, pair, instance in group); groups hold `lay` instances (the last fewer).
+        const int64_t per = (int64_t)bn.npairs * bn.lay;
+        const int64_t grp = e / per, g0 = grp * bn.lay;
+        const int64_t glen = bn.count - g0 < bn.lay ? bn.count - g0 : bn.lay;
+        const int64_t w = e - grp * per;
+        const int64_t q = w / glen, i = g0 + (w - q * glen);
         int qi = 0, rem = (int)q, len = bn.K - 1;
         while (rem >= len) {
             rem -= len;
@@ -89,6 +100,103 @@ __global__ void mix_scatter_kernel(const OT *__restrict__ sorted, const int32_t 
 
 static size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
+// How a degree bin is evaluated: `batched` runs groups of `group` instances through dp_run
+// (instance-fastest, one thread per (state, instance)); otherwise groups of `group` instances go
+// through dp_run_grouped (instance-major, each instance walked as a single instance).
+struct BinExec {
+    bool batched;
+    int64_t group;
+};
+
+// Chosen per (degree, dtype, precision) by timing on first use; kept for the process.
+static std::map<std::tuple<int, int, int>, BinExec> g_tuned;
+static std::mutex g_tuned_mu;
+
+static int launch_gather(int dtype, const void *dA, int64_t n, const int64_t *doff, const int32_t *drows,
+                         const int32_t *dorder, const MixBins &bins, int64_t total, void *dP, cudaStream_t st)
+{
+    if (total <= 0) return EGG_OK;
+    int64_t blocks = (total + 255) / 256, cap = (int64_t)ctx().num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    if (dtype == EGG_F64)
+        mix_gather_kernel<double><<<(unsigned)blocks, 256, 0, st>>>((const double *)dA, n, doff, drows, dorder, bins, total,
+                                                                    (double *)dP);
+    else if (dtype == EGG_C128)
+        mix_gather_kernel<cd><<<(unsigned)blocks, 256, 0, st>>>((const cd *)dA, n, doff, drows, dorder, bins, total, (cd *)dP);
+    else
+        mix_gather_kernel<int64_t><<<(unsigned)blocks, 256, 0, st>>>((const int64_t *)dA, n, doff, drows, dorder, bins, total,
+                                                                     (int64_t *)dP);
+    count_launch();
+    EGG_CUDA_TRY(cudaGetLastError());
+    return EGG_OK;
+}
+
+// Evaluate one bin (already gathered in the layout of `ex`) into its slice of the sorted results.
+static int run_bin(const DevPlan &plan, int dtype, int prec, const MixBin &bn, const BinExec &ex, const char *dP,
+                   char *dout, size_t es, size_t oes, cudaStream_t st)
+{
+    for (int64_t g0 = 0; g0 < bn.count; g0 += ex.group) {
+        const int64_t len = bn.count - g0 < ex.group ? bn.count - g0 : ex.group;
+        const char *P = dP + (size_t)g0 * bn.npairs * es;
+        char *o = dout + (size_t)g0 * oes;
+        const int rc = ex.batched ? dp_run(plan, dtype, prec, P, len, o, st) : dp_run_grouped(plan, dtype, prec, P, len, o, st);
+        if (rc) return rc;
+    }
+    return EGG_OK;
+}
+
+// Time each candidate on the bin's first instances (at most 64) and keep the fastest per instance.
+static int tune_bin(const DevPlan &plan, int dtype, int prec, const MixBin &bn, const void *dA, int64_t n,
+                    const int64_t *doff, const int32_t *drows, const int32_t *dorder, char *tmpP, char *tmpO, size_t es,
+                    size_t oes, cudaStream_t st, BinExec *best)
+{
+    const int64_t S = bn.count < 64 ? bn.count : 64;
+    std::vector<BinExec> cands;
+    for (int64_t L : {(int64_t)64, (int64_t)16})
+        if (L <= S || L == 64) cands.push_back({true, L < S ? L : S});
+    if (dp_grouped_ok(bn.K, dtype, prec) && plan.closed_form())
+        for (int64_t G : {(int64_t)1, (int64_t)2, (int64_t)4, (int64_t)8, (int64_t)16, (int64_t)32, (int64_t)64})
+            if (G <= S) cands.push_back({false, G});
+    cudaEvent_t e0, e1;
+    EGG_CUDA_TRY(cudaEventCreate(&e0));
+    EGG_CUDA_TRY(cudaEventCreate(&e1));
+    float bestv = 0;
+    bool have = false;
+    int rc = EGG_OK;
+    for (const BinExec &cand : cands) {
+        MixBins one;
+        one.nb = 1;
+        one.b[0] = bn;
+        one.b[0].count = S;
+        one.b[0].poff = 0;
+        one.b[0].ebase = 0;
+        one.b[0].lay = cand.batched ? cand.group : 1;
+        rc = launch_gather(dtype, dA, n, doff, drows, dorder, one, (int64_t)bn.npairs * S, tmpP, st);
+        if (!rc) rc = run_bin(plan, dtype, prec, one.b[0], cand, tmpP, tmpO, es, oes, st);  // warm-up
+        if (rc) break;
+        cudaEventRecord(e0, st);
+        rc = run_bin(plan, dtype, prec, one.b[0], cand, tmpP, tmpO, es, oes, st);
+        cudaEventRecord(e1, st);
+        if (rc) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = fail(EGG_ERR_CUDA, "tuning run failed");
+            break;
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (!have || ms < bestv) {
+            bestv = ms;
+            *best = cand;
+            have = true;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!rc && !have) rc = fail(EGG_ERR_CUDA, "no candidate to tune");
+    if (!rc && best->batched) best->group = best->group >= S ? bn.count : best->group;  // the sample stood for "all"
+    return rc;
+}
+
 // The mix with A, the row indices and out in device memory and the row-set boundaries on the host.
 int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int64_t *offsets, const int32_t *drows,
             void *dout, cudaStream_t st)
@@ -96,6 +204,8 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
     if (dtype != EGG_F64 && dtype != EGG_C128 && dtype != EGG_I64)
         return fail(EGG_ERR_ARGUMENT, "the mixed-degree batch takes Float64, ComplexF64 or Int64 parents");
     if (dtype == EGG_I64 && prec != EGG_PREC_EXACT) return fail(EGG_ERR_ARGUMENT, "integer parents run exactly");
+    if (prec != EGG_PREC_EXACT && prec != EGG_PREC_FMA && prec != EGG_PREC_MIXED)
+        return fail(EGG_ERR_ARGUMENT, "unknown precision mode");
     if (B < 0 || n < 0) return fail(EGG_ERR_ARGUMENT, "negative size");
     if (B == 0) return EGG_OK;
     if (B > INT32_MAX) return fail(EGG_ERR_TOO_LARGE, "more than 2^31 - 1 instances");
@@ -119,6 +229,7 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
         bn.first = ndp;
         bn.poff = total;
         bn.ebase = total;
+        bn.lay = bn.count;
         pos[K] = ndp;
         ndp += cnt[K];
         total += bn.npairs * bn.count;
@@ -133,57 +244,88 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
         else if (sz & 1) order[zpos++] = (int32_t)b;
         else order[pos[sz]++] = (int32_t)b;
     }
-    // 2. Plans and buffers: every bin's work buffers are sized before anything is enqueued, so no
-    // buffer is reallocated while an earlier bin's kernels may still be running.
+    // 2. Plans; buffers for the largest group of every bin (sized before anything is enqueued, so
+    // no buffer is reallocated while an earlier bin's kernels may still be running).
     const size_t es = dtype_size(dtype), oes = dtype == EGG_I64 ? 16 : es;
-    size_t hmax = 0, p32max = 0;
     std::vector<DevPlan *> plans;
     for (int k = 0; k < bins.nb; ++k) {
         int rc = EGG_OK;
         DevPlan *pl = dp_plan_for(bins.b[k].K, &rc);
         if (!pl) return rc;
         plans.push_back(pl);
-        const size_t h = dp_scratch_bytes(*pl, dtype, prec, bins.b[k].count);
-        hmax = h > hmax ? h : hmax;
-        const size_t p32 = (size_t)bins.b[k].npairs * bins.b[k].count * (dtype == EGG_C128 ? 2 : 1) * sizeof(float);
-        p32max = p32 > p32max ? p32 : p32max;
     }
     Context &c = ctx();
+    int npmax = 0;
+    for (int k = 0; k < bins.nb; ++k) npmax = bins.b[k].npairs > npmax ? bins.b[k].npairs : npmax;
     const size_t off_o = align256((size_t)(B + 1) * 8), off_p = off_o + align256((size_t)B * 4);
-    const size_t off_r = off_p + align256((size_t)total * es), arena = off_r + align256((size_t)(ndp ? ndp : 1) * oes);
+    const size_t off_r = off_p + align256((size_t)total * es), off_t = off_r + align256((size_t)(ndp ? ndp : 1) * oes);
+    const size_t off_to = off_t + align256((size_t)64 * npmax * es), arena = off_to + align256((size_t)64 * oes);
     int rc = ensure_buf(c.scratch[6], arena);
-    if (!rc && hmax) rc = ensure_buf(c.scratch[0], hmax);
-    if (!rc && prec == EGG_PREC_MIXED && p32max) rc = ensure_buf(c.scratch[5], p32max);
     if (rc) return rc;
     char *base = (char *)c.scratch[6].ptr;
     int64_t *doff = (int64_t *)base;
     int32_t *dorder = (int32_t *)(base + off_o);
-    char *dP = base + off_p, *dsorted = base + off_r;
+    char *dP = base + off_p, *dsorted = base + off_r, *tmpP = base + off_t, *tmpO = base + off_to;
     EGG_CUDA_TRY(cudaMemcpyAsync(doff, offsets, (size_t)(B + 1) * 8, cudaMemcpyHostToDevice, st));
     EGG_CUDA_TRY(cudaMemcpyAsync(dorder, order.data(), (size_t)B * 4, cudaMemcpyHostToDevice, st));
-    // 3. Gather, 4. DP per bin, 5. scatter.
-    if (total > 0) {
-        int64_t blocks = (total + 255) / 256, cap = (int64_t)c.num_sms * 16;
-        if (blocks > cap) blocks = cap;
-        if (dtype == EGG_F64)
-            mix_gather_kernel<double><<<(unsigned)blocks, 256, 0, st>>>((const double *)dA, n, doff, drows, dorder, bins, total,
-                                                                        (double *)dP);
-        else if (dtype == EGG_C128)
-            mix_gather_kernel<cd><<<(unsigned)blocks, 256, 0, st>>>((const cd *)dA, n, doff, drows, dorder, bins, total, (cd *)dP);
-        else
-            mix_gather_kernel<int64_t><<<(unsigned)blocks, 256, 0, st>>>((const int64_t *)dA, n, doff, drows, dorder, bins,
-                                                                         total, (int64_t *)dP);
-        count_launch();
-        EGG_CUDA_TRY(cudaGetLastError());
+    // 3. How each bin runs: one launch for degrees the whole-instance kernel covers, else the tuned
+    // choice (timed on first use, unless the stream is being captured).
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    EGG_CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+    std::vector<BinExec> exs(bins.nb);
+    size_t hmax = 0, p32max = 0;
+    for (int k = 0; k < bins.nb; ++k) {
+        MixBin &bn = bins.b[k];
+        BinExec ex{true, bn.count};
+        if (bn.K > 22 && bn.count > 1) {
+            const auto key = std::make_tuple(bn.K, dtype, prec);
+            bool found = false;
+            {
+                std::lock_guard<std::mutex> lk(g_tuned_mu);
+                auto it = g_tuned.find(key);
+                if (it != g_tuned.end()) {
+                    ex = it->second;
+                    found = true;
+                }
+            }
+            if (!found && cap == cudaStreamCaptureStatusNone) {
+                // Tuning needs the largest candidate's buffers.
+                size_t h = dp_scratch_bytes(*plans[k], dtype, prec, 64);
+                rc = ensure_buf(c.scratch[0], h);
+                if (!rc && prec == EGG_PREC_MIXED)
+                    rc = ensure_buf(c.scratch[5], (size_t)64 * bn.npairs * (dtype == EGG_C128 ? 2 : 1) * sizeof(float));
+                if (!rc) rc = tune_bin(*plans[k], dtype, prec, bn, dA, n, doff, drows, dorder, tmpP, tmpO, es, oes, st, &ex);
+                if (rc) return rc;
+                std::lock_guard<std::mutex> lk(g_tuned_mu);
+                g_tuned[key] = ex;
+            } else if (!found) {
+                ex = dp_grouped_ok(bn.K, dtype, prec) && plans[k]->closed_form() ? BinExec{false, 4} : BinExec{true, bn.count};
+            }
+            if (!ex.batched && !plans[k]->closed_form()) ex = BinExec{true, bn.count};  // an explicit plan is now resident
+            if (ex.group > bn.count) ex.group = bn.count;
+        }
+        exs[k] = ex;
+        bn.lay = ex.batched ? ex.group : 1;
+        const size_t h = dp_scratch_bytes(*plans[k], dtype, prec, ex.group);
+        hmax = h > hmax ? h : hmax;
+        const size_t p32 = (size_t)bn.npairs * ex.group * (dtype == EGG_C128 ? 2 : 1) * sizeof(float);
+        p32max = p32 > p32max ? p32 : p32max;
     }
+    if (hmax) rc = ensure_buf(c.scratch[0], hmax);
+    if (!rc && prec == EGG_PREC_MIXED && p32max) rc = ensure_buf(c.scratch[5], p32max);
+    if (rc) return rc;
+    // 4. Gather, 5. DP per bin, 6. scatter.
+    rc = launch_gather(dtype, dA, n, doff, drows, dorder, bins, total, dP, st);
+    if (rc) return rc;
     for (int k = 0; k < bins.nb; ++k) {
         const MixBin &bn = bins.b[k];
-        rc = dp_run(*plans[k], dtype, prec, dP + (size_t)bn.poff * es, bn.count, dsorted + (size_t)bn.first * oes, st);
+        rc = run_bin(*plans[k], dtype, prec, bn, exs[k], dP + (size_t)bn.poff * es, dsorted + (size_t)bn.first * oes, es, oes,
+                     st);
         if (rc) return rc;
     }
     {
-        int64_t blocks = (B + 255) / 256, cap = (int64_t)c.num_sms * 16;
-        if (blocks > cap) blocks = cap;
+        int64_t blocks = (B + 255) / 256, capb = (int64_t)c.num_sms * 16;
+        if (blocks > capb) blocks = capb;
         if (dtype == EGG_F64)
             mix_scatter_kernel<double><<<(unsigned)blocks, 256, 0, st>>>((const double *)dsorted, dorder, ndp, nzero,
                                                                          B - ndp - nzero, (double *)dout);
@@ -196,6 +338,27 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
         count_launch();
         EGG_CUDA_TRY(cudaGetLastError());
     }
+    return EGG_OK;
+}
+
+int mix_set_tuning(int K, int dtype, int prec, int batched, int64_t group)
+{
+    if (K < 2 || K > 64 || K % 2) return fail(EGG_ERR_ARGUMENT, "degree must be even, 2..64");
+    if (group < 1) return fail(EGG_ERR_ARGUMENT, "group must be >= 1");
+    if (!batched && !dp_grouped_ok(K, dtype, prec))
+        return fail(EGG_ERR_ARGUMENT, "no grouped single-instance evaluation for this degree and type");
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    g_tuned[std::make_tuple(K, dtype, prec)] = BinExec{batched != 0, group};
+    return EGG_OK;
+}
+
+int mix_tuned(int K, int dtype, int prec, int *batched, int64_t *group)
+{
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    auto it = g_tuned.find(std::make_tuple(K, dtype, prec));
+    if (it == g_tuned.end()) return fail(EGG_ERR_NO_PLAN, "degree " + std::to_string(K) + " has not been tuned");
+    *batched = it->second.batched ? 1 : 0;
+    *group = it->second.group;
     return EGG_OK;
 }
 

@@ -72,9 +72,24 @@ def sieve_flops(edge_reps, glynn: bool, cplx: bool) -> float:
 
 
 def dp_bytes(K: int, B: int, value_bytes: int) -> int:
+    """Algorithmic bytes of a DP that streams an explicit plan: the transition array once, every
+    state written once and read once, and the pairs."""
     nstates, ntrans = pol._dp_counts(K)
     idx = pol._dp_index_bytes(K)
     return ntrans * idx + B * (2 * nstates + K * (K - 1) // 2) * value_bytes
+
+
+def dp_bytes_closed(K: int, B: int, value_bytes: int) -> int:
+    """Compulsory bytes of a DP on a closed-form plan (no transition array): every state written
+    once and read once, and the pairs."""
+    nstates, _ = pol._dp_counts(K)
+    return B * (2 * nstates + K * (K - 1) // 2) * value_bytes
+
+
+def dp_gather_bytes(K: int, B: int, value_bytes: int) -> int:
+    """Bytes of the child-value loads, one per transition (served mostly from L2 and L1)."""
+    _, ntrans = pol._dp_counts(K)
+    return B * ntrans * value_bytes
 
 
 # Nominal FP64 peak: 148 SMs x 64 FP64 FMA lanes x 2 flops x clock.  MEASURED_PEAKS.json carries no
