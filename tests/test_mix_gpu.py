@@ -116,3 +116,26 @@ def test_mix_evaluations_agree(egg, nat, W, prec):
     if prec == "exact":
         for b, r in enumerate(rows):
             assert results[0][b] == egg.hafnian(_sub(A, r), method="dp", check_symmetric=False)
+
+
+def test_mix_graph_replay(egg, nat, W):
+    # The second call of a shape records a graph and later calls replay it: results must not
+    # change, including when the row sets change but the degree counts do not.
+    A = W.gbs_parent(48, 51)
+    rng = np.random.default_rng(3)
+    sizes = [8, 10, 24, 26, 24, 12, 26, 9, 0, 28]
+    rows1 = [rng.choice(48, size=k, replace=False) for k in sizes]
+    rows2 = [rng.choice(48, size=k, replace=False) for k in sizes]
+    L = nat.lib()
+    first = egg.hafnian_submatrices(A, rows1, check_symmetric=False)
+    n0 = L.egg_launch_count()
+    second = egg.hafnian_submatrices(A, rows1, check_symmetric=False)
+    n1 = L.egg_launch_count()
+    third = egg.hafnian_submatrices(A, rows1, check_symmetric=False)
+    n2 = L.egg_launch_count()
+    other = egg.hafnian_submatrices(A, rows2, check_symmetric=False)
+    assert np.array_equal(first, second) and np.array_equal(first, third)
+    assert n2 - n1 == n1 - n0 > 0  # a replay counts the kernels it runs
+    for b, r in enumerate(rows2):
+        exp = egg.hafnian(_sub(A, r), method="dp", check_symmetric=False) if len(r) else 1
+        assert other[b] == exp, b

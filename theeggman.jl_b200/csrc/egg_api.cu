@@ -180,6 +180,7 @@ int egg_cache_clear(void)
     std::lock_guard<std::recursive_mutex> lk(ctx().mu);
     Context &c = ctx();
     if (c.device >= 0) cudaStreamSynchronize(c.stream);
+    mix_graphs_clear();
     for (auto &kv : c.plans)
         if (kv.second.trans) cudaFree(kv.second.trans);
     c.plans.clear();

@@ -186,6 +186,8 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
 // and the group size.
 int mix_tuned(int K, int dtype, int prec, int *batched, int64_t *group);
 int mix_set_tuning(int K, int dtype, int prec, int batched, int64_t group);
+// Drop the mixed-degree batch's recorded graphs (they hold the library's buffer addresses).
+void mix_graphs_clear();
 
 // egg_sieve.cu
 // A caller-provided device region for the sieve's tables and partial sums (used instead of the

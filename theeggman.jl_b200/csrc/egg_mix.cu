@@ -197,6 +197,57 @@ static int tune_bin(const DevPlan &plan, int dtype, int prec, const MixBin &bn, 
     return rc;
 }
 
+// ---- graph replay -------------------------------------------------------------------------------
+//
+// The kernels of one mix (gather, every bin's levels, scatter) depend only on the bin sizes, the
+// chosen evaluations and the buffers; the row sets themselves are read from device memory.  So the
+// second call of the same shape captures them into one CUDA graph and later calls replay it: one
+// launch instead of hundreds.  The offsets and the sorted order are copied in before the replay.
+struct GraphKey {
+    int dtype, prec;
+    int64_t n, B;
+    std::vector<int64_t> shape;  // per bin: K, count, batched, group
+    std::vector<const void *> ptrs;
+    bool operator==(const GraphKey &o) const
+    {
+        return dtype == o.dtype && prec == o.prec && n == o.n && B == o.B && shape == o.shape && ptrs == o.ptrs;
+    }
+};
+
+struct GraphEntry {
+    GraphKey key;
+    int seen = 0;
+    cudaGraphExec_t exec = nullptr;
+    long long nodes = 0;  // kernel launches one replay makes
+};
+
+static std::vector<GraphEntry> g_graphs;  // a few recent shapes; callers hold the library's lock
+static constexpr size_t kMaxGraphs = 8;
+
+static GraphEntry &graph_entry(const GraphKey &key)
+{
+    for (GraphEntry &e : g_graphs)
+        if (e.key == key) return e;
+    if (g_graphs.size() >= kMaxGraphs) {
+        if (g_graphs.front().exec) cudaGraphExecDestroy(g_graphs.front().exec);
+        g_graphs.erase(g_graphs.begin());
+    }
+    g_graphs.push_back(GraphEntry{key});
+    return g_graphs.back();
+}
+
+void mix_graphs_clear()
+{
+    for (GraphEntry &e : g_graphs)
+        if (e.exec) cudaGraphExecDestroy(e.exec);
+    g_graphs.clear();
+}
+
+static int mix_kernels(int dtype, int prec, const void *dA, int64_t n, int64_t B, const MixBins &bins,
+                       const std::vector<BinExec> &exs, const std::vector<DevPlan *> &plans, const int64_t *doff,
+                       const int32_t *drows, const int32_t *dorder, int64_t total, int64_t ndp, int64_t nzero, char *dP,
+                       char *dsorted, void *dout, cudaStream_t st);
+
 // The mix with A, the row indices and out in device memory and the row-set boundaries on the host.
 int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int64_t *offsets, const int32_t *drows,
             void *dout, cudaStream_t st)
@@ -314,8 +365,55 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
     if (hmax) rc = ensure_buf(c.scratch[0], hmax);
     if (!rc && prec == EGG_PREC_MIXED && p32max) rc = ensure_buf(c.scratch[5], p32max);
     if (rc) return rc;
-    // 4. Gather, 5. DP per bin, 6. scatter.
-    rc = launch_gather(dtype, dA, n, doff, drows, dorder, bins, total, dP, st);
+    // 4. Gather, 5. DP per bin, 6. scatter: eagerly the first time a shape is seen, captured into a
+    // graph the second time, replayed after that (not when the caller is capturing the stream).
+    if (!binom32_device(st, &rc)) return rc;
+    GraphKey key{dtype, prec, n, B, {}, {dA, drows, dout}};
+    for (int k = 0; k < bins.nb; ++k) {
+        key.shape.insert(key.shape.end(), {(int64_t)bins.b[k].K, bins.b[k].count, exs[k].batched ? 1 : 0, exs[k].group});
+    }
+    for (const DevBuf &b : c.scratch) key.ptrs.push_back(b.ptr);
+    GraphEntry *ge = cap == cudaStreamCaptureStatusNone ? &graph_entry(key) : nullptr;
+    if (ge && ge->exec) {
+        EGG_CUDA_TRY(cudaGraphLaunch(ge->exec, st));
+        count_launch(ge->nodes);
+        return EGG_OK;
+    }
+    const bool capture = ge && ge->seen >= 1;
+    if (ge) ++ge->seen;
+    const long long launches0 = g_launches.load();
+    if (capture) EGG_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    rc = mix_kernels(dtype, prec, dA, n, B, bins, exs, plans, doff, drows, dorder, total, ndp, nzero, dP, dsorted, dout, st);
+    if (capture) {
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &graph);
+        if (rc || e != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return rc ? rc : fail(EGG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        }
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) return fail(EGG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        ge->exec = exec;
+        ge->nodes = g_launches.load() - launches0;
+        g_launches.fetch_sub(ge->nodes);  // counted when the graph runs, not when it is recorded
+        EGG_CUDA_TRY(cudaGraphLaunch(exec, st));
+        count_launch(ge->nodes);
+    }
+    return rc;
+}
+
+// Steps 4-6 of mix_run: the gather, each bin's DP, and the scatter, enqueued on `st`.
+static int mix_kernels(int dtype, int prec, const void *dA, int64_t n, int64_t B, const MixBins &bins,
+                       const std::vector<BinExec> &exs, const std::vector<DevPlan *> &plans, const int64_t *doff,
+                       const int32_t *drows, const int32_t *dorder, int64_t total, int64_t ndp, int64_t nzero, char *dP,
+                       char *dsorted, void *dout, cudaStream_t st)
+{
+    Context &c = ctx();
+    const size_t es = dtype_size(dtype), oes = dtype == EGG_I64 ? 16 : es;
+    int rc = launch_gather(dtype, dA, n, doff, drows, dorder, bins, total, dP, st);
     if (rc) return rc;
     for (int k = 0; k < bins.nb; ++k) {
         const MixBin &bn = bins.b[k];
