@@ -528,9 +528,6 @@ __global__ void __launch_bounds__(256, (SizeClass<CPLX, MHI>::min_blocks))
     const FastWs w = fast_carve(smem + (size_t)wib * fast_ws_doubles(a.nmax, CPLX, MHI), a.nmax, CPLX, MHI);
     const int wslot = blockIdx.x * warps_per_block + wib;
     const int64_t W = a.warps_per_inst;
-    const int64_t chunk = (in.steps + W - 1) / W;
-    const int64_t j0 = wslot * chunk;
-    const int64_t j1 = j0 + chunk < in.steps ? j0 + chunk : in.steps;
     dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
     const int *reps = a.reps + in.reps_off;
     const int mr1 = a.maxrep + 1;
@@ -540,48 +537,55 @@ __global__ void __launch_bounds__(256, (SizeClass<CPLX, MHI>::min_blocks))
     if (lane < E) {
         r = reps[lane];
         base = (in.glynn && lane == 0) ? (r + 2) / 2 : r + 1;
-        if (j0 < j1) digit = (int)((j0 / strides[in.reps_off + lane]) % base);
     }
-    for (int64_t j = j0; j < j1; ++j) {
-        if (j > j0) {
-            const unsigned notmax = __ballot_sync(FULL, lane < E && digit != base - 1);
-            const int h = 31 - __clz(notmax);
-            if (lane == h) ++digit;
-            else if (lane > h && lane < E) digit = 0;
-        }
-        const int kk = lane < E ? (in.glynn ? 2 * digit - r : digit) : 0;
-        const bool nz = lane < E && kk != 0;
-        const unsigned mask = __ballot_sync(FULL, nz);
-        const int mE = __popc(mask);
-        const int m = 2 * mE;
-        if (m <= MLO || m > MHI) continue;  // another size class (or an empty term, which vanishes)
-        const int esum = __reduce_add_sync(FULL, lane < E ? digit : 0);
-        double bp = 1.0;
-        if (!unit) {
-            bp = lane < E ? a.binoms[r + digit * mr1] : 1.0;
-            for (int off = 16; off > 0; off >>= 1) bp *= __shfl_xor_sync(FULL, bp, off);
-        }
-        double prefac = ((n - esum) & 1) ? -bp : bp;
-        const int k0 = __shfl_sync(FULL, kk, 0);
-        if (in.glynn && k0 == 0) prefac *= 0.5;
-        if (nz) {
-            const int pos = __popc(mask & ((1u << lane) - 1u));
-            w.eidx[pos] = lane;
-            w.kval[pos] = (double)kk;
-        }
-        __syncwarp();
-        if constexpr (!CPLX) {
-            const double val = term_real<MHI, (MHI > 32 ? 2 : 1)>((const double *)a.Ax + in.ax_off, in.lda, E, mE, n, cs, w,
-                                                                  lane);
-            if (lane == 0) dd_add(acc_re, prefac * val);
-        } else {
-            const cd val = term_cplx<MHI>((const cd *)a.Ax + in.ax_off, in.lda, E, mE, n, cs, w, lane);
-            if (lane == 0) {
-                dd_add(acc_re, prefac * val.re);
-                dd_add(acc_im, prefac * val.im);
+    // Terms are dealt to warps in runs of kRunTerms consecutive indices, round robin.  A term's size
+    // is set by its digits, and a long contiguous range fixes the high digits, so contiguous ranges
+    // would hand some warps almost all of a size class and others none of it.
+    constexpr int64_t kRunTerms = 16;
+    for (int64_t j0 = wslot * kRunTerms; j0 < in.steps; j0 += W * kRunTerms) {
+        const int64_t j1 = j0 + kRunTerms < in.steps ? j0 + kRunTerms : in.steps;
+        if (lane < E) digit = (int)((j0 / strides[in.reps_off + lane]) % base);
+        for (int64_t j = j0; j < j1; ++j) {
+            if (j > j0) {
+                const unsigned notmax = __ballot_sync(FULL, lane < E && digit != base - 1);
+                const int h = 31 - __clz(notmax);
+                if (lane == h) ++digit;
+                else if (lane > h && lane < E) digit = 0;
             }
+            const int kk = lane < E ? (in.glynn ? 2 * digit - r : digit) : 0;
+            const bool nz = lane < E && kk != 0;
+            const unsigned mask = __ballot_sync(FULL, nz);
+            const int mE = __popc(mask);
+            const int m = 2 * mE;
+            if (m <= MLO || m > MHI) continue;  // another size class (or an empty term, which vanishes)
+            const int esum = __reduce_add_sync(FULL, lane < E ? digit : 0);
+            double bp = 1.0;
+            if (!unit) {
+                bp = lane < E ? a.binoms[r + digit * mr1] : 1.0;
+                for (int off = 16; off > 0; off >>= 1) bp *= __shfl_xor_sync(FULL, bp, off);
+            }
+            double prefac = ((n - esum) & 1) ? -bp : bp;
+            const int k0 = __shfl_sync(FULL, kk, 0);
+            if (in.glynn && k0 == 0) prefac *= 0.5;
+            if (nz) {
+                const int pos = __popc(mask & ((1u << lane) - 1u));
+                w.eidx[pos] = lane;
+                w.kval[pos] = (double)kk;
+            }
+            __syncwarp();
+            if constexpr (!CPLX) {
+                const double val = term_real<MHI, (MHI > 32 ? 2 : 1)>((const double *)a.Ax + in.ax_off, in.lda, E, mE, n, cs, w,
+                                                                      lane);
+                if (lane == 0) dd_add(acc_re, prefac * val);
+            } else {
+                const cd val = term_cplx<MHI>((const cd *)a.Ax + in.ax_off, in.lda, E, mE, n, cs, w, lane);
+                if (lane == 0) {
+                    dd_add(acc_re, prefac * val.re);
+                    dd_add(acc_im, prefac * val.im);
+                }
+            }
+            __syncwarp();
         }
-        __syncwarp();
     }
     if (lane == 0) {
         dd *out = partial + ((size_t)b * W + wslot) * 2;
