@@ -67,7 +67,7 @@ struct FastWs {
     double *prow;  // pivot row, by physical slot [64]
     double *wv;    // column-update weights, by physical slot [64]
     double *cf;    // La Budde coefficients coef_i, by i [64] (complex: 32 values)
-    double *C;     // coefficient table, rows 0..mhi, row stride nmax+1
+    double *C;     // La Budde coefficient table by diagonals, (mhi+1) x (mhi+1) values (see labudde_row)
     double *kval;  // multiplicities of the surviving edges after the Glynn substitution [32]
     int *eidx;     // surviving edges, compacted [32]
 };
@@ -75,7 +75,7 @@ struct FastWs {
 __host__ __device__ inline size_t fast_ws_doubles(int nmax, int cplx, int mhi)
 {
     const size_t v = cplx ? 2 : 1;  // doubles per value
-    size_t d = 64 * 3 + v * (size_t)(mhi + 1) * (nmax + 1) + 32 /*kval*/ + 16 /*eidx*/;
+    size_t d = 64 * 3 + v * (size_t)(mhi + 1) * (mhi + 1) + 32 /*kval*/ + 16 /*eidx*/;
     return (d + 1) & ~(size_t)1;  // keep every warp's region 16-byte aligned
 }
 
@@ -87,7 +87,7 @@ __device__ inline FastWs fast_carve(double *base, int nmax, int cplx, int mhi)
     w.prow = p; p += 64;
     w.wv = p; p += 64;
     w.cf = p; p += 64;
-    w.C = p; p += v * (size_t)(mhi + 1) * (nmax + 1);
+    w.C = p; p += v * (size_t)(mhi + 1) * (mhi + 1);
     w.kval = p; p += 32;
     w.eidx = (int *)p;
     return w;
@@ -95,81 +95,75 @@ __device__ inline FastWs fast_carve(double *base, int nmax, int cplx, int mhi)
 
 // ---- La Budde row k (1-based); lane t (0..n) owns coefficient t ----------------------------------
 //   C[k][t] = (t <= min(k-1,n) ? C[k-1][t] : 0) - hkk C[k-1][t-1] - sum_{j=1}^{jmax} cf[k-j] C[k-1-j][t-1-j]
-// (j = k - i of the reference's i loop, which runs i = k-1 .. max(1, k-n+1)).  Entries of a row
-// beyond its degree are zero, so lanes past min(k, n) need no special case in the depth sum.  Row r
-// of the table is at r * cs; the depth-j entry this lane reads is one row and one column before the
-// depth-(j-1) one, so its offset steps by -(cs+1).
-__device__ __forceinline__ void labudde_row(double *C, const double *cf, int k, int n, int cs, double hkk, int lane)
+// (j = k - i of the reference's i loop, which runs i = k-1 .. max(1, k-n+1)).  The table is stored
+// by diagonals: C[r][c] at T[(r - c) * rs + r].  Every entry of lane t's depth sum lies on its
+// diagonal d = k - t, at rows k-2, k-3, ..., so the sum walks one contiguous run.  Entries left of
+// column 0 (r < d) are zero -- they are cleared once per warp and never written -- so the walk
+// needs no bounds test; entries right of the diagonal (c > r) are never read.  Every entry read
+// in a term was written earlier in the same term.
+__device__ __forceinline__ void labudde_row(double *T, const double *cf, int k, int n, int rs, double hkk, int lane)
 {
     const int t = lane;
-    const bool act = t <= n;
-    const double *Cp = C + (size_t)(k - 1) * cs;
-    const int tmax = k < n ? k : n, prevmax = (k - 1) < n ? (k - 1) : n;
+    const int tmax = k < n ? k : n;
+    const int d = k - t;  // negative for lanes past row k: clamped below, their result is not stored
     double v = 0.0;
-    if (act) {
-        if (t == 0) v = Cp[0];
-        else if (t <= tmax) v = (t <= prevmax ? Cp[t] : 0.0) - hkk * Cp[t - 1];
+    if (t <= tmax) {
+        const double a = t <= k - 1 ? T[(d - 1) * rs + (k - 1)] : 0.0;  // C[k-1][t]
+        const double b = t >= 1 ? T[d * rs + (k - 1)] : 0.0;            // C[k-1][t-1]
+        v = a - hkk * b;
     }
     const int jmax = (k - 1) < (n - 1) ? (k - 1) : (n - 1);
     const double *cfk = cf + k;
-    int off = (k - 2) * cs + (t - 2);  // row k-1-j, column t-1-j at j = 1
-    const int step = cs + 1;
+    const double *Td = T + (d > 0 ? d : 0) * rs + (k - 2);  // C[k-1-j][t-1-j] at Td[1 - j]
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
     for (int j = 1; j <= 31; ++j) {
         if (j > jmax) break;
         const double c = cfk[-j];
-        const double x = (act && t > j) ? C[off] : 0.0;
-        off -= step;
+        const double x = Td[1 - j];
         if ((j & 3) == 1) a0 = fma(c, x, a0);
         else if ((j & 3) == 2) a1 = fma(c, x, a1);
         else if ((j & 3) == 3) a2 = fma(c, x, a2);
         else a3 = fma(c, x, a3);
     }
-    if (act) C[(size_t)k * cs + t] = v - ((a0 + a1) + (a2 + a3));
+    if (t <= tmax) T[d * rs + k] = v - ((a0 + a1) + (a2 + a3));
 }
 
 // [lambda^n] det(I - lambda H)^(-1/2), push-style: lane t accumulates S_t = sum_j (2t-j) q_j f_{t-j}
-// as the f's become known; f_t = -S_t / (2t).  q_j = C[m][j].  All lanes return f_n.
-__device__ __forceinline__ double series_coeff(const double *C, int m, int n, int cs, int lane)
+// as the f's become known; f_t = -S_t / (2t).  q_j = C[m][j] = T[(m - j) * rs + m].  All lanes
+// return f_n.
+__device__ __forceinline__ double series_coeff(const double *T, int m, int n, int rs, int lane)
 {
-    const double *q = C + (size_t)m * cs;
     double S = 0.0, fs = 1.0;  // fs = f_s, starting at f_0 = 1
     for (int s = 0; s < n; ++s) {
         const int j = lane - s;
-        if (j >= 1 && j <= m && lane <= n) S = fma((double)(lane + s) * q[j], fs, S);
+        if (j >= 1 && j <= m && lane <= n) S = fma((double)(lane + s) * T[(m - j) * rs + m], fs, S);
         fs = __shfl_sync(FULL, S, s + 1) * c_neg_inv_2t[s + 1];
     }
     return fs;
 }
 
-__device__ __forceinline__ void labudde_row_c(cd *C, const cd *cf, int k, int n, int cs, cd hkk, int lane)
+__device__ __forceinline__ void labudde_row_c(cd *T, const cd *cf, int k, int n, int rs, cd hkk, int lane)
 {
     const int t = lane;
-    const bool act = t <= n;
-    const cd *Cp = C + (size_t)(k - 1) * cs;
-    const int tmax = k < n ? k : n, prevmax = (k - 1) < n ? (k - 1) : n;
+    const int tmax = k < n ? k : n;
+    const int d = k - t;
     cd v{0.0, 0.0};
-    if (act) {
-        if (t == 0) v = Cp[0];
-        else if (t <= tmax) {
-            const cd a = t <= prevmax ? Cp[t] : cd{0.0, 0.0};
-            const cd b = Cp[t - 1];
-            v.re = a.re - fma(hkk.re, b.re, -hkk.im * b.im);
-            v.im = a.im - fma(hkk.re, b.im, hkk.im * b.re);
-        }
+    if (t <= tmax) {
+        const cd a = t <= k - 1 ? T[(d - 1) * rs + (k - 1)] : cd{0.0, 0.0};
+        const cd b = t >= 1 ? T[d * rs + (k - 1)] : cd{0.0, 0.0};
+        v.re = a.re - fma(hkk.re, b.re, -hkk.im * b.im);
+        v.im = a.im - fma(hkk.re, b.im, hkk.im * b.re);
     }
     const int jmax = (k - 1) < (n - 1) ? (k - 1) : (n - 1);
     const cd *cfk = cf + k;
-    int off = (k - 2) * cs + (t - 2);
-    const int step = cs + 1;
+    const cd *Td = T + (d > 0 ? d : 0) * rs + (k - 2);
     double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
 #pragma unroll
     for (int j = 1; j <= 31; ++j) {
         if (j > jmax) break;
         const cd c = cfk[-j];
-        const cd x = (act && t > j) ? C[off] : cd{0.0, 0.0};
-        off -= step;
+        const cd x = Td[1 - j];
         if (j & 1) {
             sr0 = fma(c.re, x.re, fma(-c.im, x.im, sr0));
             si0 = fma(c.re, x.im, fma(c.im, x.re, si0));
@@ -178,18 +172,18 @@ __device__ __forceinline__ void labudde_row_c(cd *C, const cd *cf, int k, int n,
             si1 = fma(c.re, x.im, fma(c.im, x.re, si1));
         }
     }
-    if (act) C[(size_t)k * cs + t] = cd{v.re - (sr0 + sr1), v.im - (si0 + si1)};
+    if (t <= tmax) T[d * rs + k] = cd{v.re - (sr0 + sr1), v.im - (si0 + si1)};
 }
 
-__device__ __forceinline__ cd series_coeff_c(const cd *C, int m, int n, int cs, int lane)
+__device__ __forceinline__ cd series_coeff_c(const cd *T, int m, int n, int rs, int lane)
 {
-    const cd *q = C + (size_t)m * cs;
     double Sr = 0.0, Si = 0.0, fr = 1.0, fi = 0.0;
     for (int s = 0; s < n; ++s) {
         const int j = lane - s;
         if (j >= 1 && j <= m && lane <= n) {
             const double w = (double)(lane + s);
-            const double ar = w * q[j].re, ai = w * q[j].im;
+            const cd q = T[(m - j) * rs + m];
+            const double ar = w * q.re, ai = w * q.im;
             Sr = fma(ar, fr, fma(-ai, fi, Sr));
             Si = fma(ar, fi, fma(ai, fr, Si));
         }
@@ -202,9 +196,10 @@ __device__ __forceinline__ cd series_coeff_c(const cd *C, int m, int n, int cs, 
 
 // ---- one real term, m <= 32 * RPL, register tile of MW columns ----------------------------------
 template <int MW, int RPL>
-__device__ __forceinline__ double term_real(const double *__restrict__ Ax, int lda, int E, int mE, int n, int cs,
+__device__ __forceinline__ double term_real(const double *__restrict__ Ax, int lda, int E, int mE, int n,
                                             const FastWs &ws, int lane)
 {
+    constexpr int rs = MW + 1;  // La Budde table row stride
     const int m = 2 * mE;
     double *prow = ws.prow, *wv = ws.wv, *cf = ws.cf, *C = ws.C;
     double R[RPL][MW];
@@ -229,7 +224,7 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
         }
         pc[q] = R[q][0];
     }
-    if (lane <= n) C[lane] = lane == 0 ? 1.0 : 0.0;  // La Budde row 0
+    if (lane == 0) C[0] = 1.0;  // La Budde row 0: C[0][0] = 1
     int hslot = 0;       // physical slot of label s-1 (label 0 never moves)
     double xprev = 0.0;  // subdiagonal entry h_{s,s-1} of the previous step
     for (int s = 1; s <= m - 2; ++s) {
@@ -259,7 +254,7 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
                 if (lab[q] <= s - 2) cf[lab[q] + 1] = pc[q] * bet[q];
             }
             __syncwarp();
-            labudde_row(C, cf, s, n, cs, hkk, lane);
+            labudde_row(C, cf, s, n, rs, hkk, lane);
         }
         // -- relabel (similarity swap of logical s and plab)
 #pragma unroll
@@ -367,17 +362,18 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
         const int hs = last ? lastslot : hslot;
         hkk = __shfl_sync(FULL, hkk, hs & 31);
         __syncwarp();
-        labudde_row(C, cf, k, n, cs, hkk, lane);
+        labudde_row(C, cf, k, n, rs, hkk, lane);
         __syncwarp();
     }
-    return series_coeff(C, m, n, cs, lane);
+    return series_coeff(C, m, n, rs, lane);
 }
 
 // ---- one complex term, m <= 32 --------------------------------------------------------------------
 template <int MW>
-__device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int E, int mE, int n, int cs,
-                                        const FastWs &ws, int lane)
+__device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int E, int mE, int n, const FastWs &ws,
+                                        int lane)
 {
+    constexpr int rs = MW + 1;  // La Budde table row stride
     const int m = 2 * mE;
     double Rr[MW], Ri[MW];
     int lab = lane;
@@ -404,7 +400,7 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
     cd *C = (cd *)ws.C;
     cd *cfc = (cd *)ws.cf;  // 32 complex coefficients
     double *prr = ws.prow, *pri = ws.prow + 32, *wvr = ws.wv, *wvi = ws.wv + 32;
-    if (lane <= n) C[lane] = lane == 0 ? cd{1.0, 0.0} : cd{0.0, 0.0};
+    if (lane == 0) C[0] = cd{1.0, 0.0};  // La Budde row 0: C[0][0] = 1
     int hslot = 0;
     cd xprev{0.0, 0.0};
     auto feed = [&](int k, double colr, double coli, cd sub, int hs) {
@@ -415,7 +411,7 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
         }
         const cd hkk{__shfl_sync(FULL, colr, hs), __shfl_sync(FULL, coli, hs)};
         __syncwarp();
-        labudde_row_c(C, cfc, k, n, cs, hkk, lane);
+        labudde_row_c(C, cfc, k, n, rs, hkk, lane);
         __syncwarp();
     };
     for (int s = 1; s <= m - 2; ++s) {
@@ -498,7 +494,7 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
         if (k == m) feed(k, cr, ci, sub, lastslot);
         else feed(k, pcr, pci, sub, hslot);
     }
-    return series_coeff_c(C, m, n, cs, lane);
+    return series_coeff_c(C, m, n, rs, lane);
 }
 
 // ---- kernels -----------------------------------------------------------------------------------
@@ -509,14 +505,17 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
 // walks all of the instance's terms (a few dozen instructions per term) and evaluates its own.
 template <bool CPLX, int MHI>
 struct SizeClass {
-    // Blocks of 256 threads kept resident per SM, i.e. the register budget per thread
-    // (65536 / (256 * min_blocks)): sized so each class's tile fits without spilling.
+    // Block size and blocks kept resident per SM, i.e. the register budget per thread
+    // (65536 / (threads * min_blocks)): sized so each class's tile fits without spilling.  The
+    // real m <= 24 tile fits 96 registers, which 128-thread blocks turn into 20 resident warps
+    // per SM (256-thread blocks would round down to 16).
+    static constexpr int threads = (!CPLX && MHI > 16 && MHI <= 24) ? 128 : 256;
     static constexpr int min_blocks = CPLX ? (MHI <= 16 ? 2 : 1)
-                                           : (MHI <= 8 ? 4 : (MHI <= 16 ? 3 : (MHI <= 32 ? 2 : 1)));
+                                           : (MHI <= 8 ? 4 : (MHI <= 16 ? 3 : (MHI <= 24 ? 5 : (MHI <= 32 ? 2 : 1))));
 };
 
 template <bool CPLX, int MLO, int MHI>
-__global__ void __launch_bounds__(256, (SizeClass<CPLX, MHI>::min_blocks))
+__global__ void __launch_bounds__((SizeClass<CPLX, MHI>::threads), (SizeClass<CPLX, MHI>::min_blocks))
     sieve_fast_kernel(SieveArgs a, const int64_t *__restrict__ strides, int warps_per_block, dd *partial)
 {
     extern __shared__ double smem[];
@@ -524,8 +523,10 @@ __global__ void __launch_bounds__(256, (SizeClass<CPLX, MHI>::min_blocks))
     const int b = blockIdx.y;
     const SieveInst in = a.inst[b];
     const int E = in.E, n = in.n;
-    const int cs = a.nmax + 1;
     const FastWs w = fast_carve(smem + (size_t)wib * fast_ws_doubles(a.nmax, CPLX, MHI), a.nmax, CPLX, MHI);
+    // The La Budde table's entries left of column 0 must read as zero; nothing ever writes them.
+    for (int i = lane; i < (CPLX ? 2 : 1) * (MHI + 1) * (MHI + 1); i += 32) w.C[i] = 0.0;
+    __syncwarp();
     const int wslot = blockIdx.x * warps_per_block + wib;
     const int64_t W = a.warps_per_inst;
     dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
@@ -574,11 +575,11 @@ __global__ void __launch_bounds__(256, (SizeClass<CPLX, MHI>::min_blocks))
             }
             __syncwarp();
             if constexpr (!CPLX) {
-                const double val = term_real<MHI, (MHI > 32 ? 2 : 1)>((const double *)a.Ax + in.ax_off, in.lda, E, mE, n, cs, w,
+                const double val = term_real<MHI, (MHI > 32 ? 2 : 1)>((const double *)a.Ax + in.ax_off, in.lda, E, mE, n, w,
                                                                       lane);
                 if (lane == 0) dd_add(acc_re, prefac * val);
             } else {
-                const cd val = term_cplx<MHI>((const cd *)a.Ax + in.ax_off, in.lda, E, mE, n, cs, w, lane);
+                const cd val = term_cplx<MHI>((const cd *)a.Ax + in.ax_off, in.lda, E, mE, n, w, lane);
                 if (lane == 0) {
                     dd_add(acc_re, prefac * val.re);
                     dd_add(acc_im, prefac * val.im);
@@ -600,12 +601,16 @@ size_t fast_smem_bytes(int nmax, int cplx, int cls, int warps)
 }
 
 template <bool CPLX, int MLO, int MHI>
-static int launch_one(const SieveArgs &a, const int64_t *strides, dim3 grid, int wpb, size_t smem, dd *partial,
+static int launch_one(const SieveArgs &a, const int64_t *strides, dim3 grid, int wpb, int cls, dd *partial,
                       cudaStream_t st)
 {
+    // The same warps per instance as every class (grid.x * wpb), in this class's block size.
+    constexpr int cw = SizeClass<CPLX, MHI>::threads / 32;
+    grid.x = (unsigned)((int64_t)grid.x * wpb / cw);
+    const size_t smem = fast_smem_bytes(a.nmax, CPLX, cls, cw);
     auto k = sieve_fast_kernel<CPLX, MLO, MHI>;
     EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grid, wpb * 32, smem, st>>>(a, strides, wpb, partial);
+    k<<<grid, cw * 32, smem, st>>>(a, strides, cw, partial);
     count_launch();
     EGG_CUDA_TRY(cudaGetLastError());
     return EGG_OK;
@@ -628,23 +633,22 @@ int launch_fast(const SieveArgs &a, const int64_t *strides, int B, int cplx, int
 {
     int rc = upload_tables(st);
     if (rc) return rc;
-    const size_t smem = fast_smem_bytes(a.nmax, cplx, cls, wpb);
     dim3 grid((unsigned)blocks_x, (unsigned)B);
     if (cplx) {
         switch (cls) {
-        case 0: return launch_one<true, 0, 8>(a, strides, grid, wpb, smem, partial, st);
-        case 1: return launch_one<true, 8, 16>(a, strides, grid, wpb, smem, partial, st);
-        case 2: return launch_one<true, 16, 24>(a, strides, grid, wpb, smem, partial, st);
-        case 3: return launch_one<true, 24, 32>(a, strides, grid, wpb, smem, partial, st);
+        case 0: return launch_one<true, 0, 8>(a, strides, grid, wpb, cls, partial, st);
+        case 1: return launch_one<true, 8, 16>(a, strides, grid, wpb, cls, partial, st);
+        case 2: return launch_one<true, 16, 24>(a, strides, grid, wpb, cls, partial, st);
+        case 3: return launch_one<true, 24, 32>(a, strides, grid, wpb, cls, partial, st);
         }
     } else {
         switch (cls) {
-        case 0: return launch_one<false, 0, 8>(a, strides, grid, wpb, smem, partial, st);
-        case 1: return launch_one<false, 8, 16>(a, strides, grid, wpb, smem, partial, st);
-        case 2: return launch_one<false, 16, 24>(a, strides, grid, wpb, smem, partial, st);
-        case 3: return launch_one<false, 24, 32>(a, strides, grid, wpb, smem, partial, st);
-        case 4: return launch_one<false, 32, 40>(a, strides, grid, wpb, smem, partial, st);
-        case 5: return launch_one<false, 40, 48>(a, strides, grid, wpb, smem, partial, st);
+        case 0: return launch_one<false, 0, 8>(a, strides, grid, wpb, cls, partial, st);
+        case 1: return launch_one<false, 8, 16>(a, strides, grid, wpb, cls, partial, st);
+        case 2: return launch_one<false, 16, 24>(a, strides, grid, wpb, cls, partial, st);
+        case 3: return launch_one<false, 24, 32>(a, strides, grid, wpb, cls, partial, st);
+        case 4: return launch_one<false, 32, 40>(a, strides, grid, wpb, cls, partial, st);
+        case 5: return launch_one<false, 40, 48>(a, strides, grid, wpb, cls, partial, st);
         }
     }
     return fail(EGG_ERR_ARGUMENT, "no such sieve size class");
