@@ -18,9 +18,12 @@
 // evaluates the CPU loop, so results are bit-identical to the reference's _haf_dp.  EGG_PREC_FMA
 // contracts each multiply-add as the reference's GPU kernel does.  EGG_PREC_MIXED multiplies in
 // FP32 and accumulates each state in FP64.  Integer inputs run exactly in Int128.
+#include <cooperative_groups.h>
 #include <type_traits>
 
 #include "egg_dp_common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace egg {
 
@@ -137,15 +140,38 @@ __global__ void __launch_bounds__(512) dp_small_kernel(const I *__restrict__ tra
 // suf now and its C(e - 1, j) joins pre one step later.  The arithmetic per state is that of the
 // plan kernels, in the same order, so results are identical.
 
+// Loads that bypass L1, for a level written earlier in the same kernel by other SMs (their L1
+// copies of the buffer, from two levels back, would be stale).
+template <class T> __device__ __forceinline__ T ld_l2(const T *p) { return __ldcg(p); }
+template <> __device__ __forceinline__ cd ld_l2<cd>(const cd *p)
+{
+    const double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
+    return cd{v.x, v.y};
+}
+template <> __device__ __forceinline__ cf ld_l2<cf>(const cf *p)
+{
+    const float2 v = __ldcg(reinterpret_cast<const float2 *>(p));
+    return cf{v.x, v.y};
+}
+template <> __device__ __forceinline__ __int128 ld_l2<__int128>(const __int128 *p)
+{
+    const longlong2 v = __ldcg(reinterpret_cast<const longlong2 *>(p));
+    return (__int128)(unsigned long long)v.x | ((__int128)v.y << 64);
+}
+
 // One step of the walk: load the child value and pair value for element ej, then advance
-// pre/suf/ej to the next element (if this is not the last step).
-template <class M, class PT, class HT, bool B1>
+// pre/suf/ej to the next element (if this is not the last step).  L2ONLY reads the child level
+// through L2 only.
+template <class M, class PT, class HT, bool B1, bool L2ONLY = false>
 __device__ __forceinline__ void walk_step(int x, int c, M &rest, uint32_t &pre, uint32_t &suf, uint32_t &padd, int &ej,
                                           const uint2 *TP, int ld, int pb, const PT *P, const HT *Hprev, int64_t B,
                                           int64_t b, HT &h, PT &p)
 {
     const uint32_t child = pre + suf;
-    if (B1) {
+    if (L2ONLY) {
+        h = ld_l2(Hprev + (B1 ? (int64_t)child : (int64_t)child * B + b));
+        p = B1 ? P[pb + ej] : P[(int64_t)(pb + ej) * B + b];
+    } else if (B1) {
         h = Hprev[child];
         p = P[pb + ej];
     } else {
@@ -167,7 +193,7 @@ __device__ __forceinline__ void walk_step(int x, int c, M &rest, uint32_t &pre, 
 // (instance b of B, instance-fastest; B1 when B == 1).  The loads of kBatch transitions are issued
 // before any of them is used, so a state waits for one memory round trip per batch rather than one
 // per transition; the accumulation order is unchanged.
-template <class Op, class M, class PT, class HT, class AT, bool B1>
+template <class Op, class M, class PT, class HT, class AT, bool B1, bool L2ONLY = false>
 __device__ __forceinline__ AT walk_state(M m, const uint2 *TP, int ld, int c, int K, int m0, const PT *P,
                                          const HT *Hprev, int64_t B, int64_t b)
 {
@@ -210,7 +236,7 @@ __device__ __forceinline__ AT walk_state(M m, const uint2 *TP, int ld, int c, in
         PT pv[kBatch];
 #pragma unroll
         for (int u = 0; u < kBatch; ++u)
-            walk_step<M, PT, HT, B1>(x + u, c, rest, pre, suf, padd, ej, TP, ld, pb, P, Hprev, B, b, hv[u], pv[u]);
+            walk_step<M, PT, HT, B1, L2ONLY>(x + u, c, rest, pre, suf, padd, ej, TP, ld, pb, P, Hprev, B, b, hv[u], pv[u]);
 #pragma unroll
         for (int u = 0; u < kBatch; ++u) acc = madd(Op{}, acc, pv[u], hv[u]);
     }
@@ -220,7 +246,7 @@ __device__ __forceinline__ AT walk_state(M m, const uint2 *TP, int ld, int c, in
 #pragma unroll
         for (int u = 0; u < kBatch; ++u)
             if (x + u <= c)
-                walk_step<M, PT, HT, B1>(x + u, c, rest, pre, suf, padd, ej, TP, ld, pb, P, Hprev, B, b, hv[u], pv[u]);
+                walk_step<M, PT, HT, B1, L2ONLY>(x + u, c, rest, pre, suf, padd, ej, TP, ld, pb, P, Hprev, B, b, hv[u], pv[u]);
 #pragma unroll
         for (int u = 0; u < kBatch; ++u)
             if (x + u <= c) acc = madd(Op{}, acc, pv[u], hv[u]);
@@ -304,6 +330,152 @@ __global__ void __launch_bounds__(kLevelThreads) dpc_level_kernel(const uint32_t
             store(Hcur[(s0 + sl) * B + b], acc);
         }
         __syncthreads();
+    }
+}
+
+// One state of a deep level evaluated by a whole warp (the levels near the top of a plan hold few
+// states with long transition lists, so a state per thread is one long dependent chain).
+//   * Unrank by complement: complementing reverses colex order, so state s of the c-subsets of U
+//     positions is the complement of the (U-c)-subset of rank C(U,c)-1-s.  Near the top U - c is
+//     small, and each of its elements is found by one ballot over candidate positions.
+//   * Lane l owns positions l and l+32.  Element x (1-based, x >= 2) at position e contributes
+//     a_x = C(e-1, x-1) to the child ranks of later elements and b_x = C(e-1, x-2) to earlier ones,
+//     so warp scans give every child rank pre_j + suf_j at once and all loads go out together.
+//   * Lane 0 then sums the transitions in plan order from shared memory (the same madd sequence as
+//     a thread walking the state, so the same bits).
+template <class Op, class PT, class HT, class AT>
+__device__ __forceinline__ void wide_state(uint32_t srank, int c, int K, const uint2 *TP, int ld, const PT *Ps, const HT *prev,
+                                           HT *cur, PT *pbuf, HT *hbuf, int lane)
+{
+    const int m0 = (K - c) / 2, U = K - m0, k = U - c;
+    // Complement of rank C(U,c)-1-s among k-subsets, element by element from the largest.
+    uint32_t R = TP[U * ld + c].x - 1u - srank;
+    uint64_t comp = 0;
+    int xprev = U;
+    for (int i = k; i >= 1; --i) {
+        int x = -1;
+        for (int base = xprev - 1; x < 0; base -= 32) {
+            const int cand = base - lane;
+            const bool ok = cand < 0 || TP[cand * ld + i].x <= R;  // C(cand, i) is nondecreasing in cand
+            const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            if (bal) x = base - (__ffs(bal) - 1);
+        }
+        x = x < 0 ? 0 : x;
+        comp |= (uint64_t)1 << x;
+        R -= TP[x * ld + i].x;
+        xprev = x;
+    }
+    const uint64_t all = U >= 64 ? ~(uint64_t)0 : (((uint64_t)1 << U) - 1);
+    const uint64_t mask = all & ~comp;
+    const int e1 = __ffsll((long long)mask) - 1;
+    // Positions p0 = lane, p1 = lane + 32: element index, contributions.
+    uint32_t a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+    int x0 = 0, x1 = 0;
+    const int p0 = lane, p1 = lane + 32;
+    if (p0 < U && ((mask >> p0) & 1)) {
+        x0 = __popcll(mask & (((uint64_t)1 << p0) - 1)) + 1;
+        if (x0 >= 2) {
+            const uint2 t = TP[(p0 - 1) * ld + (x0 - 2)];
+            b0 = t.x;
+            a0 = t.y;
+        }
+    }
+    if (p1 < U && ((mask >> p1) & 1)) {
+        x1 = __popcll(mask & (((uint64_t)1 << p1) - 1)) + 1;
+        if (x1 >= 2) {
+            const uint2 t = TP[(p1 - 1) * ld + (x1 - 2)];
+            b1 = t.x;
+            a1 = t.y;
+        }
+    }
+    // Inclusive scans over positions 0..63 (low half in lanes, then the high half).
+    uint32_t sa0 = a0, sb0 = b0, sa1 = a1, sb1 = b1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t ta0 = __shfl_up_sync(0xffffffffu, sa0, o), tb0 = __shfl_up_sync(0xffffffffu, sb0, o);
+        const uint32_t ta1 = __shfl_up_sync(0xffffffffu, sa1, o), tb1 = __shfl_up_sync(0xffffffffu, sb1, o);
+        if (lane >= o) {
+            sa0 += ta0;
+            sb0 += tb0;
+            sa1 += ta1;
+            sb1 += tb1;
+        }
+    }
+    const uint32_t lowa = __shfl_sync(0xffffffffu, sa0, 31), lowb = __shfl_sync(0xffffffffu, sb0, 31);
+    const uint32_t totb = lowb + __shfl_sync(0xffffffffu, sb1, 31);
+    sa1 += lowa;
+    sb1 += lowb;
+    const int ib = e1 + m0 + 1;
+    const int pb = (ib - 1) * K - (ib * (ib + 1)) / 2 + m0;
+    // pre_j = sum of a over earlier elements (exclusive), suf_j = sum of b over later ones.
+    if (x0 >= 2) {
+        const uint32_t child = (sa0 - a0) + (totb - sb0);
+        pbuf[x0 - 2] = Ps[pb + p0];
+        hbuf[x0 - 2] = ld_l2(prev + child);
+    }
+    if (x1 >= 2) {
+        const uint32_t child = (sa1 - a1) + (totb - sb1);
+        pbuf[x1 - 2] = Ps[pb + p1];
+        hbuf[x1 - 2] = ld_l2(prev + child);
+    }
+    __syncwarp();
+    if (lane == 0) {
+        AT acc = zero_of<AT>();
+        for (int j = 0; j < c - 1; ++j) acc = madd(Op{}, acc, pbuf[j], hbuf[j]);
+        store(cur[srank], acc);
+    }
+    __syncwarp();
+}
+
+// Levels at or above this popcount run a warp per state inside a span launch.
+static constexpr int kWideMinC = 14;
+
+// Several consecutive small levels of one instance in one cooperative launch: the levels at either
+// end of a plan hold few states each, so a launch per level costs mostly its fixed overhead (the
+// table fill, the pairs and the launch itself).  Here the table is filled once, a grid-wide
+// barrier separates the levels, and the previous level is read through L2 (the ping-pong buffers
+// are rewritten within the launch).  Shallow levels run a thread per state, deep ones a warp per
+// state (wide_state); both keep the level kernels' arithmetic and order.
+template <class Op, class PT, class HT, class AT>
+__global__ void __launch_bounds__(256) dpc_span_kernel(const uint32_t *__restrict__ binom, const PT *__restrict__ P, HT *H0,
+                                                       HT *H1, HT *out, int K, int L0, int L1, int out_last)
+{
+    cg::grid_group grid = cg::this_grid();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ld = K + 2;  // columns 0..K+1, so every C(x, k + 1) the walk reads is in the table
+    uint2 *TP = reinterpret_cast<uint2 *>(smem_raw);
+    PT *Ps = reinterpret_cast<PT *>(smem_raw + (((size_t)(K + 1) * ld * sizeof(uint2) + 15) / 16) * 16);
+    const int npairs = K * (K - 1) / 2;
+    unsigned char *wbuf = reinterpret_cast<unsigned char *>(Ps) + (((size_t)npairs * sizeof(PT) + 15) / 16) * 16;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    HT *hbuf = reinterpret_cast<HT *>(wbuf) + wid * 64;
+    PT *pbuf = reinterpret_cast<PT *>(wbuf + (size_t)(blockDim.x / 32) * 64 * sizeof(HT)) + wid * 64;
+    fill_pair_table(TP, binom, K + 1, ld, threadIdx.x, blockDim.x);
+    for (int q = threadIdx.x; q < npairs; q += blockDim.x) Ps[q] = P[q];
+    __syncthreads();
+    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nwarps = nth / 32, gwarp = tid / 32;
+    for (int L = L0; L <= L1; ++L) {
+        const int c = 2 * L, m0 = (K - c) / 2, U = K - m0;
+        const int64_t n = TP[U * ld + c].x;
+        HT *cur = (L == L1 && out_last) ? out : ((L & 1) ? H1 : H0);
+        const HT *prev = (L & 1) ? H0 : H1;
+        if (c >= kWideMinC) {
+            for (int64_t s = gwarp; s < n; s += nwarps) wide_state<Op, PT, HT, AT>((uint32_t)s, c, K, TP, ld, Ps, prev, cur, pbuf, hbuf, lane);
+        } else {
+            for (int64_t s = tid; s < n; s += nth) {
+                HT v;
+                if (c == 2) {
+                    v = first_level_value<Op, PT, HT, AT>(s, K, Ps, 1, 0);
+                } else {
+                    const uint64_t m = colex_unrank<uint64_t>(TP, ld, U, c, (uint32_t)s);
+                    store(v, walk_state<Op, uint64_t, PT, HT, AT, true, true>(m, TP, ld, c, K, m0, Ps, prev, 1, 0));
+                }
+                cur[s] = v;
+            }
+        }
+        if (L < L1) grid.sync();
     }
 }
 
@@ -490,8 +662,51 @@ static int launch_closed_level(const uint32_t *bt, const PT *P, const HT *prev, 
     return EGG_OK;
 }
 
+// Levels whose states and transitions together stay below this run inside a span launch.
+static constexpr int64_t kSpanWork = (int64_t)1 << 18;
+
+static bool span_level(const DevPlan &plan, int L)
+{
+    const Level &lv = plan.levels[L];
+    return lv.n * (lv.deg > 1 ? lv.deg : 1) <= kSpanWork;
+}
+
+// Levels L0..L1 (L0 >= 1) of one instance in one cooperative launch (dpc_span_kernel).
+template <class Op, class PT, class HT, class AT>
+static int launch_span(const uint32_t *bt, const DevPlan &plan, const PT *P, HT *h0, HT *h1, HT *out, bool out_last, int L0,
+                       int L1, cudaStream_t st)
+{
+    const int K = plan.K;
+    auto k = dpc_span_kernel<Op, PT, HT, AT>;
+    const size_t smem = (((size_t)(K + 1) * (K + 2) * sizeof(uint2) + 15) / 16) * 16 +
+                        (((size_t)K * (K - 1) / 2 * sizeof(PT) + 15) / 16) * 16 + (size_t)8 * 64 * (sizeof(HT) + sizeof(PT));
+    static bool attr_set = false;  // per instantiation; callers hold the library's lock
+    if (!attr_set) {
+        EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+        attr_set = true;
+    }
+    int per_sm = 0;
+    EGG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
+    if (per_sm < 1) return fail(EGG_ERR_CUDA, "span kernel cannot be resident");
+    int64_t need = 1;  // threads the widest level can use (a warp per state for deep levels)
+    for (int L = L0; L <= L1; ++L) {
+        const int64_t t = plan.levels[L].n * (2 * L >= kWideMinC ? 32 : 1);
+        need = t > need ? t : need;
+    }
+    int64_t blocks = (need + 255) / 256;
+    const int64_t cap = (int64_t)per_sm * ctx().num_sms;
+    if (blocks > cap) blocks = cap;
+    int oln = out_last ? 1 : 0;
+    void *args[] = {(void *)&bt, (void *)&P, (void *)&h0, (void *)&h1, (void *)&out, (void *)&K, (void *)&L0, (void *)&L1,
+                    (void *)&oln};
+    EGG_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k, dim3((unsigned)blocks), dim3(256), args, smem, st));
+    count_launch();
+    return EGG_OK;
+}
+
 // A closed-form plan: one launch for small degrees, else one launch per level with the last level
-// written straight into `out` when the state type is the output type.
+// written straight into `out` when the state type is the output type.  For one instance, the runs of
+// small levels at either end of the plan each take one span launch.
 template <class Op, class PT, class HT, class AT>
 static int run_closed(const DevPlan &plan, const PT *P, HT *h0, HT *h1, HT *out, bool out_direct, int64_t B,
                       cudaStream_t st)
@@ -519,13 +734,28 @@ static int run_closed(const DevPlan &plan, const PT *P, HT *h0, HT *h1, HT *out,
         if (plan.levels[L].n >= ((int64_t)1 << 31))
             return fail(EGG_ERR_TOO_LARGE, "a level of the degree-" + std::to_string(K) + " plan has 2^31 states or more");
     const int nlev = (int)plan.levels.size();
-    HT *prev = (1 == nlev - 1 && out_direct) ? out : h1;  // level c = 2 lands in h1 (odd level)
-    {
+    int Lh = 0, Lt = nlev;  // levels 1..Lh and Lt..nlev-1 run as spans
+    if (B == 1 && K <= 62) {
+        while (Lh + 1 < nlev && span_level(plan, Lh + 1)) ++Lh;
+        while (Lt - 1 > Lh + 1 && span_level(plan, Lt - 1)) --Lt;
+        if (Lh < 2) Lh = 0;            // a span of one level gains nothing
+        if (nlev - Lt < 2) Lt = nlev;
+    }
+    HT *prev;
+    int Lnext;
+    if (Lh) {
+        rc = launch_span<Op, PT, HT, AT>(bt, plan, P, h0, h1, out, out_direct && Lh == nlev - 1, 1, Lh, st);
+        if (rc) return rc;
+        prev = (Lh == nlev - 1 && out_direct) ? out : ((Lh & 1) ? h1 : h0);
+        Lnext = Lh + 1;
+    } else {
+        prev = (1 == nlev - 1 && out_direct) ? out : h1;  // level c = 2 lands in h1 (odd level)
         const int64_t total = plan.levels[1].n * B;
         dpc_first_kernel<Op, PT, HT, AT><<<grid_for(total, 256), 256, 0, st>>>(P, prev, K, plan.levels[1].n, B);
         count_launch();
+        Lnext = 2;
     }
-    for (int L = 2; L < nlev; ++L) {
+    for (int L = Lnext; L < Lt; ++L) {
         const int c = 2 * L;
         HT *cur = (L == nlev - 1 && out_direct) ? out : ((L & 1) ? h1 : h0);
         const int U = K - (K - c) / 2;
@@ -533,6 +763,10 @@ static int run_closed(const DevPlan &plan, const PT *P, HT *h0, HT *h1, HT *out,
                      : launch_closed_level<Op, uint64_t, PT, HT, AT>(bt, P, prev, cur, K, c, plan.levels[L].n, B, st);
         if (rc) return rc;
         prev = cur;
+    }
+    if (Lt < nlev) {
+        rc = launch_span<Op, PT, HT, AT>(bt, plan, P, h0, h1, out, out_direct, Lt, nlev - 1, st);
+        if (rc) return rc;
     }
     EGG_CUDA_TRY(cudaGetLastError());
     return EGG_OK;
