@@ -16,6 +16,7 @@ Differences from the reference, all additive:
 from __future__ import annotations
 
 import os
+from functools import lru_cache
 import threading
 
 import numpy as np
@@ -38,8 +39,11 @@ class B200Backend:
         return f"B200Backend({self.device})"
 
 
+_NTHREADS = os.cpu_count() or 1
+
+
 def _default_nthreads() -> int:
-    return os.cpu_count() or 1
+    return _NTHREADS
 
 
 # ----------------------------------------------------------------------------------------------
@@ -161,10 +165,20 @@ def _check_symmetric(A: np.ndarray) -> None:
 # Device calls
 # ----------------------------------------------------------------------------------------------
 
+@lru_cache(maxsize=None)
 def _triu_pairs(K: int) -> tuple[np.ndarray, np.ndarray]:
-    """(i, j) 0-based for q = 1..K(K-1)/2 in _pair_index order (row-major upper triangle)."""
+    """(i, j) 0-based for q = 1..K(K-1)/2 in _pair_index order (row-major upper triangle).
+    Cached per degree; the arrays are read-only."""
     iu, ju = np.triu_indices(K, 1)
+    iu.setflags(write=False)
+    ju.setflags(write=False)
     return iu, ju
+
+
+def _gather_pairs_one(T: np.dtype, A: np.ndarray) -> np.ndarray:
+    """The 1 x npairs P of a single K x K matrix (the rows taken in order)."""
+    iu, ju = _triu_pairs(A.shape[0])
+    return A[iu, ju].astype(T, copy=False).reshape(1, -1)
 
 
 def _gather_pairs_batch(T: np.dtype, mats: np.ndarray, idxs: np.ndarray, K: int) -> np.ndarray:
@@ -316,7 +330,7 @@ def hafnian(A, *, nthreads: int | None = None, glynn: bool | None = None, method
     if exact_int and chosen == "sieve":
         raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
     if chosen in ("unrolled", "dp"):
-        P = _gather_pairs_batch(T, A, np.arange(N, dtype=np.int64)[None, :], N)
+        P = _gather_pairs_one(T, A)
         v = _dp_device(T, P, N, _dp_prec(prec), None, exact_int)[0]
         return v if exact_int else T.type(v)
     return _sieve_one(T, _permuted(T, A, _distinct_x(E)), [1] * E, use_glynn, prec)

@@ -182,6 +182,7 @@ def _choose_method(K: int, edge_reps, nthreads: int) -> tuple[str, bool]:
     return _decide(K, wg, sg, wi, si, len(edge_reps), n, nthreads)
 
 
+@lru_cache(maxsize=None)
 def _choose_method_distinct(K: int, E: int, nthreads: int) -> tuple[str, bool]:
     """As _choose_method for all-ones multiplicities (:951-956)."""
     if E == 0:
