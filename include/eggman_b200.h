@@ -177,6 +177,16 @@ int egg_sieve_batch(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax
 int egg_sieve_batch_device(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax, const int64_t *E,
                            const int64_t *edge_reps, const int32_t *glynn, void *out, void *stream);
 
+/* One sieve summed exactly as the reference sums it: every term in the reference's arithmetic
+ * (as EGG_PREC_EXACT), then plain FP64 `+=` over `nchunks` equal chunks of the term range, each
+ * in term order, and the chunk sums left to right, times 2^-(n-1) under Glynn
+ * (_sieve_sum, src/hafnian.jl:713-738).  With nchunks = _sieve_chunks(work, steps, nthreads)
+ * (src/hafnian.jl:646-647) the result is bit-identical to _calc_hafnian(Ax, edge_reps; nthreads,
+ * glynn) run with that thread count.  Host pointers; the terms are kept on the device, so sieves
+ * of more than 2^28 terms are refused with EGG_ERR_TOO_LARGE. */
+int egg_sieve_reference_sum(int dtype, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, int64_t nchunks,
+                            void *out);
+
 /* ---- mixed-degree batches -------------------------------------------------------------- */
 
 /* Hafnians of B principal submatrices of one parent: instance b is A[r, r] with

@@ -158,3 +158,57 @@ def test_config2_full_size_cross_check(egg, W):
         # FP64 evaluation lands ~1e-9 away; the reference's own CPU result differs from the DP by 5e-10.
         assert rel(ie, dp) < 1e-8, prec
     egg.empty_gpu_cache()
+
+
+# ---- prec="reference": the reference's summation order -----------------------------------------
+# Every term in the reference's arithmetic (the exact kernel), summed as _sieve_sum does for the
+# given thread count: nchunks = _sieve_chunks(work, steps, nthreads) chunks of the term range, each a
+# plain FP64 sum from zero, the chunk sums folded left to right (src/hafnian.jl:607-622, :714-738).
+# The bar is equality with the oracle's sum_mode 0, which restates that summation.
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("glynn", [False, True])
+def test_reference_order_bit_identical(egg, orc, W, cplx, glynn):
+    multi = False
+    for N in (2, 8, 14, 20, 24, 30):
+        A = W.dense_complex(N, 300 + N, 0.5) if cplx else W.dense_real(N, 300 + N)
+        E = N // 2
+        Ax = orc.permuted(A, distinct_x(E))
+        work, steps = orc.sieve_variant_cost([1] * E, E, glynn)
+        for k in (1, 3, 12, 64):
+            multi |= orc.sieve_chunks(work, steps, k) > 1
+            want = orc.calc_hafnian(Ax, [1] * E, glynn, nthreads=k, sum_mode=0)
+            got = egg.sieve(Ax, [1] * E, glynn=glynn, prec="reference", nthreads=k)
+            assert complex(got) == complex(want), (N, k, got, want)
+    assert multi  # the sizes above reach the threaded (several-chunk) summation
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_reference_order_repeated_rows(egg, orc, W, cplx):
+    """hafnian_repeated's mixed-radix odometer, both variants, through the public entry point."""
+    A = W.dense_complex(10, 91, 0.5) if cplx else W.dense_real(10, 91)
+    for rpt in ([2, 3, 1, 0, 2, 2, 1, 3, 1, 1], [4, 4, 2, 2, 2, 2, 0, 0, 1, 1], [2] * 10):
+        x, er = orc.matched_reps(rpt)
+        Ax = orc.permuted(A, x)
+        for glynn in (False, True):
+            for k in (1, 7, 32):
+                want = orc.calc_hafnian(Ax, er, glynn, nthreads=k, sum_mode=0)
+                got = egg.hafnian_repeated(A, rpt, method="sieve", glynn=glynn, prec="reference", nthreads=k)
+                assert complex(got) == complex(want), (rpt, glynn, k, got, want)
+
+
+def test_reference_order_public_api(egg, orc, W):
+    """hafnian(A; method, nthreads) end to end, the method choice included, and the batch form
+    (each instance with one thread, as the reference's batch loop runs them)."""
+    for N in (16, 22, 26):
+        A = W.dense_real(N, 700 + N)
+        for k in (1, 8, 12):
+            for method in ("auto", "sieve"):
+                want = orc.hafnian(A, method=method, nthreads=k)
+                got = egg.hafnian(A, method=method, prec="reference", nthreads=k)
+                assert complex(got) == complex(want), (N, k, method)
+    mats = [W.dense_real(18, 800 + b) for b in range(3)]
+    got = egg.hafnian(mats, method="sieve", prec="reference")
+    want = [orc.hafnian(m, method="sieve", nthreads=1) for m in mats]
+    assert [complex(g) for g in got] == [complex(w) for w in want]
+    assert egg.sieve(np.zeros((0, 0)), [], prec="reference") == 1.0

@@ -44,7 +44,7 @@ EXPORTS = (
     "egg_dp_batch_bytes", "egg_dp_counts", "egg_plan_upload", "egg_plan_build", "egg_plan_info",
     "egg_plan_download", "egg_plan_release", "egg_dp_batch", "egg_dp_batch_device", "egg_sieve",
     "egg_sieve_device", "egg_sieve_batch", "egg_sieve_batch_device", "egg_sieve_device_noalloc", "egg_launch_count",
-    "egg_dp_mix", "egg_dp_mix_device", "egg_dp_mix_tuning", "egg_dp_mix_set_tuning",
+    "egg_dp_mix", "egg_dp_mix_device", "egg_dp_mix_tuning", "egg_dp_mix_set_tuning", "egg_sieve_reference_sum",
 )
 
 
@@ -108,6 +108,7 @@ def lib() -> ctypes.CDLL:
     L.egg_dp_mix_device.argtypes = [i32, i32, vp, i64, i64, vp, vp, vp, vp]
     L.egg_dp_mix_tuning.argtypes = [i32, i32, i32, vp, vp]
     L.egg_dp_mix_set_tuning.argtypes = [i32, i32, i32, i32, i64]
+    L.egg_sieve_reference_sum.argtypes = [i32, vp, i64, vp, i32, i64, vp]
     return L
 
 

@@ -551,4 +551,25 @@ int egg_dp_mix_tuning(int K, int dtype, int prec, int *batched, int64_t *group)
     return mix_tuned(K, dtype, prec, batched, group);
 }
 
+int egg_sieve_reference_sum(int dtype, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn, int64_t nchunks,
+                            void *out)
+{
+    EGG_GUARD();
+    if (dtype != EGG_F64 && dtype != EGG_C128) return fail(EGG_ERR_ARGUMENT, "the sieve runs in Float64 or ComplexF64");
+    if (E < 0 || E > 32) return fail(EGG_ERR_TOO_LARGE, "the device sieve supports up to 32 edges (N <= 64)");
+    if (!out || (E > 0 && (!Ax || !edge_reps))) return fail(EGG_ERR_ARGUMENT, "null argument");
+    Context &c = ctx();
+    const size_t es = dtype_size(dtype);
+    const size_t abytes = (size_t)(2 * E) * (2 * E) * es;
+    int rc = ensure_buf(c.scratch[3], abytes + 64);
+    if (!rc) rc = ensure_buf(c.scratch[4], 64);
+    if (rc) return rc;
+    if (abytes) EGG_CUDA_TRY(cudaMemcpyAsync(c.scratch[3].ptr, Ax, abytes, cudaMemcpyHostToDevice, c.stream));
+    rc = sieve_reference_sum_run(dtype, c.scratch[3].ptr, E, edge_reps, glynn, nchunks, c.scratch[4].ptr, c.stream);
+    if (rc) return rc;
+    EGG_CUDA_TRY(cudaMemcpyAsync(out, c.scratch[4].ptr, es, cudaMemcpyDeviceToHost, c.stream));
+    EGG_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    return EGG_OK;
+}
+
 }  // extern "C"

@@ -132,8 +132,8 @@ struct Context {
     cudaStream_t stream = nullptr;
     int num_sms = 0;
     std::map<std::pair<int, int>, DevPlan> plans;
-    DevBuf scratch[8];   // H, P, out, sieve matrix, sieve out, misc, mixed-degree batch + its staging:
-                         // grown on demand, never shrunk
+    DevBuf scratch[9];   // H, P, out, sieve matrix, sieve out, misc, mixed-degree batch + its staging:
+                         // the reference-order sieve's terms: grown on demand, never shrunk
     std::recursive_mutex mu;
 };
 
@@ -201,7 +201,12 @@ int sieve_run(int dtype, int prec, const void *dAx, int64_t E, const int64_t *ed
               cudaStream_t st);
 int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
                     const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st,
-                    const FixedScratch *fixed = nullptr);
+                    const FixedScratch *fixed = nullptr, double *terms = nullptr);
+// One sieve summed as the reference sums it (_sieve_sum, src/hafnian.jl:713-738): every term in the
+// reference's arithmetic, then plain FP64 sums over `nchunks` equal chunks of the term range, each
+// in term order, and the chunk sums left to right.  Host edge_reps, device Ax and out.
+int sieve_reference_sum_run(int dtype, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, int64_t nchunks,
+                            void *dout, cudaStream_t st);
 
 inline size_t dtype_size(int dtype)
 {

@@ -352,7 +352,17 @@ __device__ void sieve_warp_exact(const SieveArgs &a, const SieveInst &in, WarpWs
         prefac = __shfl_sync(0xffffffffu, prefac, 0);
         __syncwarp();
         const int m = 2 * mE;
-        if (m == 0) continue;           // empty submatrix contributes zero (:566-567)
+        if (m == 0) {                   // empty submatrix contributes zero (:566-567)
+            if (a.terms && lane == 0) {
+                if (CPLX) {
+                    a.terms[2 * j] = 0.0;
+                    a.terms[2 * j + 1] = 0.0;
+                } else {
+                    a.terms[j] = 0.0;
+                }
+            }
+            continue;
+        }
         if (m <= a.skip_le) continue;   // evaluated by the fast kernels
         const int ld = w.ldm;
         // M = A_S X D (:582-593).
@@ -372,7 +382,8 @@ __device__ void sieve_warp_exact(const SieveArgs &a, const SieveInst &in, WarpWs
             charpoly_real_exact(w, m, n, lane);
             if (lane == 0) {
                 const double val = inv_sqrt_real_exact(w.C + (size_t)m * (n + 1), w.f, m, n);
-                dd_add(acc_re, __dmul_rn(prefac, val));
+                if (a.terms) a.terms[j] = __dmul_rn(prefac, val);
+                else dd_add(acc_re, __dmul_rn(prefac, val));
             }
         } else {
             const cd *Ax = (const cd *)a.Ax + in.ax_off;
@@ -393,8 +404,13 @@ __device__ void sieve_warp_exact(const SieveArgs &a, const SieveInst &in, WarpWs
             charpoly_cplx_exact(w, m, n, lane);
             if (lane == 0) {
                 const cd val = inv_sqrt_cplx_exact((const cd *)w.C + (size_t)m * (n + 1), (cd *)w.f, m, n);
-                dd_add(acc_re, __dmul_rn(prefac, val.re));
-                dd_add(acc_im, __dmul_rn(prefac, val.im));
+                if (a.terms) {
+                    a.terms[2 * j] = __dmul_rn(prefac, val.re);
+                    a.terms[2 * j + 1] = __dmul_rn(prefac, val.im);
+                } else {
+                    dd_add(acc_re, __dmul_rn(prefac, val.re));
+                    dd_add(acc_im, __dmul_rn(prefac, val.im));
+                }
             }
         }
         __syncwarp();
@@ -490,8 +506,10 @@ static int64_t align256(int64_t x) { return (x + 255) & ~(int64_t)255; }
 
 int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
                     const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st,
-                    const FixedScratch *fixed)
+                    const FixedScratch *fixed, double *terms)
 {
+    // terms: instead of summing, store every term of the single instance (exact kernel).
+    if (terms && (B != 1 || prec != EGG_PREC_EXACT)) return fail(EGG_ERR_ARGUMENT, "term output needs one instance in exact mode");
     Context &c = ctx();
     const int num_sms = fixed ? fixed->num_sms : c.num_sms;
     const int cplx = dtype == EGG_C128;
@@ -622,6 +640,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.Emax = Ews;
     a.nmax = nmax;
     a.skip_le = skip_le;
+    a.terms = terms;
     PartialSet ps;
     for (int k = 0; k < 7; ++k) {
         ps.p[k] = nullptr;
@@ -657,6 +676,10 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         ps.p[0] = a.partial;
         ps.w[0] = a.warps_per_inst;
     }
+    if (terms) {
+        EGG_CUDA_TRY(cudaGetLastError());
+        return EGG_OK;
+    }
     if (cplx) sieve_reduce_kernel<true><<<(unsigned)B, 256, 0, st>>>(ps, a.inst, dout);
     else sieve_reduce_kernel<false><<<(unsigned)B, 256, 0, st>>>(ps, a.inst, dout);
     count_launch();
@@ -672,6 +695,93 @@ int sieve_run(int dtype, int prec, const void *dAx, int64_t E, const int64_t *ed
     std::vector<int64_t> reps(edge_reps, edge_reps + E);
     if (reps.empty()) reps.push_back(0);
     return sieve_batch_run(dtype, prec, 1, E, dAx, &e, reps.data(), &g, dout, st, nullptr);
+}
+
+// ---- the reference's summation ------------------------------------------------------------------
+
+// Chunk c of [0, steps) (c = 0..nchunks-1, the reference's div((c-1) steps, nchunks) bounds, 0-based):
+// a plain FP64 sum in term order, starting from zero.
+template <bool CPLX>
+__global__ void sieve_chunk_sum_kernel(const double *__restrict__ terms, int64_t steps, int64_t nchunks, double *__restrict__ part)
+{
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= nchunks) return;
+    const int64_t lo = (c * steps) / nchunks, hi = ((c + 1) * steps) / nchunks;
+    double hr = 0.0, hi_ = 0.0;
+    for (int64_t j = lo; j < hi; ++j) {
+        if (CPLX) {
+            hr = __dadd_rn(hr, terms[2 * j]);
+            hi_ = __dadd_rn(hi_, terms[2 * j + 1]);
+        } else {
+            hr = __dadd_rn(hr, terms[j]);
+        }
+    }
+    part[2 * c] = hr;
+    part[2 * c + 1] = hi_;
+}
+
+// The chunk sums left to right (Julia's sum over a short array), then Glynn's 2^-(n-1).
+template <bool CPLX>
+__global__ void sieve_chunk_fold_kernel(const double *__restrict__ part, int64_t nchunks, int glynn, int n, double *__restrict__ out)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double hr = part[0], hi_ = part[1];
+    for (int64_t c = 1; c < nchunks; ++c) {
+        hr = __dadd_rn(hr, part[2 * c]);
+        hi_ = __dadd_rn(hi_, part[2 * c + 1]);
+    }
+    if (glynn) {
+        double s = 1.0;  // R(0.5)^(n-1), exact
+        for (int i = 0; i < n - 1; ++i) s = __dmul_rn(s, 0.5);
+        hr = __dmul_rn(hr, s);
+        hi_ = __dmul_rn(hi_, s);
+    }
+    out[0] = hr;
+    if (CPLX) out[1] = hi_;
+}
+
+int sieve_reference_sum_run(int dtype, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, int64_t nchunks,
+                            void *dout, cudaStream_t st)
+{
+    const int cplx = dtype == EGG_C128;
+    if (dtype != EGG_F64 && dtype != EGG_C128) return fail(EGG_ERR_ARGUMENT, "the sieve runs in Float64 or ComplexF64");
+    if (nchunks < 1) return fail(EGG_ERR_ARGUMENT, "nchunks must be >= 1");
+    std::vector<int64_t> reps(edge_reps, edge_reps + E);
+    if (reps.empty()) reps.push_back(0);
+    const int64_t steps = term_count(reps.data(), E, glynn);
+    if (steps < 0) return fail(EGG_ERR_TOO_LARGE, "the sieve's term count overflows Int64");
+    if (steps == 0) {  // no edges: the hafnian of the empty matrix
+        const double one[2] = {1.0, 0.0};
+        EGG_CUDA_TRY(cudaMemcpyAsync(dout, one, cplx ? 16 : 8, cudaMemcpyHostToDevice, st));
+        return EGG_OK;
+    }
+    if (steps > ((int64_t)1 << 28))
+        return fail(EGG_ERR_TOO_LARGE, "the reference-order sum keeps every term; " + std::to_string(steps) +
+                                           " terms exceed its limit of 2^28");
+    if (nchunks > steps) nchunks = steps;
+    int n = 0;
+    for (int64_t i = 0; i < E; ++i) n += (int)edge_reps[i];
+    Context &c = ctx();
+    const size_t tbytes = (size_t)steps * (cplx ? 16 : 8), pbytes = (size_t)nchunks * 16;
+    int rc = ensure_buf(c.scratch[8], tbytes + pbytes + 256);
+    if (rc) return rc;
+    double *terms = (double *)c.scratch[8].ptr;
+    double *part = (double *)((char *)c.scratch[8].ptr + ((tbytes + 255) / 256) * 256);
+    int32_t g = glynn ? 1 : 0;
+    int64_t e = E;
+    rc = sieve_batch_run(dtype, EGG_PREC_EXACT, 1, E, dAx, &e, reps.data(), &g, nullptr, st, nullptr, terms);
+    if (rc) return rc;
+    const unsigned blocks = (unsigned)((nchunks + 255) / 256);
+    if (cplx) {
+        sieve_chunk_sum_kernel<true><<<blocks, 256, 0, st>>>(terms, steps, nchunks, part);
+        sieve_chunk_fold_kernel<true><<<1, 32, 0, st>>>(part, nchunks, glynn, n, (double *)dout);
+    } else {
+        sieve_chunk_sum_kernel<false><<<blocks, 256, 0, st>>>(terms, steps, nchunks, part);
+        sieve_chunk_fold_kernel<false><<<1, 32, 0, st>>>(part, nchunks, glynn, n, (double *)dout);
+    }
+    count_launch(2);
+    EGG_CUDA_TRY(cudaGetLastError());
+    return EGG_OK;
 }
 
 }  // namespace egg

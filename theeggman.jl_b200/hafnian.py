@@ -220,16 +220,18 @@ def _dp_device(T: np.dtype, P: np.ndarray, K: int, prec: str, max_batch, exact_i
 
 
 def _dp_prec(prec) -> str:
-    """DP rounding: the reference CPU's (exact) unless asked otherwise."""
-    return "exact" if prec is None else prec
+    """DP rounding: the reference CPU's (exact) unless asked otherwise.  'reference' is 'exact':
+    the DP's sum order is fixed by its plan, so its exact kernels already reproduce the reference
+    bit for bit."""
+    return "exact" if prec in (None, "reference") else prec
 
 
 def _sieve_prec(prec) -> int:
-    """Sieve kernel: reference loop order for prec='exact', the register-resident FMA kernels
-    otherwise (the default)."""
-    if prec not in (None, "exact", "fma", "mixed"):
-        raise ArgumentError("prec must be one of None, 'exact', 'fma', 'mixed'")
-    return nat.PREC["exact"] if prec == "exact" else nat.PREC["fma"]
+    """Sieve kernel: reference term arithmetic for prec='exact' (and 'reference', which also sums
+    in the reference's order), the register-resident FMA kernels otherwise (the default)."""
+    if prec not in (None, "exact", "fma", "mixed", "reference"):
+        raise ArgumentError("prec must be one of None, 'exact', 'fma', 'mixed', 'reference'")
+    return nat.PREC["exact"] if prec in ("exact", "reference") else nat.PREC["fma"]
 
 
 def _sieve_device_batch(T: np.dtype, Axs: list[np.ndarray], reps_list: list[list[int]], glynns: list[bool],
@@ -250,6 +252,11 @@ def _sieve_device_batch(T: np.dtype, Axs: list[np.ndarray], reps_list: list[list
     for b, r in enumerate(reps_list):
         reps[b, : len(r)] = r
     g = np.array([1 if x else 0 for x in glynns], dtype=np.int32)
+    if prec == "reference":
+        # The reference's batch loop runs each instance with nthreads = 1, i.e. one chunk
+        # (src/hafnian.jl:1297-1300, :1355-1358).
+        return np.array([_sieve_reference(T, Ax, list(r), bool(gl), 1) for Ax, r, gl in zip(Axs, reps_list, glynns)],
+                        dtype=T)
     out = np.zeros(B, CT)
     with _lock:
         nat.check(nat.lib().egg_sieve_batch(nat.EGG_C128 if cplx else nat.EGG_F64, _sieve_prec(prec), B, Emax, nat.ptr(slab),
@@ -257,9 +264,12 @@ def _sieve_device_batch(T: np.dtype, Axs: list[np.ndarray], reps_list: list[list
     return out.astype(T, copy=False)
 
 
-def _sieve_one(T: np.dtype, Ax: np.ndarray, edge_reps: list[int], glynn: bool, prec=None):
-    """The device sieve in place of _calc_hafnian(Ax, edge_reps; glynn) (src/hafnian.jl:684-738).
-    The sieve runs in FP64 (complex: ComplexF64); the result is returned in T."""
+def _sieve_one(T: np.dtype, Ax: np.ndarray, edge_reps: list[int], glynn: bool, prec=None, nthreads: int = 1):
+    """The device sieve in place of _calc_hafnian(Ax, edge_reps; nthreads, glynn)
+    (src/hafnian.jl:684-738).  The sieve runs in FP64 (complex: ComplexF64); the result is
+    returned in T.  `nthreads` matters only for prec='reference'."""
+    if prec == "reference":
+        return _sieve_reference(T, Ax, edge_reps, glynn, nthreads)
     cplx = np.dtype(T).kind == "c"
     CT = np.complex128 if cplx else np.float64
     E = len(edge_reps)
@@ -269,6 +279,27 @@ def _sieve_one(T: np.dtype, Ax: np.ndarray, edge_reps: list[int], glynn: bool, p
     with _lock:
         nat.check(nat.lib().egg_sieve(nat.EGG_C128 if cplx else nat.EGG_F64, _sieve_prec(prec), nat.ptr(A) if E else None, E,
                                       nat.ptr(reps), 1 if glynn else 0, nat.ptr(out)))
+    return np.dtype(T).type(out[0])
+
+
+def _sieve_reference(T: np.dtype, Ax: np.ndarray, edge_reps: list[int], glynn: bool, nthreads: int):
+    """_calc_hafnian(Ax, edge_reps; nthreads, glynn) to the last bit (src/hafnian.jl:684-738):
+    every term in the reference's arithmetic, summed in the reference's chunks, nchunks =
+    _sieve_chunks(work, steps, nthreads) (:646-647, :703-712), each chunk a plain FP64 sum from
+    zero (:607-622), the chunk sums folded left to right (:729-732), Glynn's 2^-(n-1) last."""
+    cplx = np.dtype(T).kind == "c"
+    CT = np.complex128 if cplx else np.float64
+    E = len(edge_reps)
+    if E == 0:
+        return np.dtype(T).type(1)
+    work, steps = pol._sieve_variant_cost(edge_reps, int(sum(edge_reps)), glynn)
+    nchunks = pol._sieve_chunks(work, steps, max(int(nthreads), 1))
+    A = np.asfortranarray(np.asarray(Ax, dtype=CT))
+    reps = np.ascontiguousarray(edge_reps, dtype=np.int64)
+    out = np.zeros(1, CT)
+    with _lock:
+        nat.check(nat.lib().egg_sieve_reference_sum(nat.EGG_C128 if cplx else nat.EGG_F64, nat.ptr(A), E, nat.ptr(reps),
+                                                    1 if glynn else 0, nchunks, nat.ptr(out)))
     return np.dtype(T).type(out[0])
 
 
@@ -333,7 +364,7 @@ def hafnian(A, *, nthreads: int | None = None, glynn: bool | None = None, method
         P = _gather_pairs_one(T, A)
         v = _dp_device(T, P, N, _dp_prec(prec), None, exact_int)[0]
         return v if exact_int else T.type(v)
-    return _sieve_one(T, _permuted(T, A, _distinct_x(E)), [1] * E, use_glynn, prec)
+    return _sieve_one(T, _permuted(T, A, _distinct_x(E)), [1] * E, use_glynn, prec, nthreads)
 
 
 def hafnian_repeated(A, rpt, *, nthreads: int | None = None, glynn: bool | None = None, method: str = "auto",
@@ -375,7 +406,7 @@ def hafnian_repeated(A, rpt, *, nthreads: int | None = None, glynn: bool | None 
         return v if exact_int else T.type(v)
     if exact_int:
         raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
-    return _sieve_one(T, _permuted(T, A, x), edge_reps, use_glynn, prec)
+    return _sieve_one(T, _permuted(T, A, x), edge_reps, use_glynn, prec, nthreads)
 
 
 def _hafnian_batch(As, *, nthreads, glynn, method, check_symmetric, backend, max_batch, prec, exact):
@@ -538,10 +569,12 @@ def reduction(A, rpt) -> np.ndarray:
     return A[np.ix_(idx, idx)]
 
 
-def sieve(Ax, edge_reps, *, glynn: bool = False, prec: str | None = None):
-    """The device sieve on a pre-permuted matrix: _calc_hafnian(Ax, edge_reps; glynn)
+def sieve(Ax, edge_reps, *, glynn: bool = False, prec: str | None = None, nthreads: int | None = None):
+    """The device sieve on a pre-permuted matrix: _calc_hafnian(Ax, edge_reps; nthreads, glynn)
     (src/hafnian.jl:684), the seam the reference has no device hook for.  prec='exact' evaluates
-    every term in the reference's order and rounding; the default uses the fast kernels."""
+    every term in the reference's rounding and sums them in double-double; prec='reference' also
+    sums them in the reference's order for `nthreads` threads, so the result is the reference's to
+    the last bit; the default uses the fast kernels."""
     Ax = np.asarray(Ax)
     T = _haf_dtype(Ax)
-    return _sieve_one(T, Ax, list(edge_reps), glynn, prec)
+    return _sieve_one(T, Ax, list(edge_reps), glynn, prec, nthreads or _default_nthreads())
