@@ -20,9 +20,10 @@
 //     vector that is mult_i on the live rows' slots and exactly 1 on the pivot slot, which yields
 //     the updated column s directly -- the next step's `pc` -- with no dynamic register index.
 //
-// Each finished Hessenberg column feeds La Budde's recurrence (src/hafnian.jl:454-492) at once:
-// lanes own coefficient orders t and walk the coefficient table (shared memory, one row per order
-// of leading minor) along a diagonal, one address step per term of the depth sum.  The [lambda^n] series coefficient
+// La Budde's recurrence (src/hafnian.jl:454-492): each finished Hessenberg column stores its
+// order-k coefficients; after the reduction lane d computes diagonal d of the coefficient table in
+// registers (labudde_diag).  Tiles of two rows per lane instead feed each column at once into a
+// shared-memory table walked along diagonals (labudde_row).  The [lambda^n] series coefficient
 // (src/hafnian.jl:502-514) is accumulated push-style: once f_s is known every lane t > s adds its
 // (t+s) q_{t-s} f_s, so each order costs one multiply-add per lane and one broadcast.  All arithmetic
 // is FP64 with fused multiply-adds; terms are accumulated in double-double per warp.
@@ -66,16 +67,32 @@ __device__ __forceinline__ unsigned pivot_key(double a, int slot)
 struct FastWs {
     double *prow;  // pivot row, by physical slot [64]
     double *wv;    // column-update weights, by physical slot [64]
-    double *cf;    // La Budde coefficients coef_i, by i [64] (complex: 32 values)
-    double *C;     // La Budde coefficient table by diagonals, (mhi+1) x (mhi+1) values (see labudde_row)
+    double *cf;    // La Budde coefficients coef_i, by i [64] (tiles of two rows per lane)
+    double *C;     // La Budde coefficient table by diagonals, (mhi+1) x (mhi+1) values (tiles of two
+                   // rows per lane, see labudde_row)
+    double *cft;   // La Budde coefficients of every order k, a triangle (one-row tiles, see labudde_diag)
+    double *hk;    // Hessenberg diagonal h_kk by k [mhi + 1] (one-row tiles)
+    double *q;     // det(I - lambda H) coefficients q_j by j [32] (one-row tiles)
     double *kval;  // multiplicities of the surviving edges after the Glynn substitution [32]
     int *eidx;     // surviving edges, compacted [32]
 };
 
-__host__ __device__ inline size_t fast_ws_doubles(int nmax, int cplx, int mhi)
+// Start of order k's row in the coefficient triangle (k = 1..mhi, k - 1 coefficients each).  Real
+// rows are padded to an even length so that each starts on a 16-byte boundary.
+__host__ __device__ constexpr int cft_row_real(int k) { return (k - 1) * (k - 2) / 2 + (k - 1) / 2; }
+__host__ __device__ constexpr int cft_row_cplx(int k) { return (k - 1) * (k - 2) / 2; }
+
+__host__ __device__ inline size_t fast_body_doubles(int cplx, int mhi)
 {
     const size_t v = cplx ? 2 : 1;  // doubles per value
-    size_t d = 64 * 3 + v * (size_t)(mhi + 1) * (mhi + 1) + 32 /*kval*/ + 16 /*eidx*/;
+    if (mhi > 32) return v * (size_t)(mhi + 1) * (mhi + 1);
+    const size_t tri = cplx ? 2 * (size_t)cft_row_cplx(mhi + 1) : (size_t)cft_row_real(mhi + 1);
+    return tri + v * (size_t)((mhi + 2) & ~1) + v * 32;
+}
+
+__host__ __device__ inline size_t fast_ws_doubles(int nmax, int cplx, int mhi)
+{
+    size_t d = 64 * 3 + fast_body_doubles(cplx, mhi) + 32 /*kval*/ + 16 /*eidx*/;
     return (d + 1) & ~(size_t)1;  // keep every warp's region 16-byte aligned
 }
 
@@ -87,7 +104,15 @@ __device__ inline FastWs fast_carve(double *base, int nmax, int cplx, int mhi)
     w.prow = p; p += 64;
     w.wv = p; p += 64;
     w.cf = p; p += 64;
-    w.C = p; p += v * (size_t)(mhi + 1) * (mhi + 1);
+    w.C = p;
+    w.cft = p;
+    if (mhi <= 32) {
+        w.hk = w.cft + (cplx ? 2 * (size_t)cft_row_cplx(mhi + 1) : (size_t)cft_row_real(mhi + 1));
+        w.q = w.hk + v * (size_t)((mhi + 2) & ~1);
+    } else {
+        w.hk = w.q = nullptr;
+    }
+    p += fast_body_doubles(cplx, mhi);
     w.kval = p; p += 32;
     w.eidx = (int *)p;
     return w;
@@ -143,47 +168,105 @@ __device__ __forceinline__ double series_coeff(const double *T, int m, int n, in
     return fs;
 }
 
-__device__ __forceinline__ void labudde_row_c(cd *T, const cd *cf, int k, int n, int rs, cd hkk, int lane)
+// ---- La Budde by diagonals, in registers (tiles of one row per lane) ------------------------------
+// The same recurrence as labudde_row, run after the Hessenberg reduction from the coefficients it
+// stored: for order k, cft[cft_row(k) + i - 1] = h_{i,k} prod_{l=i+1..k} h_{l,l-1} (i = 1..k-1) and
+// hk[k] = h_{k,k}.  Lane d owns diagonal d of the table, D[r] = C[r][r - d], zero left of column 0:
+//   C[k][t] = C[k-1][t] - h_kk C[k-1][t-1] - sum_{i=1}^{k-1} cf_k[i] C[i-1][t-1-(k-i)],
+// where C[k-1][t] lies on diagonal d - 1 (one shuffle) and every other entry on the lane's own
+// diagonal, so with k unrolled every index is a compile-time register.  Columns beyond n are
+// computed too but never read by the columns <= n.  The depth sum runs over all i: entries left of
+// column 0 are exact zeros.  Diagonal 32 (only C[32][0] = 1, never read) has no lane.
+// q_j = C[m][j] (j = 1..min(m, n)) goes to q[j] for the series.
+template <int MW>
+__device__ __forceinline__ void labudde_diag(const double *__restrict__ cft, const double *__restrict__ hk, double *q,
+                                             int m, int n, int lane)
 {
-    const int t = lane;
-    const int tmax = k < n ? k : n;
-    const int d = k - t;
-    cd v{0.0, 0.0};
-    if (t <= tmax) {
-        const cd a = t <= k - 1 ? T[(d - 1) * rs + (k - 1)] : cd{0.0, 0.0};
-        const cd b = t >= 1 ? T[d * rs + (k - 1)] : cd{0.0, 0.0};
-        v.re = a.re - fma(hkk.re, b.re, -hkk.im * b.im);
-        v.im = a.im - fma(hkk.re, b.im, hkk.im * b.re);
-    }
-    const int jmax = (k - 1) < (n - 1) ? (k - 1) : (n - 1);
-    const cd *cfk = cf + k;
-    const cd *Td = T + (d > 0 ? d : 0) * rs + (k - 2);
-    double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
+    double D[MW + 1];
+    D[0] = lane == 0 ? 1.0 : 0.0;
 #pragma unroll
-    for (int j = 1; j <= 31; ++j) {
-        if (j > jmax) break;
-        const cd c = cfk[-j];
-        const cd x = Td[1 - j];
-        if (j & 1) {
-            sr0 = fma(c.re, x.re, fma(-c.im, x.im, sr0));
-            si0 = fma(c.re, x.im, fma(c.im, x.re, si0));
-        } else {
-            sr1 = fma(c.re, x.re, fma(-c.im, x.im, sr1));
-            si1 = fma(c.re, x.im, fma(c.im, x.re, si1));
+    for (int r = 1; r <= MW; ++r) D[r] = 0.0;
+#pragma unroll
+    for (int k = 1; k <= MW; ++k) {
+        if (k > m) break;
+        double up = __shfl_up_sync(FULL, D[k - 1], 1);
+        if (lane == 0) up = 0.0;
+        const double *row = cft + cft_row_real(k);
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int i = 1; i < k; i += 2) {
+            const double2 c2 = *reinterpret_cast<const double2 *>(row + (i - 1));
+            s0 = fma(c2.x, D[i - 1], s0);
+            if (i + 1 < k) s1 = fma(c2.y, D[i], s1);
         }
+        D[k] = fma(-hk[k], D[k - 1], up) - (s0 + s1);
+        if (k == m && lane < m && lane >= m - n) q[m - lane] = D[k];
     }
-    if (t <= tmax) T[d * rs + k] = cd{v.re - (sr0 + sr1), v.im - (si0 + si1)};
 }
 
-__device__ __forceinline__ cd series_coeff_c(const cd *T, int m, int n, int rs, int lane)
+template <int MW>
+__device__ __forceinline__ void labudde_diag_c(const cd *__restrict__ cft, const cd *__restrict__ hk, cd *q, int m, int n,
+                                               int lane)
+{
+    double Dr[MW + 1], Di[MW + 1];
+    Dr[0] = lane == 0 ? 1.0 : 0.0;
+    Di[0] = 0.0;
+#pragma unroll
+    for (int r = 1; r <= MW; ++r) {
+        Dr[r] = 0.0;
+        Di[r] = 0.0;
+    }
+#pragma unroll
+    for (int k = 1; k <= MW; ++k) {
+        if (k > m) break;
+        double ur = __shfl_up_sync(FULL, Dr[k - 1], 1), ui = __shfl_up_sync(FULL, Di[k - 1], 1);
+        if (lane == 0) {
+            ur = 0.0;
+            ui = 0.0;
+        }
+        const cd h = hk[k];
+        const double vr = fma(-h.re, Dr[k - 1], fma(h.im, Di[k - 1], ur));
+        const double vi = fma(-h.re, Di[k - 1], fma(-h.im, Dr[k - 1], ui));
+        const cd *row = cft + cft_row_cplx(k);
+        double sr0 = 0.0, si0 = 0.0, sr1 = 0.0, si1 = 0.0;
+#pragma unroll
+        for (int i = 1; i < k; ++i) {
+            const cd c = row[i - 1];
+            if (i & 1) {
+                sr0 = fma(c.re, Dr[i - 1], fma(-c.im, Di[i - 1], sr0));
+                si0 = fma(c.re, Di[i - 1], fma(c.im, Dr[i - 1], si0));
+            } else {
+                sr1 = fma(c.re, Dr[i - 1], fma(-c.im, Di[i - 1], sr1));
+                si1 = fma(c.re, Di[i - 1], fma(c.im, Dr[i - 1], si1));
+            }
+        }
+        Dr[k] = vr - (sr0 + sr1);
+        Di[k] = vi - (si0 + si1);
+        if (k == m && lane < m && lane >= m - n) q[m - lane] = cd{Dr[k], Di[k]};
+    }
+}
+
+// [lambda^n] det(I - lambda H)^(-1/2) from q_1..q_min(m,n), as series_coeff.
+__device__ __forceinline__ double series_q(const double *q, int m, int n, int lane)
+{
+    double S = 0.0, fs = 1.0;
+    for (int s = 0; s < n; ++s) {
+        const int j = lane - s;
+        if (j >= 1 && j <= m && lane <= n) S = fma((double)(lane + s) * q[j], fs, S);
+        fs = __shfl_sync(FULL, S, s + 1) * c_neg_inv_2t[s + 1];
+    }
+    return fs;
+}
+
+__device__ __forceinline__ cd series_q_c(const cd *q, int m, int n, int lane)
 {
     double Sr = 0.0, Si = 0.0, fr = 1.0, fi = 0.0;
     for (int s = 0; s < n; ++s) {
         const int j = lane - s;
         if (j >= 1 && j <= m && lane <= n) {
             const double w = (double)(lane + s);
-            const cd q = T[(m - j) * rs + m];
-            const double ar = w * q.re, ai = w * q.im;
+            const cd qj = q[j];
+            const double ar = w * qj.re, ai = w * qj.im;
             Sr = fma(ar, fr, fma(-ai, fi, Sr));
             Si = fma(ar, fi, fma(ai, fr, Si));
         }
@@ -224,7 +307,7 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
         }
         pc[q] = R[q][0];
     }
-    if (lane == 0) C[0] = 1.0;  // La Budde row 0: C[0][0] = 1
+    if (RPL > 1 && lane == 0) C[0] = 1.0;  // La Budde row 0: C[0][0] = 1
     int hslot = 0;       // physical slot of label s-1 (label 0 never moves)
     double xprev = 0.0;  // subdiagonal entry h_{s,s-1} of the previous step
     for (int s = 1; s <= m - 2; ++s) {
@@ -244,7 +327,13 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
         const double x = __shfl_sync(FULL, pcp, plane);
         const int plab = __shfl_sync(FULL, labp, plane);
         // -- column s-1 is final for rows with label <= s-1 plus the pivot; feed La Budde step k = s
-        {
+        if constexpr (RPL == 1) {
+            // Stored for labudde_diag, which runs once the reduction is done.
+            if (lab[0] <= s - 3) bet[0] *= xprev;
+            else if (lab[0] == s - 2) bet[0] = xprev;
+            if (lab[0] <= s - 2) ws.cft[cft_row_real(s) + lab[0]] = pc[0] * bet[0];
+            if (lab[0] == s - 1) ws.hk[s] = pc[0];
+        } else {
             const double hcand = (RPL > 1 && (hslot >> 5) == 1) ? pc[RPL - 1] : pc[0];
             const double hkk = __shfl_sync(FULL, hcand, hslot & 31);
 #pragma unroll
@@ -355,17 +444,31 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
             if (k >= 2) {
                 if (lab[q] <= k - 3) bet[q] *= sub;
                 else if (lab[q] == k - 2) bet[q] = sub;
-                if (lab[q] <= k - 2) cf[lab[q] + 1] = colv * bet[q];
+                if (lab[q] <= k - 2) {
+                    if constexpr (RPL == 1) ws.cft[cft_row_real(k) + lab[q]] = colv * bet[q];
+                    else cf[lab[q] + 1] = colv * bet[q];
+                }
             }
             if (lab[q] == k - 1) hkk = colv;
         }
-        const int hs = last ? lastslot : hslot;
-        hkk = __shfl_sync(FULL, hkk, hs & 31);
-        __syncwarp();
-        labudde_row(C, cf, k, n, rs, hkk, lane);
-        __syncwarp();
+        if constexpr (RPL == 1) {
+            if (lab[0] == k - 1) ws.hk[k] = hkk;
+        } else {
+            const int hs = last ? lastslot : hslot;
+            hkk = __shfl_sync(FULL, hkk, hs & 31);
+            __syncwarp();
+            labudde_row(C, cf, k, n, rs, hkk, lane);
+            __syncwarp();
+        }
     }
-    return series_coeff(C, m, n, rs, lane);
+    if constexpr (RPL == 1) {
+        __syncwarp();
+        labudde_diag<MW>(ws.cft, ws.hk, ws.q, m, n, lane);
+        __syncwarp();
+        return series_q(ws.q, m, n, lane);
+    } else {
+        return series_coeff(C, m, n, rs, lane);
+    }
 }
 
 // ---- one complex term, m <= 32 --------------------------------------------------------------------
@@ -373,7 +476,6 @@ template <int MW>
 __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int E, int mE, int n, const FastWs &ws,
                                         int lane)
 {
-    constexpr int rs = MW + 1;  // La Budde table row stride
     const int m = 2 * mE;
     double Rr[MW], Ri[MW];
     int lab = lane;
@@ -397,22 +499,18 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
     }
     double pcr = Rr[0], pci = Ri[0];
     cd bet{0.0, 0.0};
-    cd *C = (cd *)ws.C;
-    cd *cfc = (cd *)ws.cf;  // 32 complex coefficients
+    cd *cft = (cd *)ws.cft, *hk = (cd *)ws.hk;
     double *prr = ws.prow, *pri = ws.prow + 32, *wvr = ws.wv, *wvi = ws.wv + 32;
-    if (lane == 0) C[0] = cd{1.0, 0.0};  // La Budde row 0: C[0][0] = 1
-    int hslot = 0;
     cd xprev{0.0, 0.0};
-    auto feed = [&](int k, double colr, double coli, cd sub, int hs) {
+    // Store La Budde's order-k coefficients for labudde_diag_c, which runs once the reduction is done.
+    auto feed = [&](int k, double colr, double coli, cd sub) {
         if (k >= 2) {
             if (lab <= k - 3) bet = cd{fma(bet.re, sub.re, -bet.im * sub.im), fma(bet.re, sub.im, bet.im * sub.re)};
             else if (lab == k - 2) bet = sub;
-            if (lab <= k - 2) cfc[lab + 1] = cd{fma(colr, bet.re, -coli * bet.im), fma(colr, bet.im, coli * bet.re)};
+            if (lab <= k - 2)
+                cft[cft_row_cplx(k) + lab] = cd{fma(colr, bet.re, -coli * bet.im), fma(colr, bet.im, coli * bet.re)};
         }
-        const cd hkk{__shfl_sync(FULL, colr, hs), __shfl_sync(FULL, coli, hs)};
-        __syncwarp();
-        labudde_row_c(C, cfc, k, n, rs, hkk, lane);
-        __syncwarp();
+        if (lab == k - 1) hk[k] = cd{colr, coli};
     };
     for (int s = 1; s <= m - 2; ++s) {
         unsigned key = 0;
@@ -421,10 +519,9 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
         const int plane = 63 - (int)(best & 63u);
         const double xr = __shfl_sync(FULL, pcr, plane), xi = __shfl_sync(FULL, pci, plane);
         const int plab = __shfl_sync(FULL, lab, plane);
-        feed(s, pcr, pci, xprev, hslot);
+        feed(s, pcr, pci, xprev);
         if (lab == s) lab = plab;
         else if (lab == plab) lab = s;
-        hslot = plane;
         xprev = cd{xr, xi};
         const double d = fma(xr, xr, xi * xi);
         if (d == 0.0) {
@@ -491,10 +588,13 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
     for (int k = (m >= 3 ? m - 1 : 1); k <= m; ++k) {
         cd sub = xprev;
         if (k == m && k >= 2) sub = cd{__shfl_sync(FULL, pcr, lastslot), __shfl_sync(FULL, pci, lastslot)};
-        if (k == m) feed(k, cr, ci, sub, lastslot);
-        else feed(k, pcr, pci, sub, hslot);
+        if (k == m) feed(k, cr, ci, sub);
+        else feed(k, pcr, pci, sub);
     }
-    return series_coeff_c(C, m, n, rs, lane);
+    __syncwarp();
+    labudde_diag_c<MW>(cft, hk, (cd *)ws.q, m, n, lane);
+    __syncwarp();
+    return series_q_c((const cd *)ws.q, m, n, lane);
 }
 
 // ---- kernels -----------------------------------------------------------------------------------
@@ -525,8 +625,10 @@ __global__ void __launch_bounds__((SizeClass<CPLX, MHI>::threads), (SizeClass<CP
     const int E = in.E, n = in.n;
     const FastWs w = fast_carve(smem + (size_t)wib * fast_ws_doubles(a.nmax, CPLX, MHI), a.nmax, CPLX, MHI);
     // The La Budde table's entries left of column 0 must read as zero; nothing ever writes them.
-    for (int i = lane; i < (CPLX ? 2 : 1) * (MHI + 1) * (MHI + 1); i += 32) w.C[i] = 0.0;
-    __syncwarp();
+    if constexpr (MHI > 32) {
+        for (int i = lane; i < (MHI + 1) * (MHI + 1); i += 32) w.C[i] = 0.0;
+        __syncwarp();
+    }
     const int wslot = blockIdx.x * warps_per_block + wib;
     const int64_t W = a.warps_per_inst;
     dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
