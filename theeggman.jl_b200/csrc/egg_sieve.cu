@@ -488,6 +488,13 @@ __global__ void sieve_reduce_kernel(PartialSet ps, const SieveInst *inst, void *
 
 // ---- host side ---------------------------------------------------------------------------------
 
+static int64_t maxrep_of(const int64_t *reps, int64_t E)
+{
+    int64_t m = 0;
+    for (int64_t i = 0; i < E; ++i) m = reps[i] > m ? reps[i] : m;
+    return m;
+}
+
 static int64_t term_count(const int64_t *reps, int64_t E, int glynn)
 {
     // The odometer's range: prod(r_i + 1), the leading digit clipped to (r_1 + 2) / 2 under Glynn
@@ -541,6 +548,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         }
         if (n > 63) return fail(EGG_ERR_TOO_LARGE, "the device sieve extracts coefficients up to lambda^63");
         s.n = (int)n;
+        s.subset = (!s.glynn && s.E > 0 && s.E <= 32 && n == s.E && maxrep_of(edge_reps + b * Emax, s.E) == 1) ? 1 : 0;
         nmax = s.n > nmax ? s.n : nmax;
         s.steps = term_count(edge_reps + b * Emax, s.E, s.glynn);
         if (s.steps < 0) return fail(EGG_ERR_TOO_LARGE, "the sieve's term count overflows Int64");
@@ -598,11 +606,25 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     if (ex_wpb > 8) ex_wpb = 8;
     if (run_ex && ex_wpb < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
     const int ex_bx = run_ex ? per_inst_blocks(ex_wpb) : 0;
-    const int fwpb = 8;
-    for (int k = 0; k < nclass; ++k)
-        if (run_cls[k] && fast_smem_bytes(nmax, cplx, k, fwpb) > 220 * 1024)
+    // Each fast class runs as one wave: its resident blocks across the machine, shared among the
+    // instances.  Every warp gets the same share of term runs, so a second, partial wave would leave
+    // most of the machine idle while it runs.
+    int f_cw[kFastClassesReal] = {0, 0, 0, 0, 0, 0}, f_bx[kFastClassesReal] = {0, 0, 0, 0, 0, 0};
+    int64_t f_warps = 0;  // sum over classes of warps per instance
+    for (int k = 0; k < nclass; ++k) {
+        if (!run_cls[k]) continue;
+        int bps = 0;
+        int rc0 = fast_class_shape(nmax, cplx, k, &f_cw[k], &bps);
+        if (rc0) return rc0;
+        if (bps < 1 || fast_smem_bytes(nmax, cplx, k, f_cw[k]) > 220 * 1024)
             return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
-    const int f_bx = ncls_run ? per_inst_blocks(fwpb) : 0;
+        int64_t per = ((int64_t)num_sms * bps + B - 1) / B;
+        const int64_t cap = (maxsteps + f_cw[k] - 1) / f_cw[k];  // no more warps than terms
+        if (per > cap) per = cap;
+        if (per < 1) per = 1;
+        f_bx[k] = (int)per;
+        f_warps += per * f_cw[k];
+    }
 
     // Device staging: instance table, reps, strides, binoms, partials -- one scratch allocation.
     int64_t off = 0;
@@ -611,7 +633,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     const int64_t off_str = off; off = align256(off + (int64_t)((strides.size() + 1) * sizeof(int64_t)));
     const int64_t off_bin = off; off = align256(off + (int64_t)(binoms.size() * sizeof(double)));
     const int64_t off_pex = off; off = align256(off + (run_ex ? B * ex_bx * ex_wpb * 2 * (int64_t)sizeof(dd) : 0));
-    const int64_t off_pf = off; off = align256(off + (int64_t)ncls_run * B * f_bx * fwpb * 2 * (int64_t)sizeof(dd));
+    const int64_t off_pf = off; off = align256(off + B * f_warps * 2 * (int64_t)sizeof(dd));
     char *base;
     int rc;
     if (fixed) {
@@ -647,16 +669,17 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         ps.w[k] = 0;
     }
     if (ncls_run) {
-        a.warps_per_inst = f_bx * fwpb;
         a.partial = nullptr;
         int slot = 1;
+        dd *part = (dd *)(base + off_pf);
         for (int k = 0; k < nclass; ++k) {
             if (!run_cls[k]) continue;
-            dd *part = (dd *)(base + off_pf) + (size_t)(slot - 1) * B * a.warps_per_inst * 2;
-            rc = launch_fast(a, (const int64_t *)(base + off_str), (int)B, cplx, k, part, fwpb, f_bx, st);
+            a.warps_per_inst = f_bx[k] * f_cw[k];
+            rc = launch_fast(a, (const int64_t *)(base + off_str), (int)B, cplx, k, part, f_bx[k], st);
             if (rc) return rc;
             ps.p[slot] = part;
             ps.w[slot] = a.warps_per_inst;
+            part += (size_t)B * a.warps_per_inst * 2;
             ++slot;
         }
     }

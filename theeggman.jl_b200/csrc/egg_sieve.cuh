@@ -10,6 +10,7 @@ struct SieveInst {
     int64_t steps;      // number of sieve terms
     int64_t reps_off;   // offset into the reps / strides arrays
     int E, n, glynn, lda;
+    int subset;         // all multiplicities 1 under inclusion-exclusion: term j is the edge subset j
 };
 
 struct SieveArgs {
@@ -29,7 +30,11 @@ struct SieveArgs {
 extern const int kFastClasses[][2];
 constexpr int kFastClassesReal = 6, kFastClassesCplx = 4;
 size_t fast_smem_bytes(int nmax, int cplx, int cls, int warps);
-int launch_fast(const SieveArgs &a, const int64_t *strides, int B, int cplx, int cls, dd *partial, int wpb,
-                int blocks_x, cudaStream_t st);
+// Launches class `cls` on a grid of blocks_x x B blocks; a.warps_per_inst must be blocks_x times
+// the class's warps per block.
+int launch_fast(const SieveArgs &a, const int64_t *strides, int B, int cplx, int cls, dd *partial, int blocks_x,
+                cudaStream_t st);
+// The class's block size in warps and how many of its blocks one SM holds.
+int fast_class_shape(int nmax, int cplx, int cls, int *warps_per_block, int *blocks_per_sm);
 
 }  // namespace egg
