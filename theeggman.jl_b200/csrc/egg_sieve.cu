@@ -320,7 +320,8 @@ __device__ void sieve_warp_exact(const SieveArgs &a, const SieveInst &in, WarpWs
     const int E = in.E, n = in.n, glynn = in.glynn, lda = in.lda;
     const int *reps = a.reps + in.reps_off;
     const int mr1 = a.maxrep + 1;
-    for (int64_t j = wslot; j < in.steps; j += a.warps_per_inst) {
+    // Term j: decode, build, reduce, accumulate.
+    auto term = [&](int64_t j) {
         // Mixed-radix decode, Glynn substitution, surviving edges (:542-580), on lane 0.
         int mE = 0;
         double prefac = 0.0;
@@ -361,9 +362,9 @@ __device__ void sieve_warp_exact(const SieveArgs &a, const SieveInst &in, WarpWs
                     a.terms[j] = 0.0;
                 }
             }
-            continue;
+            return;
         }
-        if (m <= a.skip_le) continue;   // evaluated by the fast kernels
+        if (m <= a.skip_le) return;   // evaluated by the fast kernels
         const int ld = w.ldm;
         // M = A_S X D (:582-593).
         if (!CPLX) {
@@ -414,6 +415,39 @@ __device__ void sieve_warp_exact(const SieveArgs &a, const SieveInst &in, WarpWs
             }
         }
         __syncwarp();
+    };
+    if (in.subset) {
+        // All multiplicities 1 under inclusion-exclusion: term j is the edge subset whose bit E-1-i
+        // is edge i.  Each warp takes an equal share of every popcount level it evaluates (colex
+        // unrank, then successors; bit i = edge i here, reversed into j), so that when only the
+        // largest terms are left to this kernel they are spread evenly over the warps.
+        const int k0 = a.skip_le > 0 ? a.skip_le / 2 + 1 : 0;
+        const uint64_t W = (uint64_t)a.warps_per_inst;
+        for (int k = k0; k <= E; ++k) {
+            const uint64_t cnt = a.binom32[E * 65 + k];
+            const uint64_t lo = (uint64_t)wslot * cnt / W, hi = ((uint64_t)wslot + 1) * cnt / W;
+            if (lo >= hi) continue;
+            uint32_t S = 0;
+            {
+                uint32_t R = (uint32_t)lo;
+                int x = E - 1;
+                for (int i = k; i >= 1; --i) {
+                    while (a.binom32[x * 65 + i] > R) --x;
+                    S |= 1u << x;
+                    R -= a.binom32[x * 65 + i];
+                    --x;
+                }
+            }
+            for (uint64_t rk = lo; rk < hi; ++rk) {
+                if (rk > lo) {
+                    const uint32_t t = S | (S - 1);
+                    S = (t + 1) | (((~t & (0u - ~t)) - 1) >> (__ffs((int)S)));
+                }
+                term((int64_t)(__brev(S) >> (32 - E)));
+            }
+        }
+    } else {
+        for (int64_t j = wslot; j < in.steps; j += a.warps_per_inst) term(j);
     }
 }
 
@@ -605,7 +639,22 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     int ex_wpb = (int)((200 * 1024) / ex_per_warp);
     if (ex_wpb > 8) ex_wpb = 8;
     if (run_ex && ex_wpb < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
-    const int ex_bx = run_ex ? per_inst_blocks(ex_wpb) : 0;
+    bool all_subset = true;
+    for (const SieveInst &s : inst) all_subset = all_subset && s.subset;
+    int ex_bx = 0;
+    if (run_ex && all_subset) {
+        // Terms dealt as equal shares of each popcount level: one wave of resident blocks.
+        int nb = 0;
+        if (cplx) EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(ex_wpb * ex_per_warp)));
+        else EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(ex_wpb * ex_per_warp)));
+        if (cplx) EGG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sieve_exact_kernel<true>, ex_wpb * 32, ex_wpb * ex_per_warp));
+        else EGG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sieve_exact_kernel<false>, ex_wpb * 32, ex_wpb * ex_per_warp));
+        int64_t per = ((int64_t)num_sms * (nb > 0 ? nb : 1) + B - 1) / B;
+        const int64_t cap = (maxsteps + ex_wpb - 1) / ex_wpb;
+        ex_bx = (int)(per < cap ? (per > 0 ? per : 1) : cap);
+    } else if (run_ex) {
+        ex_bx = per_inst_blocks(ex_wpb);
+    }
     // Each fast class runs as one wave: its resident blocks across the machine, shared among the
     // instances.  Every warp gets the same share of term runs, so a second, partial wave would leave
     // most of the machine idle while it runs.
@@ -657,6 +706,8 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.Ax = dAx;
     a.reps = (const int *)(base + off_reps);
     a.binoms = (const double *)(base + off_bin);
+    a.binom32 = binom32_device(st, &rc);
+    if (!a.binom32) return rc;
     a.inst = (const SieveInst *)(base + off_inst);
     a.maxrep = maxrep;
     a.Emax = Ews;
