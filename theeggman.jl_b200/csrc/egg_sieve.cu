@@ -472,8 +472,8 @@ __global__ void __launch_bounds__(256) sieve_exact_kernel(SieveArgs a, int warps
 // Sums each instance's per-warp partials (one array per kernel that evaluated some of its terms) in a fixed tree, applies the Glynn rescaling 2^-(n-1) (:737) and writes the result.
 // One block of 256 threads per instance.
 struct PartialSet {
-    const dd *p[7];  // exact kernel, then up to six register-tile size classes
-    int w[7];
+    const dd *p[kMaxPartials];  // exact kernel, then the register-tile launches (size classes or levels)
+    int w[kMaxPartials];
 };
 
 template <bool CPLX>
@@ -482,7 +482,7 @@ __global__ void sieve_reduce_kernel(PartialSet ps, const SieveInst *inst, void *
     __shared__ dd sre[256], sim[256];
     const int b = blockIdx.x, t = threadIdx.x;
     dd r{0.0, 0.0}, i{0.0, 0.0};
-    for (int a = 0; a < 7; ++a) {
+    for (int a = 0; a < kMaxPartials; ++a) {
         if (!ps.p[a]) continue;
         const dd *p = ps.p[a] + (size_t)b * ps.w[a] * 2;
         for (int w = t; w < ps.w[a]; w += 256) {
@@ -615,14 +615,14 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     // fall in; the exact kernel takes everything in exact mode, else whatever exceeds the tiles.
     // The register tiles handle orders n <= 31 (one lane per coefficient).
     const bool fast_ok = prec == EGG_PREC_FMA && nmax <= 31;
+    bool all_subset = true;
+    for (const SieveInst &si : inst) all_subset = all_subset && si.subset;
     const int fast_hi = cplx ? 32 : 48;
     const int nclass = cplx ? kFastClassesCplx : kFastClassesReal;
     bool run_cls[kFastClassesReal] = {false, false, false, false, false, false};
-    int ncls_run = 0;
     if (fast_ok)
         for (int k = 0; k < nclass; ++k) {
             run_cls[k] = mmax_all > kFastClasses[k][0] && mmin_all <= kFastClasses[k][1] && mmax_all > 0;
-            ncls_run += run_cls[k];
         }
     const bool run_ex = !fast_ok || mmax_all > fast_hi || mmax_all == 0;
     const int skip_le = fast_ok ? fast_hi : 0;
@@ -639,8 +639,6 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     int ex_wpb = (int)((200 * 1024) / ex_per_warp);
     if (ex_wpb > 8) ex_wpb = 8;
     if (run_ex && ex_wpb < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
-    bool all_subset = true;
-    for (const SieveInst &s : inst) all_subset = all_subset && s.subset;
     int ex_bx = 0;
     if (run_ex && all_subset) {
         // Terms dealt as equal shares of each popcount level: one wave of resident blocks.
@@ -655,25 +653,45 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     } else if (run_ex) {
         ex_bx = per_inst_blocks(ex_wpb);
     }
-    // Each fast class runs as one wave: its resident blocks across the machine, shared among the
-    // instances.  Every warp gets the same share of term runs, so a second, partial wave would leave
-    // most of the machine idle while it runs.
-    int f_cw[kFastClassesReal] = {0, 0, 0, 0, 0, 0}, f_bx[kFastClassesReal] = {0, 0, 0, 0, 0, 0};
-    int64_t f_warps = 0;  // sum over classes of warps per instance
-    for (int k = 0; k < nclass; ++k) {
-        if (!run_cls[k]) continue;
-        int bps = 0;
-        int rc0 = fast_class_shape(nmax, cplx, k, &f_cw[k], &bps);
-        if (rc0) return rc0;
-        if (bps < 1 || fast_smem_bytes(nmax, cplx, k, f_cw[k]) > 220 * 1024)
-            return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
+    // The fast launches, each one wave of its resident blocks across the machine, shared among the
+    // instances (every warp gets the same share of the launch's terms, so a second, partial wave
+    // would leave most of the machine idle while it ran).  When every instance is a distinct-row
+    // inclusion-exclusion sieve, one launch per popcount level with a tile of exactly its size;
+    // otherwise one per size class.
+    struct FastLaunch {
+        int level, cls, cw, bx;
+    };
+    std::vector<FastLaunch> fl;
+    int64_t f_warps = 0;  // sum over launches of warps per instance
+    auto add_launch = [&](int level, int cls, int cw, int bps, size_t smem) -> int {
+        if (bps < 1 || smem > 220 * 1024) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
         int64_t per = ((int64_t)num_sms * bps + B - 1) / B;
-        const int64_t cap = (maxsteps + f_cw[k] - 1) / f_cw[k];  // no more warps than terms
+        const int64_t cap = (maxsteps + cw - 1) / cw;  // no more warps than terms
         if (per > cap) per = cap;
         if (per < 1) per = 1;
-        f_bx[k] = (int)per;
-        f_warps += per * f_cw[k];
+        fl.push_back(FastLaunch{level, cls, cw, (int)per});
+        f_warps += per * cw;
+        return EGG_OK;
+    };
+    const bool use_levels = fast_ok && all_subset;
+    if (use_levels) {
+        const int kmax = (int)(Emax < fast_hi / 2 ? Emax : fast_hi / 2);
+        for (int k = 1; k <= kmax; ++k) {
+            int cw = 0, bps = 0;
+            int rc0 = cplx ? level_shape_cplx(nmax, k, &cw, &bps) : level_shape_real(nmax, k, &cw, &bps);
+            if (!rc0) rc0 = add_launch(k, -1, cw, bps, (size_t)cw * fast_ws_bytes(nmax, cplx, 2 * k));
+            if (rc0) return rc0;
+        }
+    } else {
+        for (int k = 0; k < nclass; ++k) {
+            if (!run_cls[k]) continue;
+            int cw = 0, bps = 0;
+            int rc0 = fast_class_shape(nmax, cplx, k, &cw, &bps);
+            if (!rc0) rc0 = add_launch(0, k, cw, bps, fast_smem_bytes(nmax, cplx, k, cw));
+            if (rc0) return rc0;
+        }
     }
+    if ((int)fl.size() + 1 > kMaxPartials) return fail(EGG_ERR_TOO_LARGE, "too many sieve launches");
 
     // Device staging: instance table, reps, strides, binoms, partials -- one scratch allocation.
     int64_t off = 0;
@@ -715,18 +733,21 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.skip_le = skip_le;
     a.terms = terms;
     PartialSet ps;
-    for (int k = 0; k < 7; ++k) {
+    for (int k = 0; k < kMaxPartials; ++k) {
         ps.p[k] = nullptr;
         ps.w[k] = 0;
     }
-    if (ncls_run) {
+    {
         a.partial = nullptr;
         int slot = 1;
         dd *part = (dd *)(base + off_pf);
-        for (int k = 0; k < nclass; ++k) {
-            if (!run_cls[k]) continue;
-            a.warps_per_inst = f_bx[k] * f_cw[k];
-            rc = launch_fast(a, (const int64_t *)(base + off_str), (int)B, cplx, k, part, f_bx[k], st);
+        for (const FastLaunch &L : fl) {
+            a.warps_per_inst = L.bx * L.cw;
+            if (L.level > 0)
+                rc = cplx ? level_launch_cplx(a, (int)B, L.level, part, L.bx, st)
+                          : level_launch_real(a, (int)B, L.level, part, L.bx, st);
+            else
+                rc = launch_fast(a, (const int64_t *)(base + off_str), (int)B, cplx, L.cls, part, L.bx, st);
             if (rc) return rc;
             ps.p[slot] = part;
             ps.w[slot] = a.warps_per_inst;

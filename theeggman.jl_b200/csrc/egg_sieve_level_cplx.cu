@@ -1,0 +1,39 @@
+// egg_sieve_level_cplx.cu -- popcount-level sieve kernels for ComplexF64 terms, m = 2 .. 32.
+#include "egg_sieve_level.cuh"
+
+namespace egg {
+
+#define EGG_LVL_LAUNCH(CPLX, K) \
+    case K: return level_launch_k<CPLX, K>(a, B, partial, blocks_x, st);
+#define EGG_LVL_SHAPE(CPLX, K) \
+    case K: rc = level_shape_k<CPLX, K>(nmax, warps_per_block, blocks_per_sm); break;
+
+int level_launch_cplx(const SieveArgs &a, int B, int k, dd *partial, int blocks_x, cudaStream_t st)
+{
+    int rc = upload_fast_tables_once(st);
+    if (rc) return rc;
+    switch (k) {
+        EGG_LEVEL_CASES(true, EGG_LVL_LAUNCH)
+    }
+    return fail(EGG_ERR_ARGUMENT, "no such sieve level");
+}
+
+int level_shape_cplx(int nmax, int k, int *warps_per_block, int *blocks_per_sm)
+{
+    static int cache[kLevelMaxCplx + 1][2];
+    if (k >= 1 && k <= kLevelMaxCplx && cache[k][1] > 0) {
+        *warps_per_block = cache[k][0];
+        *blocks_per_sm = cache[k][1];
+        return EGG_OK;
+    }
+    int rc = fail(EGG_ERR_ARGUMENT, "no such sieve level");
+    switch (k) {
+        EGG_LEVEL_CASES(true, EGG_LVL_SHAPE)
+    }
+    if (rc) return rc;
+    cache[k][0] = *warps_per_block;
+    cache[k][1] = *blocks_per_sm;
+    return EGG_OK;
+}
+
+}  // namespace egg
