@@ -36,9 +36,19 @@ int ensure_init()
     if (e != cudaSuccess || n == 0)
         return fail(EGG_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
     EGG_CUDA_TRY(cudaSetDevice(0));
-    EGG_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-    EGG_CUDA_TRY(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, 0));
+    int rc = create_streams(c, 0);
+    if (rc) return rc;
     c.device = 0;
+    return EGG_OK;
+}
+
+int create_streams(Context &c, int device)
+{
+    EGG_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    EGG_CUDA_TRY(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+    EGG_CUDA_TRY(cudaEventCreateWithFlags(&c.fork_ev, cudaEventDisableTiming));
+    EGG_CUDA_TRY(cudaEventCreateWithFlags(&c.join_ev, cudaEventDisableTiming));
+    EGG_CUDA_TRY(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
     return EGG_OK;
 }
 
@@ -160,8 +170,8 @@ int egg_init(int device)
     if (e != cudaSuccess || n == 0) return fail(EGG_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
     if (device < 0 || device >= n) return fail(EGG_ERR_ARGUMENT, "device index out of range");
     EGG_CUDA_TRY(cudaSetDevice(device));
-    EGG_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-    EGG_CUDA_TRY(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
+    int rc = create_streams(c, device);
+    if (rc) return rc;
     c.device = device;
     return EGG_OK;
 }

@@ -130,6 +130,10 @@ struct DevBuf {
 struct Context {
     int device = -1;
     cudaStream_t stream = nullptr;
+    // A second stream for launches that leave most of the machine idle (they overlap the main
+    // stream's), with the events that fork it from and join it back to the calling stream.
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     int num_sms = 0;
     std::map<std::pair<int, int>, DevPlan> plans;
     DevBuf scratch[9];   // H, P, out, sieve matrix, sieve out, misc, mixed-degree batch + its staging:
@@ -139,6 +143,7 @@ struct Context {
 
 Context &ctx();
 int ensure_init();
+int create_streams(Context &c, int device);
 
 // Kernel launches the library has made since it was loaded (reported by egg_launch_count).
 extern std::atomic<long long> g_launches;

@@ -471,32 +471,34 @@ __global__ void __launch_bounds__(256) sieve_exact_kernel(SieveArgs a, int warps
 
 // Sums each instance's per-warp partials (one array per kernel that evaluated some of its terms) in a fixed tree, applies the Glynn rescaling 2^-(n-1) (:737) and writes the result.
 // One block of 256 threads per instance.
+constexpr int kReduceThreads = 512;
+
 struct PartialSet {
     const dd *p[kMaxPartials];  // exact kernel, then the register-tile launches (size classes or levels)
     int w[kMaxPartials];
 };
 
 template <bool CPLX>
-__global__ void sieve_reduce_kernel(PartialSet ps, const SieveInst *inst, void *out)
+__global__ void __launch_bounds__(kReduceThreads) sieve_reduce_kernel(PartialSet ps, const SieveInst *inst, void *out)
 {
-    __shared__ dd sre[256], sim[256];
+    __shared__ dd sre[kReduceThreads], sim[CPLX ? kReduceThreads : 1];
     const int b = blockIdx.x, t = threadIdx.x;
     dd r{0.0, 0.0}, i{0.0, 0.0};
     for (int a = 0; a < kMaxPartials; ++a) {
         if (!ps.p[a]) continue;
         const dd *p = ps.p[a] + (size_t)b * ps.w[a] * 2;
-        for (int w = t; w < ps.w[a]; w += 256) {
+        for (int w = t; w < ps.w[a]; w += kReduceThreads) {
             dd_add(r, p[2 * w]);
-            dd_add(i, p[2 * w + 1]);
+            if (CPLX) dd_add(i, p[2 * w + 1]);
         }
     }
     sre[t] = r;
-    sim[t] = i;
+    if (CPLX) sim[t] = i;
     __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
+    for (int s = kReduceThreads / 2; s > 0; s >>= 1) {
         if (t < s) {
             dd_add(sre[t], sre[t + s]);
-            dd_add(sim[t], sim[t + s]);
+            if (CPLX) dd_add(sim[t], sim[t + s]);
         }
         __syncthreads();
     }
@@ -508,7 +510,7 @@ __global__ void sieve_reduce_kernel(PartialSet ps, const SieveInst *inst, void *
             hi = 0.0;
         } else {
             hr = __dadd_rn(sre[0].hi, sre[0].lo);
-            hi = __dadd_rn(sim[0].hi, sim[0].lo);
+            hi = CPLX ? __dadd_rn(sim[0].hi, sim[0].lo) : 0.0;
             if (in.glynn) {
                 const double s = ldexp(1.0, -(in.n - 1));
                 hr = __dmul_rn(hr, s);
@@ -521,6 +523,13 @@ __global__ void sieve_reduce_kernel(PartialSet ps, const SieveInst *inst, void *
 }
 
 // ---- host side ---------------------------------------------------------------------------------
+
+static uint64_t binom_u64(int64_t n, int64_t k)
+{
+    uint64_t r = 1;
+    for (int64_t i = 1; i <= k; ++i) r = r * (uint64_t)(n - k + i) / (uint64_t)i;  // exact at each step
+    return r;
+}
 
 static int64_t maxrep_of(const int64_t *reps, int64_t E)
 {
@@ -658,28 +667,35 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     // would leave most of the machine idle while it ran).  When every instance is a distinct-row
     // inclusion-exclusion sieve, one launch per popcount level with a tile of exactly its size;
     // otherwise one per size class.
+    // A level whose terms number at most two per resident warp is latency-bound: it runs on the
+    // side stream, overlapping the main stream's launches, as does the exact kernel when it only
+    // takes the terms too large for the tiles.
     struct FastLaunch {
-        int level, cls, cw, bx;
+        int level, cls, cw, bx, parts;
+        bool side;
     };
     std::vector<FastLaunch> fl;
-    int64_t f_warps = 0;  // sum over launches of warps per instance
-    auto add_launch = [&](int level, int cls, int cw, int bps, size_t smem) -> int {
+    int64_t f_parts = 0;  // sum over launches of partials per instance
+    auto add_launch = [&](int level, int cls, int cw, int bps, size_t smem, int64_t terms) -> int {
         if (bps < 1 || smem > 220 * 1024) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
         int64_t per = ((int64_t)num_sms * bps + B - 1) / B;
         const int64_t cap = (maxsteps + cw - 1) / cw;  // no more warps than terms
         if (per > cap) per = cap;
         if (per < 1) per = 1;
-        fl.push_back(FastLaunch{level, cls, cw, (int)per});
-        f_warps += per * cw;
+        const int parts = (int)(level > 0 ? per : per * cw);  // a level kernel writes one partial per block
+        fl.push_back(FastLaunch{level, cls, cw, (int)per, parts, terms >= 0 && terms <= 2 * per * cw * B});
+        f_parts += parts;
         return EGG_OK;
     };
     const bool use_levels = fast_ok && all_subset;
     if (use_levels) {
         const int kmax = (int)(Emax < fast_hi / 2 ? Emax : fast_hi / 2);
         for (int k = 1; k <= kmax; ++k) {
+            int64_t terms = 0;
+            for (const SieveInst &si : inst) terms += si.E >= k ? (int64_t)binom_u64(si.E, k) : 0;
             int cw = 0, bps = 0;
             int rc0 = cplx ? level_shape_cplx(nmax, k, &cw, &bps) : level_shape_real(nmax, k, &cw, &bps);
-            if (!rc0) rc0 = add_launch(k, -1, cw, bps, (size_t)cw * fast_ws_bytes(nmax, cplx, 2 * k));
+            if (!rc0) rc0 = add_launch(k, -1, cw, bps, (size_t)cw * fast_ws_bytes(nmax, cplx, 2 * k), terms);
             if (rc0) return rc0;
         }
     } else {
@@ -687,7 +703,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             if (!run_cls[k]) continue;
             int cw = 0, bps = 0;
             int rc0 = fast_class_shape(nmax, cplx, k, &cw, &bps);
-            if (!rc0) rc0 = add_launch(0, k, cw, bps, fast_smem_bytes(nmax, cplx, k, cw));
+            if (!rc0) rc0 = add_launch(0, k, cw, bps, fast_smem_bytes(nmax, cplx, k, cw), -1);
             if (rc0) return rc0;
         }
     }
@@ -700,7 +716,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     const int64_t off_str = off; off = align256(off + (int64_t)((strides.size() + 1) * sizeof(int64_t)));
     const int64_t off_bin = off; off = align256(off + (int64_t)(binoms.size() * sizeof(double)));
     const int64_t off_pex = off; off = align256(off + (run_ex ? B * ex_bx * ex_wpb * 2 * (int64_t)sizeof(dd) : 0));
-    const int64_t off_pf = off; off = align256(off + B * f_warps * 2 * (int64_t)sizeof(dd));
+    const int64_t off_pf = off; off = align256(off + B * f_parts * 2 * (int64_t)sizeof(dd));
     char *base;
     int rc;
     if (fixed) {
@@ -737,46 +753,62 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         ps.p[k] = nullptr;
         ps.w[k] = 0;
     }
+    const bool ex_side = run_ex && fast_ok;  // the exact kernel only takes the terms too large for the tiles
+    bool any_side = ex_side;
+    for (const FastLaunch &L : fl) any_side = any_side || L.side;
+    if (any_side) {
+        EGG_CUDA_TRY(cudaEventRecord(c.fork_ev, st));
+        EGG_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork_ev, 0));
+    }
+    if (run_ex) {
+        // First, so that on the side stream its long terms start at once.
+        SieveArgs ae = a;
+        ae.warps_per_inst = ex_bx * ex_wpb;
+        ae.partial = (dd *)(base + off_pex);
+        const size_t smem = (size_t)ex_wpb * ex_per_warp;
+        const dim3 grid((unsigned)ex_bx, (unsigned)B);
+        cudaStream_t es = ex_side ? c.side : st;
+        if (cplx) {
+            EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            sieve_exact_kernel<true><<<grid, ex_wpb * 32, smem, es>>>(ae, ex_wpb);
+        } else {
+            EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            sieve_exact_kernel<false><<<grid, ex_wpb * 32, smem, es>>>(ae, ex_wpb);
+        }
+        count_launch();
+        EGG_CUDA_TRY(cudaGetLastError());
+        ps.p[0] = ae.partial;
+        ps.w[0] = ae.warps_per_inst;
+    }
     {
         a.partial = nullptr;
         int slot = 1;
         dd *part = (dd *)(base + off_pf);
         for (const FastLaunch &L : fl) {
             a.warps_per_inst = L.bx * L.cw;
+            cudaStream_t ls = L.side ? c.side : st;
             if (L.level > 0)
-                rc = cplx ? level_launch_cplx(a, (int)B, L.level, part, L.bx, st)
-                          : level_launch_real(a, (int)B, L.level, part, L.bx, st);
+                rc = cplx ? level_launch_cplx(a, (int)B, L.level, part, L.bx, ls)
+                          : level_launch_real(a, (int)B, L.level, part, L.bx, ls);
             else
-                rc = launch_fast(a, (const int64_t *)(base + off_str), (int)B, cplx, L.cls, part, L.bx, st);
+                rc = launch_fast(a, (const int64_t *)(base + off_str), (int)B, cplx, L.cls, part, L.bx, ls);
             if (rc) return rc;
             ps.p[slot] = part;
-            ps.w[slot] = a.warps_per_inst;
-            part += (size_t)B * a.warps_per_inst * 2;
+            ps.w[slot] = L.parts;
+            part += (size_t)B * L.parts * 2;
             ++slot;
         }
     }
-    if (run_ex) {
-        a.warps_per_inst = ex_bx * ex_wpb;
-        a.partial = (dd *)(base + off_pex);
-        size_t smem = (size_t)ex_wpb * ex_per_warp;
-        dim3 grid((unsigned)ex_bx, (unsigned)B);
-        if (cplx) {
-            EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sieve_exact_kernel<true><<<grid, ex_wpb * 32, smem, st>>>(a, ex_wpb);
-        } else {
-            EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sieve_exact_kernel<false><<<grid, ex_wpb * 32, smem, st>>>(a, ex_wpb);
-        }
-        count_launch();
-        ps.p[0] = a.partial;
-        ps.w[0] = a.warps_per_inst;
+    if (any_side) {
+        EGG_CUDA_TRY(cudaEventRecord(c.join_ev, c.side));
+        EGG_CUDA_TRY(cudaStreamWaitEvent(st, c.join_ev, 0));
     }
     if (terms) {
         EGG_CUDA_TRY(cudaGetLastError());
         return EGG_OK;
     }
-    if (cplx) sieve_reduce_kernel<true><<<(unsigned)B, 256, 0, st>>>(ps, a.inst, dout);
-    else sieve_reduce_kernel<false><<<(unsigned)B, 256, 0, st>>>(ps, a.inst, dout);
+    if (cplx) sieve_reduce_kernel<true><<<(unsigned)B, kReduceThreads, 0, st>>>(ps, a.inst, dout);
+    else sieve_reduce_kernel<false><<<(unsigned)B, kReduceThreads, 0, st>>>(ps, a.inst, dout);
     count_launch();
     EGG_CUDA_TRY(cudaGetLastError());
     return EGG_OK;

@@ -5,7 +5,8 @@
 // its size is m = 2k for a k-subset.  One kernel per popcount level k evaluates exactly the
 // k-subsets, on a register tile of exactly m columns: no slot, step or La Budde order is spent on
 // sizes the level does not have.  Every warp takes an equal share of the level (one colex unrank,
-// then Gosper successors), so the level runs as one balanced wave.
+// then Gosper successors), so the level runs as one balanced wave.  Each block writes one partial
+// (re, im) per instance: its warps' double-double sums added in a fixed order.
 #pragma once
 #include "egg_sieve_fast.cuh"
 
@@ -69,10 +70,23 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K>::threads, LevelShape<CPLX,
             __syncwarp();
         }
     }
+    // The block's warps summed in a fixed order: one partial per block.
+    __shared__ dd red[2 * cw];
     if (lane == 0) {
-        dd *out = partial + ((size_t)b * W + wslot) * 2;
-        out[0] = acc_re;
-        out[1] = acc_im;
+        red[2 * wib] = acc_re;
+        red[2 * wib + 1] = acc_im;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        dd r = red[0], i = red[1];
+#pragma unroll
+        for (int q = 1; q < cw; ++q) {
+            dd_add(r, red[2 * q]);
+            dd_add(i, red[2 * q + 1]);
+        }
+        dd *out = partial + ((size_t)b * gridDim.x + blockIdx.x) * 2;
+        out[0] = r;
+        out[1] = i;
     }
 }
 
