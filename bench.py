@@ -58,8 +58,7 @@ def measured_peaks() -> dict:
 
 
 # The committed ncu summary (kernel and workload) whose DRAM traffic figure belongs to a workload.
-PROFILE_OF = {"sieve40": "sieve_fast_kernel_sieve40.md", "dp40": "dpc_fixed_kernel_dp40.md",
-              "dp32": "dpc_fixed_kernel_dp32.md"}
+PROFILE_OF = {"sieve40": "sieve_level_kernel_sieve40.md", "dp40": "dpc_fixed_kernel_dp40.md"}
 
 
 def profile_traffic(name: str):
