@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(256) sieve_exact_kernel(SieveArgs a, int warps
 constexpr int kReduceThreads = 512;
 
 struct PartialSet {
-    const dd *p[kMaxPartials];  // exact kernel, then the register-tile launches (size classes or levels)
+    const dd *p[kMaxPartials];  // exact kernel, then the register-tile level launches
     int w[kMaxPartials];
 };
 
@@ -570,7 +570,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     std::vector<int64_t> strides;
     int maxrep = 0, nmax = 0;
     int64_t maxsteps = 0;
-    int mmin_all = 1 << 30, mmax_all = 0;  // range of term sizes any instance can produce
+    int mmax_all = 0;  // the largest term size any instance can produce
     const int lda = (int)(2 * Emax);
     for (int64_t b = 0; b < B; ++b) {
         SieveInst &s = inst[(size_t)b];
@@ -580,14 +580,12 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         s.ax_off = b * (int64_t)lda * lda;
         s.reps_off = (int64_t)reps.size();
         int64_t n = 0;
-        int fixed = 0;  // edges that never vanish (Glynn with odd multiplicity)
         for (int64_t i = 0; i < s.E; ++i) {
             int64_t r = edge_reps[b * Emax + i];
             if (r < 0 || r > 1000000) return fail(EGG_ERR_ARGUMENT, "edge multiplicities must be non-negative");
             reps.push_back((int)r);
             n += r;
             if (r > maxrep) maxrep = (int)r;
-            if (s.glynn && (r % 2 == 1)) ++fixed;
         }
         if (n > 63) return fail(EGG_ERR_TOO_LARGE, "the device sieve extracts coefficients up to lambda^63");
         s.n = (int)n;
@@ -606,7 +604,6 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         }
         strides.insert(strides.end(), pv.begin(), pv.end());
         if (s.steps > 0) {
-            mmin_all = 2 * fixed < mmin_all ? 2 * fixed : mmin_all;
             mmax_all = 2 * s.E > mmax_all ? 2 * s.E : mmax_all;
         }
     }
@@ -620,19 +617,13 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     }
     const int Ews = (int)(Emax > 0 ? Emax : 1);
 
-    // Which kernels run: in FMA mode, each register-tile size class that some instance's terms can
-    // fall in; the exact kernel takes everything in exact mode, else whatever exceeds the tiles.
-    // The register tiles handle orders n <= 31 (one lane per coefficient).
+    // Which kernels run: in FMA mode, each popcount level that some instance has terms in, on the
+    // register tiles (orders n <= 31, one lane per coefficient); the exact kernel takes everything
+    // in exact mode, else whatever exceeds the tiles.
     const bool fast_ok = prec == EGG_PREC_FMA && nmax <= 31;
     bool all_subset = true;
     for (const SieveInst &si : inst) all_subset = all_subset && si.subset;
     const int fast_hi = cplx ? 32 : 48;
-    const int nclass = cplx ? kFastClassesCplx : kFastClassesReal;
-    bool run_cls[kFastClassesReal] = {false, false, false, false, false, false};
-    if (fast_ok)
-        for (int k = 0; k < nclass; ++k) {
-            run_cls[k] = mmax_all > kFastClasses[k][0] && mmin_all <= kFastClasses[k][1] && mmax_all > 0;
-        }
     const bool run_ex = !fast_ok || mmax_all > fast_hi || mmax_all == 0;
     const int skip_le = fast_ok ? fast_hi : 0;
 
@@ -662,49 +653,53 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     } else if (run_ex) {
         ex_bx = per_inst_blocks(ex_wpb);
     }
-    // The fast launches, each one wave of its resident blocks across the machine, shared among the
-    // instances (every warp gets the same share of the launch's terms, so a second, partial wave
-    // would leave most of the machine idle while it ran).  When every instance is a distinct-row
-    // inclusion-exclusion sieve, one launch per popcount level with a tile of exactly its size;
-    // otherwise one per size class.
-    // A level whose terms number at most two per resident warp is latency-bound: it runs on the
-    // side stream, overlapping the main stream's launches, as does the exact kernel when it only
-    // takes the terms too large for the tiles.
+    // The fast launches: one per popcount level with terms, each one wave of its resident blocks
+    // across the machine, shared among the instances (every warp gets the same share of the level's
+    // terms, so a second, partial wave would leave most of the machine idle while it ran).  A level
+    // whose terms number at most two per resident warp is latency-bound: it runs on the side
+    // stream, overlapping the main stream's launches, as does the exact kernel when it only takes
+    // the terms too large for the tiles.
     struct FastLaunch {
-        int level, cls, cw, bx, parts;
+        int level, cw, bx;
         bool side;
     };
     std::vector<FastLaunch> fl;
-    int64_t f_parts = 0;  // sum over launches of partials per instance
-    auto add_launch = [&](int level, int cls, int cw, int bps, size_t smem, int64_t terms) -> int {
-        if (bps < 1 || smem > 220 * 1024) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
-        int64_t per = ((int64_t)num_sms * bps + B - 1) / B;
-        const int64_t cap = (maxsteps + cw - 1) / cw;  // no more warps than terms
-        if (per > cap) per = cap;
-        if (per < 1) per = 1;
-        const int parts = (int)(level > 0 ? per : per * cw);  // a level kernel writes one partial per block
-        fl.push_back(FastLaunch{level, cls, cw, (int)per, parts, terms >= 0 && terms <= 2 * per * cw * B});
-        f_parts += parts;
-        return EGG_OK;
-    };
-    const bool use_levels = fast_ok && all_subset;
-    if (use_levels) {
+    int64_t f_parts = 0;  // sum over launches of partials (one per block) per instance
+    if (fast_ok) {
+        // Terms per level over all instances: the `counts` recursion of the cost model
+        // (src/hafnian.jl:855-884), per instance.
         const int kmax = (int)(Emax < fast_hi / 2 ? Emax : fast_hi / 2);
+        std::vector<double> lvl((size_t)kmax + 1, 0.0);
+        for (int64_t b = 0; b < B; ++b) {
+            const SieveInst &si = inst[(size_t)b];
+            std::vector<double> cnt((size_t)si.E + 1, 0.0);
+            cnt[0] = 1.0;
+            for (int i = 0; i < si.E; ++i) {
+                const int64_t r = edge_reps[b * Emax + i];
+                const double total = (double)(si.glynn ? (i == 0 ? (r + 2) / 2 : r + 1) : r + 1);
+                const double nzero = si.glynn ? (r % 2 == 0 ? 1.0 : 0.0) : 1.0;
+                for (int c = i + 1; c >= 1; --c) cnt[(size_t)c] = cnt[(size_t)c] * nzero + cnt[(size_t)c - 1] * (total - nzero);
+                cnt[0] *= nzero;
+            }
+            for (int k = 1; k <= kmax && k <= si.E; ++k) lvl[(size_t)k] += cnt[(size_t)k];
+        }
         for (int k = 1; k <= kmax; ++k) {
-            int64_t terms = 0;
-            for (const SieveInst &si : inst) terms += si.E >= k ? (int64_t)binom_u64(si.E, k) : 0;
+            if (lvl[(size_t)k] <= 0.0) continue;
             int cw = 0, bps = 0;
             int rc0 = cplx ? level_shape_cplx(nmax, k, &cw, &bps) : level_shape_real(nmax, k, &cw, &bps);
-            if (!rc0) rc0 = add_launch(k, -1, cw, bps, (size_t)cw * fast_ws_bytes(nmax, cplx, 2 * k), terms);
             if (rc0) return rc0;
-        }
-    } else {
-        for (int k = 0; k < nclass; ++k) {
-            if (!run_cls[k]) continue;
-            int cw = 0, bps = 0;
-            int rc0 = fast_class_shape(nmax, cplx, k, &cw, &bps);
-            if (!rc0) rc0 = add_launch(0, k, cw, bps, fast_smem_bytes(nmax, cplx, k, cw), -1);
-            if (rc0) return rc0;
+            if (bps < 1 || (size_t)cw * fast_ws_bytes(nmax, cplx, 2 * k) > 220 * 1024)
+                return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
+            // Distinct-row levels deal equal shares: one wave.  Odometer runs are only balanced on
+            // average and instances differ in size, so those levels get about four waves of blocks
+            // for the block scheduler to even out.
+            const int64_t waves = all_subset ? 1 : 4;
+            int64_t per = ((int64_t)num_sms * bps * waves + B - 1) / B;
+            const int64_t cap = (maxsteps + cw - 1) / cw;  // no more warps than terms
+            if (per > cap) per = cap;
+            if (per < 1) per = 1;
+            fl.push_back(FastLaunch{k, cw, (int)per, lvl[(size_t)k] <= 2.0 * (double)(num_sms * bps * cw)});
+            f_parts += per;
         }
     }
     if ((int)fl.size() + 1 > kMaxPartials) return fail(EGG_ERR_TOO_LARGE, "too many sieve launches");
@@ -784,18 +779,16 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         a.partial = nullptr;
         int slot = 1;
         dd *part = (dd *)(base + off_pf);
+        const int64_t *dstr = (const int64_t *)(base + off_str);
         for (const FastLaunch &L : fl) {
             a.warps_per_inst = L.bx * L.cw;
             cudaStream_t ls = L.side ? c.side : st;
-            if (L.level > 0)
-                rc = cplx ? level_launch_cplx(a, (int)B, L.level, part, L.bx, ls)
-                          : level_launch_real(a, (int)B, L.level, part, L.bx, ls);
-            else
-                rc = launch_fast(a, (const int64_t *)(base + off_str), (int)B, cplx, L.cls, part, L.bx, ls);
+            rc = cplx ? level_launch_cplx(a, dstr, (int)B, L.level, part, L.bx, ls)
+                      : level_launch_real(a, dstr, (int)B, L.level, part, L.bx, ls);
             if (rc) return rc;
             ps.p[slot] = part;
-            ps.w[slot] = L.parts;
-            part += (size_t)B * L.parts * 2;
+            ps.w[slot] = L.bx;
+            part += (size_t)B * L.bx * 2;
             ++slot;
         }
     }

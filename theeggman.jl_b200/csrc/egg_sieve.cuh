@@ -25,27 +25,17 @@ struct SieveArgs {
     int skip_le;           // the exact kernel leaves terms with m <= skip_le to the fast kernels
 };
 
-// Fast path (egg_sieve_fast.cu): size class `cls` covers terms with kFastClasses[cls][0] < m <=
-// kFastClasses[cls][1]; classes 0-3 exist for real and complex terms, 4-5 (two rows per lane) for
-// real terms only.
-extern const int kFastClasses[][2];
-constexpr int kFastClassesReal = 6, kFastClassesCplx = 4;
-size_t fast_smem_bytes(int nmax, int cplx, int cls, int warps);
-size_t fast_ws_bytes(int nmax, int cplx, int mhi);  // one warp's scratch for a tile of mhi columns
-constexpr int kMaxPartials = 26;                    // the exact kernel and up to 25 fast launches
-// Launches class `cls` on a grid of blocks_x x B blocks; a.warps_per_inst must be blocks_x times
-// the class's warps per block.
-int launch_fast(const SieveArgs &a, const int64_t *strides, int B, int cplx, int cls, dd *partial, int blocks_x,
-                cudaStream_t st);
-// The class's block size in warps and how many of its blocks one SM holds.
-int fast_class_shape(int nmax, int cplx, int cls, int *warps_per_block, int *blocks_per_sm);
-
-// Popcount levels (egg_sieve_level*.cu): level k evaluates the k-subset terms of distinct-row
-// inclusion-exclusion instances, m = 2k <= 48 (real) or 32 (complex).
+// Register-tile path (egg_sieve_fast.cuh, egg_sieve_level*.cu): level k evaluates the terms with
+// k surviving edges, m = 2k <= 48 (real) or 32 (complex), for any multiplicities.
 constexpr int kLevelMaxReal = 24, kLevelMaxCplx = 16;
-int level_launch_real(const SieveArgs &a, int B, int k, dd *partial, int blocks_x, cudaStream_t st);
-int level_launch_real_hi(const SieveArgs &a, int B, int k, dd *partial, int blocks_x, cudaStream_t st);
-int level_launch_cplx(const SieveArgs &a, int B, int k, dd *partial, int blocks_x, cudaStream_t st);
+constexpr int kMaxPartials = 26;  // the exact kernel and up to 25 level launches
+size_t fast_ws_bytes(int nmax, int cplx, int mhi);  // one warp's scratch for a tile of mhi columns
+// Launches level k on a grid of blocks_x x B blocks; a.warps_per_inst must be blocks_x times the
+// level's warps per block.  Each block writes one partial (re, im) per instance.
+int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, dd *partial, int blocks_x, cudaStream_t st);
+int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int k, dd *partial, int blocks_x, cudaStream_t st);
+int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, dd *partial, int blocks_x, cudaStream_t st);
+// The level's block size in warps and how many of its blocks one SM holds.
 int level_shape_real(int nmax, int k, int *warps_per_block, int *blocks_per_sm);
 int level_shape_real_hi(int nmax, int k, int *warps_per_block, int *blocks_per_sm);
 int level_shape_cplx(int nmax, int k, int *warps_per_block, int *blocks_per_sm);

@@ -1,12 +1,19 @@
 // egg_sieve_level.cuh -- the popcount-level kernels of the register-resident sieve.
 //
-// With every multiplicity 1 under inclusion-exclusion (distinct rows: hafnian(A; method=:sieve)'s
-// default variant, src/hafnian.jl:1139-1146), term j is the subset of edges whose digit is 1 and
-// its size is m = 2k for a k-subset.  One kernel per popcount level k evaluates exactly the
-// k-subsets, on a register tile of exactly m columns: no slot, step or La Budde order is spent on
-// sizes the level does not have.  Every warp takes an equal share of the level (one colex unrank,
-// then Gosper successors), so the level runs as one balanced wave.  Each block writes one partial
-// (re, im) per instance: its warps' double-double sums added in a fixed order.
+// A term's size is m = 2k for its k surviving edges (multiplicity nonzero after the Glynn
+// substitution).  One kernel per level k evaluates exactly the terms with k surviving edges, on a
+// register tile of exactly m columns: no slot, step or La Budde order is spent on sizes the level
+// does not have, and each level's block count follows its own register need.
+//
+//   * Distinct rows under inclusion-exclusion (every multiplicity 1: hafnian(A; method=:sieve)'s
+//     variant for distinct rows, src/hafnian.jl:1139-1146): term j is the subset of edges whose
+//     digit is 1, so the level's terms are the k-subsets.  Every warp takes an equal share of them
+//     (one colex unrank, then Gosper successors), and the level runs as one balanced wave.
+//   * Any other multiplicities (hafnian_repeated, Glynn): each warp walks runs of 16 consecutive
+//     odometer indices, dealt round robin, and evaluates the terms of its level among them.
+//
+// Each block writes one partial (re, im) per instance: its warps' double-double sums added in a
+// fixed order.
 #pragma once
 #include "egg_sieve_fast.cuh"
 
@@ -25,7 +32,7 @@ struct LevelShape {
 
 template <bool CPLX, int K>
 __global__ void __launch_bounds__(LevelShape<CPLX, K>::threads, LevelShape<CPLX, K>::min_blocks)
-    sieve_level_kernel(SieveArgs a, dd *partial)
+    sieve_level_kernel(SieveArgs a, const int64_t *__restrict__ strides, dd *partial)
 {
     constexpr int MW = 2 * K;
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
@@ -43,6 +50,20 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K>::threads, LevelShape<CPLX,
     const int wslot = blockIdx.x * cw + wib;
     const uint64_t W = (uint64_t)a.warps_per_inst;
     dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
+    // One term: the surviving edges are compacted into w.eidx / w.kval (K of them) by the caller.
+    auto eval_term = [&](double prefac) {
+        if constexpr (!CPLX) {
+            const double val = term_real<MW, (MW > 32 ? 2 : 1)>((const double *)a.Ax + in.ax_off, in.lda, E, K, n, w,
+                                                                lane);
+            if (lane == 0) dd_add(acc_re, prefac * val);
+        } else {
+            const cd val = term_cplx<MW>((const cd *)a.Ax + in.ax_off, in.lda, E, K, n, w, lane);
+            if (lane == 0) {
+                dd_add(acc_re, prefac * val.re);
+                dd_add(acc_im, prefac * val.im);
+            }
+        }
+    };
     if (in.subset && K <= E) {
         const uint64_t cnt = c_binom[E * 33 + K];
         const uint64_t lo = (uint64_t)wslot * cnt / W, hi = ((uint64_t)wslot + 1) * cnt / W;
@@ -56,18 +77,56 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K>::threads, LevelShape<CPLX,
                 w.kval[pos] = 1.0;
             }
             __syncwarp();
-            if constexpr (!CPLX) {
-                const double val = term_real<MW, (MW > 32 ? 2 : 1)>((const double *)a.Ax + in.ax_off, in.lda, E, K, n, w,
-                                                                    lane);
-                if (lane == 0) dd_add(acc_re, prefac * val);
-            } else {
-                const cd val = term_cplx<MW>((const cd *)a.Ax + in.ax_off, in.lda, E, K, n, w, lane);
-                if (lane == 0) {
-                    dd_add(acc_re, prefac * val.re);
-                    dd_add(acc_im, prefac * val.im);
-                }
-            }
+            eval_term(prefac);
             __syncwarp();
+        }
+    } else if (K <= E) {
+        // Mixed-radix odometer (src/hafnian.jl:542-580): lane i holds digit i (edge E-1 least
+        // significant), digit 0 clipped to its lower half under Glynn.  Runs of kRunTerms
+        // consecutive indices are dealt round robin: a term's size is set by its digits, and a long
+        // contiguous range fixes the high digits, so contiguous ranges would hand some warps most of
+        // a level and others none of it.
+        const int *reps = a.reps + in.reps_off;
+        const int mr1 = a.maxrep + 1;
+        const bool unit = a.maxrep <= 1;  // all multiplicities <= 1: every binomial factor is 1
+        int r = 0, base = 1, digit = 0;
+        if (lane < E) {
+            r = reps[lane];
+            base = (in.glynn && lane == 0) ? (r + 2) / 2 : r + 1;
+        }
+        constexpr int64_t kRunTerms = 16;
+        for (int64_t j0 = (int64_t)wslot * kRunTerms; j0 < in.steps; j0 += (int64_t)W * kRunTerms) {
+            const int64_t j1 = j0 + kRunTerms < in.steps ? j0 + kRunTerms : in.steps;
+            if (lane < E) digit = (int)((j0 / strides[in.reps_off + lane]) % base);
+            for (int64_t j = j0; j < j1; ++j) {
+                if (j > j0) {
+                    const unsigned notmax = __ballot_sync(FULL, lane < E && digit != base - 1);
+                    const int h = 31 - __clz(notmax);
+                    if (lane == h) ++digit;
+                    else if (lane > h && lane < E) digit = 0;
+                }
+                const int kk = lane < E ? (in.glynn ? 2 * digit - r : digit) : 0;
+                const bool nz = lane < E && kk != 0;
+                const unsigned mask = __ballot_sync(FULL, nz);
+                if (__popc(mask) != K) continue;  // another level
+                const int esum = __reduce_add_sync(FULL, lane < E ? digit : 0);
+                double bp = 1.0;
+                if (!unit) {
+                    bp = lane < E ? a.binoms[r + digit * mr1] : 1.0;
+                    for (int off = 16; off > 0; off >>= 1) bp *= __shfl_xor_sync(FULL, bp, off);
+                }
+                double prefac = ((n - esum) & 1) ? -bp : bp;
+                const int k0 = __shfl_sync(FULL, kk, 0);
+                if (in.glynn && k0 == 0) prefac *= 0.5;  // the mirror's fixed point (:570-573)
+                if (nz) {
+                    const int pos = __popc(mask & ((1u << lane) - 1u));
+                    w.eidx[pos] = lane;
+                    w.kval[pos] = (double)kk;
+                }
+                __syncwarp();
+                eval_term(prefac);
+                __syncwarp();
+            }
         }
     }
     // The block's warps summed in a fixed order: one partial per block.
@@ -91,13 +150,13 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K>::threads, LevelShape<CPLX,
 }
 
 template <bool CPLX, int K>
-static int level_launch_k(const SieveArgs &a, int B, dd *partial, int blocks_x, cudaStream_t st)
+static int level_launch_k(const SieveArgs &a, const int64_t *strides, int B, dd *partial, int blocks_x, cudaStream_t st)
 {
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
     const size_t smem = (size_t)cw * fast_ws_doubles(a.nmax, CPLX, 2 * K) * sizeof(double);
     auto k = sieve_level_kernel<CPLX, K>;
     EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<dim3((unsigned)blocks_x, (unsigned)B), cw * 32, smem, st>>>(a, partial);
+    k<<<dim3((unsigned)blocks_x, (unsigned)B), cw * 32, smem, st>>>(a, strides, partial);
     count_launch();
     EGG_CUDA_TRY(cudaGetLastError());
     return EGG_OK;

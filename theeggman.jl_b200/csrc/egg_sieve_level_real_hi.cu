@@ -4,11 +4,11 @@
 namespace egg {
 
 #define EGG_LVL_LAUNCH(CPLX, K) \
-    case K: return level_launch_k<CPLX, K>(a, B, partial, blocks_x, st);
+    case K: return level_launch_k<CPLX, K>(a, strides, B, partial, blocks_x, st);
 #define EGG_LVL_SHAPE(CPLX, K) \
     case K: rc = level_shape_k<CPLX, K>(nmax, warps_per_block, blocks_per_sm); break;
 
-int level_launch_real_hi(const SieveArgs &a, int B, int k, dd *partial, int blocks_x, cudaStream_t st)
+int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int k, dd *partial, int blocks_x, cudaStream_t st)
 {
     int rc = upload_fast_tables_once(st);
     if (rc) return rc;
