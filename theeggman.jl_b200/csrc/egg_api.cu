@@ -6,6 +6,8 @@
 // one call at a time uses the shared buffers (ext/TheEggmanKernelAbstractionsExt.jl:117-119).
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <tuple>
 
 #include "egg_internal.cuh"
 
@@ -49,6 +51,32 @@ int create_streams(Context &c, int device)
     EGG_CUDA_TRY(cudaEventCreateWithFlags(&c.fork_ev, cudaEventDisableTiming));
     EGG_CUDA_TRY(cudaEventCreateWithFlags(&c.join_ev, cudaEventDisableTiming));
     EGG_CUDA_TRY(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
+    return EGG_OK;
+}
+
+int smem_limit_at_least(const void *k, size_t bytes)
+{
+    static std::map<const void *, size_t> done;
+    auto it = done.find(k);
+    if (it != done.end() && it->second >= bytes) return EGG_OK;
+    EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done[k] = bytes;
+    return EGG_OK;
+}
+
+int blocks_per_sm(const void *k, int threads, size_t smem, int *out)
+{
+    static std::map<std::tuple<const void *, int, size_t>, int> done;
+    const auto key = std::make_tuple(k, threads, smem);
+    auto it = done.find(key);
+    if (it != done.end()) {
+        *out = it->second;
+        return EGG_OK;
+    }
+    int nb = 0;
+    EGG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem));
+    done[key] = nb;
+    *out = nb;
     return EGG_OK;
 }
 
@@ -403,6 +431,22 @@ int egg_dp_batch(int K, int idx_bytes, int dtype, int prec, const void *P, int64
     if (rc) return rc;
     rc = ensure_buf(c.scratch[2], (size_t)chunk * oes);
     if (rc) return rc;
+    const size_t in_bytes = (size_t)B * npairs * es, out_bytes = (size_t)B * oes;
+    if (chunk == B && in_bytes + out_bytes + 256 <= Context::kPinnedBytes) {
+        // A small call: both transfers through the page-locked staging buffer.
+        if (!c.pinned) EGG_CUDA_TRY(cudaHostAlloc(&c.pinned, Context::kPinnedBytes, cudaHostAllocDefault));
+        char *pin_in = (char *)c.pinned, *pin_out = pin_in + ((in_bytes + 255) / 256) * 256;
+        if (in_bytes) {
+            std::memcpy(pin_in, P, in_bytes);
+            EGG_CUDA_TRY(cudaMemcpyAsync(c.scratch[1].ptr, pin_in, in_bytes, cudaMemcpyHostToDevice, c.stream));
+        }
+        rc = dp_run(*plan, dtype, prec, c.scratch[1].ptr, B, c.scratch[2].ptr, c.stream);
+        if (rc) return rc;
+        EGG_CUDA_TRY(cudaMemcpyAsync(pin_out, c.scratch[2].ptr, out_bytes, cudaMemcpyDeviceToHost, c.stream));
+        EGG_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        std::memcpy(out, pin_out, out_bytes);
+        return EGG_OK;
+    }
     for (int64_t b0 = 0; b0 < B; b0 += chunk) {
         int64_t nb = B - b0 < chunk ? B - b0 : chunk;
         // This chunk's pairs, re-laid with the chunk's own instance count as leading dimension

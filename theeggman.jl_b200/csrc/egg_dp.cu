@@ -604,7 +604,8 @@ static int run_small(const DevPlan &plan, const PT *P, HT *out, int64_t B, size_
         maxlev = plan.levels[L].n > maxlev ? plan.levels[L].n : maxlev;
     }
     auto k = dp_small_kernel<Op, I, PT, HT, AT>;
-    EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int rc0 = smem_limit_at_least((const void *)k, smem);
+    if (rc0) return rc0;
     int64_t grid = B;
     const int64_t cap = (int64_t)ctx().num_sms * 8;
     if (grid > cap) grid = cap;
@@ -686,7 +687,8 @@ static int launch_span(const uint32_t *bt, const DevPlan &plan, const PT *P, HT 
         attr_set = true;
     }
     int per_sm = 0;
-    EGG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
+    int rc0 = blocks_per_sm((const void *)k, 256, smem, &per_sm);
+    if (rc0) return rc0;
     if (per_sm < 1) return fail(EGG_ERR_CUDA, "span kernel cannot be resident");
     int64_t need = 1;  // threads the widest level can use (a warp per state for deep levels)
     for (int L = L0; L <= L1; ++L) {
@@ -715,16 +717,18 @@ static int run_closed(const DevPlan &plan, const PT *P, HT *h0, HT *h1, HT *out,
     const uint32_t *bt = binom32_device(st, &rc);
     if (!bt) return rc;
     const int K = plan.K;
-    const size_t small = out_direct ? closed_small_smem<PT, HT>(plan) : 0;
+    // Batches of small degrees: one CTA per instance, the whole plan in shared memory.  A single
+    // instance runs as spans across the machine instead (below), which finishes sooner.
+    const size_t small = (out_direct && B > 1) ? closed_small_smem<PT, HT>(plan) : 0;
     if (small) {
-        // One instance: as many threads as keep the state type's registers unspilled.
         constexpr int kMaxT = sizeof(HT) <= 8 ? 1024 : 512;
         auto k = dpc_small_kernel<Op, PT, HT, AT, kMaxT>;
-        EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)small));
+        rc = smem_limit_at_least((const void *)k, small);
+        if (rc) return rc;
         int64_t grid = B;
         const int64_t cap = (int64_t)ctx().num_sms * 8;
         if (grid > cap) grid = cap;
-        const int threads = B == 1 ? kMaxT : (max_level(plan) >= 1024 ? 256 : 128);
+        const int threads = max_level(plan) >= 1024 ? 256 : 128;
         k<<<(unsigned)grid, threads, small, st>>>(bt, P, out, B, K, (int)max_level(plan));
         count_launch();
         EGG_CUDA_TRY(cudaGetLastError());

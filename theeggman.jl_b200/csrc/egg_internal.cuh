@@ -134,6 +134,10 @@ struct Context {
     // stream's), with the events that fork it from and join it back to the calling stream.
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // Page-locked host staging for small transfers: a copy from pageable memory is staged by the
+    // driver at a fixed cost of several microseconds, a copy from page-locked memory is not.
+    void *pinned = nullptr;
+    static constexpr size_t kPinnedBytes = 128 * 1024;
     int num_sms = 0;
     std::map<std::pair<int, int>, DevPlan> plans;
     DevBuf scratch[9];   // H, P, out, sieve matrix, sieve out, misc, mixed-degree batch + its staging:
@@ -150,6 +154,11 @@ extern std::atomic<long long> g_launches;
 inline void count_launch(long long n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int ensure_buf(DevBuf &b, size_t bytes);
+// Raises kernel k's dynamic shared-memory limit to at least `bytes`; the runtime is called only
+// when the limit last set for k is lower (callers hold the library's lock).
+int smem_limit_at_least(const void *k, size_t bytes);
+// Resident blocks per SM of kernel k at this block size and dynamic shared memory, cached.
+int blocks_per_sm(const void *k, int threads, size_t smem, int *out);
 DevPlan *find_plan(int K, int idx_bytes);
 
 // Closed-form plan size (_dp_counts, src/dp.jl:192-208).

@@ -643,10 +643,10 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     if (run_ex && all_subset) {
         // Terms dealt as equal shares of each popcount level: one wave of resident blocks.
         int nb = 0;
-        if (cplx) EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(ex_wpb * ex_per_warp)));
-        else EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(ex_wpb * ex_per_warp)));
-        if (cplx) EGG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sieve_exact_kernel<true>, ex_wpb * 32, ex_wpb * ex_per_warp));
-        else EGG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sieve_exact_kernel<false>, ex_wpb * 32, ex_wpb * ex_per_warp));
+        const void *ek = cplx ? (const void *)sieve_exact_kernel<true> : (const void *)sieve_exact_kernel<false>;
+        int rc0 = smem_limit_at_least(ek, ex_wpb * ex_per_warp);
+        if (!rc0) rc0 = blocks_per_sm(ek, ex_wpb * 32, ex_wpb * ex_per_warp, &nb);
+        if (rc0) return rc0;
         int64_t per = ((int64_t)num_sms * (nb > 0 ? nb : 1) + B - 1) / B;
         const int64_t cap = (maxsteps + ex_wpb - 1) / ex_wpb;
         ex_bx = (int)(per < cap ? (per > 0 ? per : 1) : cap);
@@ -763,13 +763,10 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         const size_t smem = (size_t)ex_wpb * ex_per_warp;
         const dim3 grid((unsigned)ex_bx, (unsigned)B);
         cudaStream_t es = ex_side ? c.side : st;
-        if (cplx) {
-            EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sieve_exact_kernel<true><<<grid, ex_wpb * 32, smem, es>>>(ae, ex_wpb);
-        } else {
-            EGG_CUDA_TRY(cudaFuncSetAttribute(sieve_exact_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sieve_exact_kernel<false><<<grid, ex_wpb * 32, smem, es>>>(ae, ex_wpb);
-        }
+        rc = smem_limit_at_least(cplx ? (const void *)sieve_exact_kernel<true> : (const void *)sieve_exact_kernel<false>, smem);
+        if (rc) return rc;
+        if (cplx) sieve_exact_kernel<true><<<grid, ex_wpb * 32, smem, es>>>(ae, ex_wpb);
+        else sieve_exact_kernel<false><<<grid, ex_wpb * 32, smem, es>>>(ae, ex_wpb);
         count_launch();
         EGG_CUDA_TRY(cudaGetLastError());
         ps.p[0] = ae.partial;

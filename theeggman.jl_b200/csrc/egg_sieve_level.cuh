@@ -155,7 +155,8 @@ static int level_launch_k(const SieveArgs &a, const int64_t *strides, int B, dd 
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
     const size_t smem = (size_t)cw * fast_ws_doubles(a.nmax, CPLX, 2 * K) * sizeof(double);
     auto k = sieve_level_kernel<CPLX, K>;
-    EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int rc = smem_limit_at_least((const void *)k, smem);
+    if (rc) return rc;
     k<<<dim3((unsigned)blocks_x, (unsigned)B), cw * 32, smem, st>>>(a, strides, partial);
     count_launch();
     EGG_CUDA_TRY(cudaGetLastError());
@@ -168,9 +169,10 @@ static int level_shape_k(int nmax, int *warps_per_block, int *blocks_per_sm)
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
     const size_t smem = (size_t)cw * fast_ws_doubles(nmax, CPLX, 2 * K) * sizeof(double);
     auto k = sieve_level_kernel<CPLX, K>;
-    EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int nb = 0;
-    EGG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, cw * 32, smem));
+    int rc = smem_limit_at_least((const void *)k, smem);
+    if (!rc) rc = egg::blocks_per_sm((const void *)k, cw * 32, smem, &nb);
+    if (rc) return rc;
     *warps_per_block = cw;
     *blocks_per_sm = nb;
     return EGG_OK;
