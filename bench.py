@@ -78,18 +78,22 @@ def profile_traffic(name: str):
 # ------------------------------------------------------------------------------------------------
 
 class SieveWorkload:
-    """One N x N sieve hafnian per step (configuration 2: N = 40, real or complex)."""
+    """One N x N sieve hafnian per step (configuration 2: N = 40, real or complex; configuration 1's
+    sieve run: N = 20 real U[-1,1])."""
 
     kind = "sieve"
 
-    def __init__(self, egg, W, N: int, cplx: bool, glynn, seed: int):
+    def __init__(self, egg, W, N: int, cplx: bool, glynn, seed: int, config: str = "2"):
         from theeggman_b200 import policy as pol
         from theeggman_b200 import roofline as R
 
         self.egg, self.N, self.cplx = egg, N, cplx
         E = N // 2
         self.E = E
-        self.A = (W.dense_complex(N, seed, 1.0 / (2 * N)) if cplx else W.dense_real(N, seed, scale=1.0 / np.sqrt(N)))
+        if config == "1":
+            self.A = W.dense_real(N, seed)
+        else:
+            self.A = (W.dense_complex(N, seed, 1.0 / (2 * N)) if cplx else W.dense_real(N, seed, scale=1.0 / np.sqrt(N)))
         sel_glynn = pol._choose_method_distinct(N, E, os.cpu_count() or 1)[1]
         self.glynn = sel_glynn if glynn is None else glynn
         x = [2 * i + 1 for i in range(E)] + [2 * i + 2 for i in range(E)]
@@ -101,7 +105,9 @@ class SieveWorkload:
         self.prec = 1  # EGG_PREC_FMA: the register-resident kernels (the API default for the sieve)
         self.hafnians_per_step = 1
         self.dtype_name = "c128" if cplx else "f64"
-        self.name = (f"config2{'b' if cplx else 'a'}: N={N} {'ComplexF64 N(0,1/(2N)) parts' if cplx else 'Float64 U[-1,1]/sqrt(N)'}, "
+        label = ("config1: N=20 Float64 U[-1,1]" if config == "1" else
+                 f"config2{'b' if cplx else 'a'}: N={N} {'ComplexF64 N(0,1/(2N)) parts' if cplx else 'Float64 U[-1,1]/sqrt(N)'}")
+        self.name = (f"{label}, "
                      f"hafnian(A; method=:sieve) = {'Glynn' if self.glynn else 'inclusion-exclusion'}, "
                      f"{2 ** (E - 1) if self.glynn else 2 ** E} terms")
 
@@ -460,6 +466,8 @@ def make_workload(name: str, egg, W, rank: int):
         return SieveWorkload(egg, W, 40, True, None, 2025 + rank)
     if name == "sieve40g":
         return SieveWorkload(egg, W, 40, False, True, 2024 + rank)
+    if name == "sieve20":
+        return SieveWorkload(egg, W, 20, False, None, 2020 + rank, config="1")
     if name == "dp20":
         return DPWorkload(egg, W, 20, 1, "f64", "exact", 2020 + rank)
     if name == "dp32":

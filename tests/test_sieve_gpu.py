@@ -144,6 +144,35 @@ def test_batch_equals_scalar(egg, orc, W, prec):
         assert rel(v, dd) <= tol
 
 
+@pytest.mark.parametrize("cplx", [False, True])
+def test_batch_mixes_subset_and_odometer_instances(egg, orc, W, cplx):
+    """One batch holding distinct-row inclusion-exclusion instances (dealt as edge subsets) beside
+    Glynn and repeated-row instances (walked on the odometer), of different edge counts: every
+    level kernel takes each instance its own way, and each result is the scalar call's."""
+    from theeggman_b200.hafnian import _sieve_device_batch
+
+    T = np.dtype(np.complex128 if cplx else np.float64)
+    Axs, reps, gs = [], [], []
+    for i, N in enumerate((8, 14, 20, 12, 16, 18)):
+        A = W.dense_complex(N, 500 + i, 0.5) if cplx else W.dense_real(N, 500 + i)
+        E = N // 2
+        Axs.append(orc.permuted(A, distinct_x(E)))
+        reps.append([1] * E)
+        gs.append(i % 3 == 1)  # two Glynn instances among the distinct-row ones
+    mats, rpts = (W.repeated_complex(4, d=10, total_max=22, seed=41) if cplx else W.repeated_real(4, 9, seed=41))
+    for A, r in zip(mats, rpts):
+        x, er = orc.matched_reps(r)
+        Axs.append(orc.permuted(A, x))
+        reps.append(er)
+        gs.append(len(Axs) % 2 == 0)
+    vals = _sieve_device_batch(T, Axs, reps, gs, "fma")
+    for Ax, er, g, v in zip(Axs, reps, gs, vals):
+        dd = orc.calc_hafnian(Ax, er, g, sum_mode=1)
+        tol = 4 * 2 * sum(er) * EPS * kappa(orc, Ax, er, g, dd) + 1e-15
+        assert rel(v, dd) <= tol, (er, g, v, dd)
+        assert rel(v, egg.sieve(Ax, er, glynn=g)) <= 1e-15
+
+
 def test_config2_full_size_cross_check(egg, W):
     """N = 40 (E = 20, 2^20 inclusion-exclusion terms / 2^19 Glynn terms), both kernels: Glynn agrees
     with the device DP (machine precision, no cancellation) within the metric's 1e-10 (the

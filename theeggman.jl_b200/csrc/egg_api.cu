@@ -47,9 +47,11 @@ int ensure_init()
 int create_streams(Context &c, int device)
 {
     EGG_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-    EGG_CUDA_TRY(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
     EGG_CUDA_TRY(cudaEventCreateWithFlags(&c.fork_ev, cudaEventDisableTiming));
-    EGG_CUDA_TRY(cudaEventCreateWithFlags(&c.join_ev, cudaEventDisableTiming));
+    for (int i = 0; i < Context::kSideStreams; ++i) {
+        EGG_CUDA_TRY(cudaStreamCreateWithFlags(&c.side[i], cudaStreamNonBlocking));
+        EGG_CUDA_TRY(cudaEventCreateWithFlags(&c.join_ev[i], cudaEventDisableTiming));
+    }
     EGG_CUDA_TRY(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, device));
     return EGG_OK;
 }

@@ -130,10 +130,12 @@ struct DevBuf {
 struct Context {
     int device = -1;
     cudaStream_t stream = nullptr;
-    // A second stream for launches that leave most of the machine idle (they overlap the main
-    // stream's), with the events that fork it from and join it back to the calling stream.
-    cudaStream_t side = nullptr;
-    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // Side streams for launches that leave most of the machine idle (they overlap the main
+    // stream's and each other), with the events that fork them from and join them back to the
+    // calling stream.
+    static constexpr int kSideStreams = 4;
+    cudaStream_t side[kSideStreams] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kSideStreams] = {};
     // Page-locked host staging for small transfers: a copy from pageable memory is staged by the
     // driver at a fixed cost of several microseconds, a copy from page-locked memory is not.
     void *pinned = nullptr;

@@ -748,13 +748,16 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         ps.p[k] = nullptr;
         ps.w[k] = 0;
     }
+    // Side launches go round robin over the side streams, the exact kernel first.
     const bool ex_side = run_ex && fast_ok;  // the exact kernel only takes the terms too large for the tiles
-    bool any_side = ex_side;
-    for (const FastLaunch &L : fl) any_side = any_side || L.side;
-    if (any_side) {
+    int nside = ex_side ? 1 : 0;
+    for (const FastLaunch &L : fl) nside += L.side ? 1 : 0;
+    const int nstreams = nside < Context::kSideStreams ? nside : Context::kSideStreams;
+    if (nstreams > 0) {
         EGG_CUDA_TRY(cudaEventRecord(c.fork_ev, st));
-        EGG_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork_ev, 0));
+        for (int i = 0; i < nstreams; ++i) EGG_CUDA_TRY(cudaStreamWaitEvent(c.side[i], c.fork_ev, 0));
     }
+    int next_side = 0;
     if (run_ex) {
         // First, so that on the side stream its long terms start at once.
         SieveArgs ae = a;
@@ -762,7 +765,8 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         ae.partial = (dd *)(base + off_pex);
         const size_t smem = (size_t)ex_wpb * ex_per_warp;
         const dim3 grid((unsigned)ex_bx, (unsigned)B);
-        cudaStream_t es = ex_side ? c.side : st;
+        cudaStream_t es = st;
+        if (ex_side) es = c.side[next_side++ % Context::kSideStreams];
         rc = smem_limit_at_least(cplx ? (const void *)sieve_exact_kernel<true> : (const void *)sieve_exact_kernel<false>, smem);
         if (rc) return rc;
         if (cplx) sieve_exact_kernel<true><<<grid, ex_wpb * 32, smem, es>>>(ae, ex_wpb);
@@ -779,7 +783,8 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         const int64_t *dstr = (const int64_t *)(base + off_str);
         for (const FastLaunch &L : fl) {
             a.warps_per_inst = L.bx * L.cw;
-            cudaStream_t ls = L.side ? c.side : st;
+            cudaStream_t ls = st;
+            if (L.side) ls = c.side[next_side++ % Context::kSideStreams];
             rc = cplx ? level_launch_cplx(a, dstr, (int)B, L.level, part, L.bx, ls)
                       : level_launch_real(a, dstr, (int)B, L.level, part, L.bx, ls);
             if (rc) return rc;
@@ -789,9 +794,9 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             ++slot;
         }
     }
-    if (any_side) {
-        EGG_CUDA_TRY(cudaEventRecord(c.join_ev, c.side));
-        EGG_CUDA_TRY(cudaStreamWaitEvent(st, c.join_ev, 0));
+    for (int i = 0; i < nstreams; ++i) {
+        EGG_CUDA_TRY(cudaEventRecord(c.join_ev[i], c.side[i]));
+        EGG_CUDA_TRY(cudaStreamWaitEvent(st, c.join_ev[i], 0));
     }
     if (terms) {
         EGG_CUDA_TRY(cudaGetLastError());
