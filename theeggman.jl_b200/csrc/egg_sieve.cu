@@ -11,6 +11,8 @@
 // Work layout.  Instance b's terms j = 0..steps-1 are dealt round-robin to that instance's warps
 // (grid.y = instance).  The mixed-radix odometer (edge E least significant, the leading digit
 // clipped to its lower half under Glynn, :655-657) is decoded per term.
+#include <cstring>
+
 #include "egg_sieve.cuh"
 
 namespace egg {
@@ -725,12 +727,17 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         if (rc) return rc;
         base = (char *)c.scratch[5].ptr;
     }
-    EGG_CUDA_TRY(cudaMemcpyAsync(base + off_inst, inst.data(), inst.size() * sizeof(SieveInst), cudaMemcpyHostToDevice, st));
-    if (!reps.empty())
-        EGG_CUDA_TRY(cudaMemcpyAsync(base + off_reps, reps.data(), reps.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-    if (!strides.empty())
-        EGG_CUDA_TRY(cudaMemcpyAsync(base + off_str, strides.data(), strides.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-    EGG_CUDA_TRY(cudaMemcpyAsync(base + off_bin, binoms.data(), binoms.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    {
+        // The instance table, reps, strides and binomials in their device layout, sent as one copy
+        // (each copy from pageable memory has a fixed staging cost).
+        const size_t img = (size_t)(off_bin + (int64_t)(binoms.size() * sizeof(double)));
+        std::vector<char> h(img, 0);
+        std::memcpy(h.data() + off_inst, inst.data(), inst.size() * sizeof(SieveInst));
+        if (!reps.empty()) std::memcpy(h.data() + off_reps, reps.data(), reps.size() * sizeof(int));
+        if (!strides.empty()) std::memcpy(h.data() + off_str, strides.data(), strides.size() * sizeof(int64_t));
+        std::memcpy(h.data() + off_bin, binoms.data(), binoms.size() * sizeof(double));
+        EGG_CUDA_TRY(cudaMemcpyAsync(base, h.data(), img, cudaMemcpyHostToDevice, st));
+    }
     SieveArgs a;
     a.Ax = dAx;
     a.reps = (const int *)(base + off_reps);

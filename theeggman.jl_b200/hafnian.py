@@ -240,18 +240,24 @@ def _sieve_device_batch(T: np.dtype, Axs: list[np.ndarray], reps_list: list[list
     B = len(Axs)
     cplx = np.dtype(T).kind == "c"
     CT = np.complex128 if cplx else np.float64
-    Emax = max((len(r) for r in reps_list), default=0)
+    E = np.fromiter((len(r) for r in reps_list), dtype=np.int64, count=B)
+    Emax = int(E.max()) if B else 0
     lda = max(2 * Emax, 1)
-    slab = np.zeros((B, lda, lda), dtype=CT)  # per instance: column-major leading block
-    for b, (Ax, r) in enumerate(zip(Axs, reps_list)):
-        m = 2 * len(r)
-        if m:
-            slab[b, :m, :m] = np.asarray(Ax, dtype=CT).T  # store transposed so memory is column-major
-    E = np.array([len(r) for r in reps_list], dtype=np.int64)
-    reps = np.zeros((B, max(Emax, 1)), dtype=np.int64)
-    for b, r in enumerate(reps_list):
-        reps[b, : len(r)] = r
-    g = np.array([1 if x else 0 for x in glynns], dtype=np.int32)
+    if B and Emax and int(E.min()) == Emax:
+        # Every instance the same size (a batch of one pattern): one stacked transpose, so each
+        # instance's block is column-major.
+        slab = np.ascontiguousarray(np.stack([np.asarray(a) for a in Axs]).astype(CT, copy=False).transpose(0, 2, 1))
+        reps = np.array(reps_list, dtype=np.int64).reshape(B, Emax)
+    else:
+        slab = np.zeros((B, lda, lda), dtype=CT)  # per instance: column-major leading block
+        for b, (Ax, r) in enumerate(zip(Axs, reps_list)):
+            m = 2 * len(r)
+            if m:
+                slab[b, :m, :m] = np.asarray(Ax, dtype=CT).T  # store transposed so memory is column-major
+        reps = np.zeros((B, max(Emax, 1)), dtype=np.int64)
+        for b, r in enumerate(reps_list):
+            reps[b, : len(r)] = r
+    g = np.fromiter((1 if x else 0 for x in glynns), dtype=np.int32, count=B)
     if prec == "reference":
         # The reference's batch loop runs each instance with nthreads = 1, i.e. one chunk
         # (src/hafnian.jl:1297-1300, :1355-1358).
