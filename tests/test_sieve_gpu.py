@@ -173,6 +173,20 @@ def test_batch_mixes_subset_and_odometer_instances(egg, orc, W, cplx):
         assert rel(v, egg.sieve(Ax, er, glynn=g)) <= 1e-15
 
 
+@pytest.mark.parametrize("glynn", [False, True])
+def test_two_rows_per_lane_tiles(egg, orc, W, glynn):
+    """Real terms with 32 < m <= 48 run on tiles of two rows per lane (La Budde's table by two
+    diagonals per lane): N = 34 puts every Glynn term, and the largest inclusion-exclusion terms,
+    there.  Bar as for the other register-tile results: 4 N eps kappa against the oracle's
+    double-double sum of the reference's terms."""
+    N, E = 34, 17
+    A = W.dense_real(N, 3434, scale=1.0 / np.sqrt(N))
+    Ax = orc.permuted(A, distinct_x(E))
+    dd = orc.calc_hafnian(Ax, [1] * E, glynn, nthreads=8, sum_mode=1)
+    got = egg.sieve(Ax, [1] * E, glynn=glynn, prec="fma")
+    assert rel(got, dd) <= 4 * N * EPS * kappa(orc, Ax, [1] * E, glynn, dd) + 1e-15, (got, dd)
+
+
 def test_config2_full_size_cross_check(egg, W):
     """N = 40 (E = 20, 2^20 inclusion-exclusion terms / 2^19 Glynn terms), both kernels: Glynn agrees
     with the device DP (machine precision, no cancellation) within the metric's 1e-10 (the

@@ -22,8 +22,8 @@
 //
 // La Budde's recurrence (src/hafnian.jl:454-492): each finished Hessenberg column stores its
 // order-k coefficients; after the reduction lane d computes diagonal d of the coefficient table in
-// registers (labudde_diag).  Tiles of two rows per lane instead feed each column at once into a
-// shared-memory table walked along diagonals (labudde_row).  The [lambda^n] series coefficient
+// registers (labudde_diag), and diagonal d + 32 too for tiles of two rows per lane
+// (labudde_diag2).  The [lambda^n] series coefficient
 // (src/hafnian.jl:502-514) is accumulated push-style: once f_s is known every lane t > s adds its
 // (t+s) q_{t-s} f_s, so each order costs one multiply-add per lane and one broadcast.  All arithmetic
 // is FP64 with fused multiply-adds; terms are accumulated in double-double per warp.
@@ -94,12 +94,9 @@ __device__ __forceinline__ unsigned pivot_key(double a, int slot)
 struct FastWs {
     double *prow;  // pivot row, by physical slot [64]
     double *wv;    // column-update weights, by physical slot [64]
-    double *cf;    // La Budde coefficients coef_i, by i [64] (tiles of two rows per lane)
-    double *C;     // La Budde coefficient table by diagonals, (mhi+1) x (mhi+1) values (tiles of two
-                   // rows per lane, see labudde_row)
-    double *cft;   // La Budde coefficients of every order k, a triangle (one-row tiles, see labudde_diag)
-    double *hk;    // Hessenberg diagonal h_kk by k [mhi + 1] (one-row tiles)
-    double *q;     // det(I - lambda H) coefficients q_j by j [32] (one-row tiles)
+    double *cft;   // La Budde coefficients of every order k, a triangle (see labudde_diag)
+    double *hk;    // Hessenberg diagonal h_kk by k [mhi + 1]
+    double *q;     // det(I - lambda H) coefficients q_j by j [32]
     double *kval;  // multiplicities of the surviving edges after the Glynn substitution [32]
     int *eidx;     // surviving edges, compacted [32]
 };
@@ -112,14 +109,13 @@ __host__ __device__ constexpr int cft_row_cplx(int k) { return (k - 1) * (k - 2)
 __host__ __device__ inline size_t fast_body_doubles(int cplx, int mhi)
 {
     const size_t v = cplx ? 2 : 1;  // doubles per value
-    if (mhi > 32) return v * (size_t)(mhi + 1) * (mhi + 1);
     const size_t tri = cplx ? 2 * (size_t)cft_row_cplx(mhi + 1) : (size_t)cft_row_real(mhi + 1);
     return tri + v * (size_t)((mhi + 2) & ~1) + v * 32;
 }
 
 __host__ __device__ inline size_t fast_ws_doubles(int nmax, int cplx, int mhi)
 {
-    size_t d = 64 * 3 + fast_body_doubles(cplx, mhi) + 32 /*kval*/ + 16 /*eidx*/;
+    size_t d = 64 * 2 + fast_body_doubles(cplx, mhi) + 32 /*kval*/ + 16 /*eidx*/;
     return (d + 1) & ~(size_t)1;  // keep every warp's region 16-byte aligned
 }
 
@@ -130,75 +126,21 @@ __device__ inline FastWs fast_carve(double *base, int nmax, int cplx, int mhi)
     double *p = base;
     w.prow = p; p += 64;
     w.wv = p; p += 64;
-    w.cf = p; p += 64;
-    w.C = p;
     w.cft = p;
-    if (mhi <= 32) {
-        w.hk = w.cft + (cplx ? 2 * (size_t)cft_row_cplx(mhi + 1) : (size_t)cft_row_real(mhi + 1));
-        w.q = w.hk + v * (size_t)((mhi + 2) & ~1);
-    } else {
-        w.hk = w.q = nullptr;
-    }
+    w.hk = w.cft + (cplx ? 2 * (size_t)cft_row_cplx(mhi + 1) : (size_t)cft_row_real(mhi + 1));
+    w.q = w.hk + v * (size_t)((mhi + 2) & ~1);
     p += fast_body_doubles(cplx, mhi);
     w.kval = p; p += 32;
     w.eidx = (int *)p;
     return w;
 }
 
-// ---- La Budde row k (1-based); lane t (0..n) owns coefficient t ----------------------------------
-//   C[k][t] = (t <= min(k-1,n) ? C[k-1][t] : 0) - hkk C[k-1][t-1] - sum_{j=1}^{jmax} cf[k-j] C[k-1-j][t-1-j]
-// (j = k - i of the reference's i loop, which runs i = k-1 .. max(1, k-n+1)).  The table is stored
-// by diagonals: C[r][c] at T[(r - c) * rs + r].  Every entry of lane t's depth sum lies on its
-// diagonal d = k - t, at rows k-2, k-3, ..., so the sum walks one contiguous run.  Entries left of
-// column 0 (r < d) are zero -- they are cleared once per warp and never written -- so the walk
-// needs no bounds test; entries right of the diagonal (c > r) are never read.  Every entry read
-// in a term was written earlier in the same term.
-__device__ __forceinline__ void labudde_row(double *T, const double *cf, int k, int n, int rs, double hkk, int lane)
-{
-    const int t = lane;
-    const int tmax = k < n ? k : n;
-    const int d = k - t;  // negative for lanes past row k: clamped below, their result is not stored
-    double v = 0.0;
-    if (t <= tmax) {
-        const double a = t <= k - 1 ? T[(d - 1) * rs + (k - 1)] : 0.0;  // C[k-1][t]
-        const double b = t >= 1 ? T[d * rs + (k - 1)] : 0.0;            // C[k-1][t-1]
-        v = a - hkk * b;
-    }
-    const int jmax = (k - 1) < (n - 1) ? (k - 1) : (n - 1);
-    const double *cfk = cf + k;
-    const double *Td = T + (d > 0 ? d : 0) * rs + (k - 2);  // C[k-1-j][t-1-j] at Td[1 - j]
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-#pragma unroll
-    for (int j = 1; j <= 31; ++j) {
-        if (j > jmax) break;
-        const double c = cfk[-j];
-        const double x = Td[1 - j];
-        if ((j & 3) == 1) a0 = fma(c, x, a0);
-        else if ((j & 3) == 2) a1 = fma(c, x, a1);
-        else if ((j & 3) == 3) a2 = fma(c, x, a2);
-        else a3 = fma(c, x, a3);
-    }
-    if (t <= tmax) T[d * rs + k] = v - ((a0 + a1) + (a2 + a3));
-}
-
-// [lambda^n] det(I - lambda H)^(-1/2), push-style: lane t accumulates S_t = sum_j (2t-j) q_j f_{t-j}
-// as the f's become known; f_t = -S_t / (2t).  q_j = C[m][j] = T[(m - j) * rs + m].  All lanes
-// return f_n.
-__device__ __forceinline__ double series_coeff(const double *T, int m, int n, int rs, int lane)
-{
-    double S = 0.0, fs = 1.0;  // fs = f_s, starting at f_0 = 1
-    for (int s = 0; s < n; ++s) {
-        const int j = lane - s;
-        if (j >= 1 && j <= m && lane <= n) S = fma((double)(lane + s) * T[(m - j) * rs + m], fs, S);
-        fs = __shfl_sync(FULL, S, s + 1) * c_neg_inv_2t[s + 1];
-    }
-    return fs;
-}
-
 // ---- La Budde by diagonals, in registers (tiles of one row per lane) ------------------------------
-// The same recurrence as labudde_row, run after the Hessenberg reduction from the coefficients it
-// stored: for order k, cft[cft_row(k) + i - 1] = h_{i,k} prod_{l=i+1..k} h_{l,l-1} (i = 1..k-1) and
-// hk[k] = h_{k,k}.  Lane d owns diagonal d of the table, D[r] = C[r][r - d], zero left of column 0:
+// La Budde's recurrence over the leading minors (src/hafnian.jl:454-492), with C[k][t] the
+// coefficient of lambda^t in det(I - lambda H_k), run after the Hessenberg reduction from the
+// coefficients it stored: for order k, cft[cft_row(k) + i - 1] = h_{i,k} prod_{l=i+1..k} h_{l,l-1}
+// (i = 1..k-1) and hk[k] = h_{k,k}.  Lane d owns diagonal d of the table, D[r] = C[r][r - d], zero
+// left of column 0:
 //   C[k][t] = C[k-1][t] - h_kk C[k-1][t-1] - sum_{i=1}^{k-1} cf_k[i] C[i-1][t-1-(k-i)],
 // where C[k-1][t] lies on diagonal d - 1 (one shuffle) and every other entry on the lane's own
 // diagonal, so with k unrolled every index is a compile-time register.  Columns beyond n are
@@ -228,6 +170,54 @@ __device__ __forceinline__ void labudde_diag(const double *__restrict__ cft, con
         }
         D[k] = fma(-hk[k], D[k - 1], up) - (s0 + s1);
         if (k == m && lane < m && lane >= m - n) q[m - lane] = D[k];
+    }
+}
+
+// Tiles of two rows per lane (33 <= m <= 48): lane l owns diagonals l and l + 32.  The upper one
+// has entries only in rows r >= 32 (at Dh[r - 32]); its entry above-right lies on diagonal l + 31,
+// lane l - 1's upper diagonal, or lane 31's lower one for l = 0.
+template <int MW>
+__device__ __forceinline__ void labudde_diag2(const double *__restrict__ cft, const double *__restrict__ hk, double *q,
+                                              int m, int n, int lane)
+{
+    static_assert(MW > 32 && MW <= 64, "two diagonals per lane");
+    double Dl[MW + 1], Dh[MW - 31];
+    Dl[0] = lane == 0 ? 1.0 : 0.0;
+#pragma unroll
+    for (int r = 1; r <= MW; ++r) Dl[r] = 0.0;
+#pragma unroll
+    for (int r = 0; r < MW - 31; ++r) Dh[r] = 0.0;
+#pragma unroll
+    for (int k = 1; k <= MW; ++k) {
+        if (k > m) break;
+        const double h = hk[k];
+        const double *row = cft + cft_row_real(k);
+        double up = __shfl_up_sync(FULL, Dl[k - 1], 1);
+        if (lane == 0) up = 0.0;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int i = 1; i < k; i += 2) {
+            const double2 c2 = *reinterpret_cast<const double2 *>(row + (i - 1));
+            s0 = fma(c2.x, Dl[i - 1], s0);
+            if (i + 1 < k) s1 = fma(c2.y, Dl[i], s1);
+        }
+        if (k >= 32) {
+            // Upper diagonal, row k (k - 1 >= 31: Dh[k - 33] is row k - 1 when k >= 33).
+            const double prev = k >= 33 ? Dh[k - 33] : 0.0;
+            double uh = __shfl_up_sync(FULL, prev, 1);
+            const double from31 = __shfl_sync(FULL, Dl[k - 1], 31);
+            if (lane == 0) uh = from31;
+            double t = 0.0;
+#pragma unroll
+            for (int i = 33; i < k; ++i) t = fma(row[i - 1], Dh[i - 33], t);  // rows i - 1 >= 32
+            Dh[k - 32] = fma(-h, prev, uh) - t;
+        }
+        Dl[k] = fma(-h, Dl[k - 1], up) - (s0 + s1);
+        if (k == m) {
+            const int jl = m - lane, jh = m - lane - 32;
+            if (jl >= 1 && jl <= n) q[jl] = Dl[k];
+            if (jh >= 1 && jh <= n) q[jh] = Dh[k - 32];
+        }
     }
 }
 
@@ -273,7 +263,8 @@ __device__ __forceinline__ void labudde_diag_c(const cd *__restrict__ cft, const
     }
 }
 
-// [lambda^n] det(I - lambda H)^(-1/2) from q_1..q_min(m,n), as series_coeff.
+// [lambda^n] det(I - lambda H)^(-1/2) from q_1..q_min(m,n), push-style: lane t accumulates
+// S_t = sum_j (2t-j) q_j f_{t-j} as the f's become known; f_t = -S_t / (2t).  All lanes return f_n.
 __device__ __forceinline__ double series_q(const double *q, int m, int n, int lane)
 {
     double S = 0.0, fs = 1.0;
@@ -309,9 +300,8 @@ template <int MW, int RPL>
 __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int lda, int E, int mE, int n,
                                             const FastWs &ws, int lane)
 {
-    constexpr int rs = MW + 1;  // La Budde table row stride
     const int m = 2 * mE;
-    double *prow = ws.prow, *wv = ws.wv, *cf = ws.cf, *C = ws.C;
+    double *prow = ws.prow, *wv = ws.wv;
     double R[RPL][MW];
     int lab[RPL];
     double pc[RPL], bet[RPL];
@@ -334,8 +324,6 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
         }
         pc[q] = R[q][0];
     }
-    if (RPL > 1 && lane == 0) C[0] = 1.0;  // La Budde row 0: C[0][0] = 1
-    int hslot = 0;       // physical slot of label s-1 (label 0 never moves)
     double xprev = 0.0;  // subdiagonal entry h_{s,s-1} of the previous step
     for (int s = 1; s <= m - 2; ++s) {
         // -- pivot among rows with s <= label < m
@@ -353,24 +341,14 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
         const int labp = (RPL > 1 && pq == 1) ? lab[RPL - 1] : lab[0];
         const double x = __shfl_sync(FULL, pcp, plane);
         const int plab = __shfl_sync(FULL, labp, plane);
-        // -- column s-1 is final for rows with label <= s-1 plus the pivot; feed La Budde step k = s
-        if constexpr (RPL == 1) {
-            // Stored for labudde_diag, which runs once the reduction is done.
-            if (lab[0] <= s - 3) bet[0] *= xprev;
-            else if (lab[0] == s - 2) bet[0] = xprev;
-            if (lab[0] <= s - 2) ws.cft[cft_row_real(s) + lab[0]] = pc[0] * bet[0];
-            if (lab[0] == s - 1) ws.hk[s] = pc[0];
-        } else {
-            const double hcand = (RPL > 1 && (hslot >> 5) == 1) ? pc[RPL - 1] : pc[0];
-            const double hkk = __shfl_sync(FULL, hcand, hslot & 31);
+        // -- column s-1 is final for rows with label <= s-1 plus the pivot: store La Budde's order
+        //    k = s coefficients for labudde_diag, which runs once the reduction is done
 #pragma unroll
-            for (int q = 0; q < RPL; ++q) {
-                if (lab[q] <= s - 3) bet[q] *= xprev;
-                else if (lab[q] == s - 2) bet[q] = xprev;
-                if (lab[q] <= s - 2) cf[lab[q] + 1] = pc[q] * bet[q];
-            }
-            __syncwarp();
-            labudde_row(C, cf, s, n, rs, hkk, lane);
+        for (int q = 0; q < RPL; ++q) {
+            if (lab[q] <= s - 3) bet[q] *= xprev;
+            else if (lab[q] == s - 2) bet[q] = xprev;
+            if (lab[q] <= s - 2) ws.cft[cft_row_real(s) + lab[q]] = pc[q] * bet[q];
+            if (lab[q] == s - 1) ws.hk[s] = pc[q];
         }
         // -- relabel (similarity swap of logical s and plab)
 #pragma unroll
@@ -378,7 +356,6 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
             if (lab[q] == s) lab[q] = plab;
             else if (lab[q] == plab) lab[q] = s;
         }
-        hslot = pslot;
         xprev = x;
         if (x == 0.0) {
             // Nothing to eliminate (:231-232): the next pivot column is the physical slot of label s.
@@ -466,38 +443,22 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
             const double cand = (RPL > 1 && (lastslot >> 5) == 1) ? pc[RPL - 1] : pc[0];
             sub = __shfl_sync(FULL, cand, lastslot & 31);
         }
-        double hkk = 0.0;
 #pragma unroll
         for (int q = 0; q < RPL; ++q) {
             const double colv = last ? colm1[q] : pc[q];
             if (k >= 2) {
                 if (lab[q] <= k - 3) bet[q] *= sub;
                 else if (lab[q] == k - 2) bet[q] = sub;
-                if (lab[q] <= k - 2) {
-                    if constexpr (RPL == 1) ws.cft[cft_row_real(k) + lab[q]] = colv * bet[q];
-                    else cf[lab[q] + 1] = colv * bet[q];
-                }
+                if (lab[q] <= k - 2) ws.cft[cft_row_real(k) + lab[q]] = colv * bet[q];
             }
-            if (lab[q] == k - 1) hkk = colv;
-        }
-        if constexpr (RPL == 1) {
-            if (lab[0] == k - 1) ws.hk[k] = hkk;
-        } else {
-            const int hs = last ? lastslot : hslot;
-            hkk = __shfl_sync(FULL, hkk, hs & 31);
-            __syncwarp();
-            labudde_row(C, cf, k, n, rs, hkk, lane);
-            __syncwarp();
+            if (lab[q] == k - 1) ws.hk[k] = colv;
         }
     }
-    if constexpr (RPL == 1) {
-        __syncwarp();
-        labudde_diag<MW>(ws.cft, ws.hk, ws.q, m, n, lane);
-        __syncwarp();
-        return series_q(ws.q, m, n, lane);
-    } else {
-        return series_coeff(C, m, n, rs, lane);
-    }
+    __syncwarp();
+    if constexpr (RPL == 1) labudde_diag<MW>(ws.cft, ws.hk, ws.q, m, n, lane);
+    else labudde_diag2<MW>(ws.cft, ws.hk, ws.q, m, n, lane);
+    __syncwarp();
+    return series_q(ws.q, m, n, lane);
 }
 
 // ---- one complex term, m <= 32 --------------------------------------------------------------------

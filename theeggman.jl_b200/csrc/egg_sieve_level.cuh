@@ -42,11 +42,6 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K>::threads, LevelShape<CPLX,
     const SieveInst in = a.inst[b];
     const int E = in.E, n = in.n;
     const FastWs w = fast_carve(smem + (size_t)wib * fast_ws_doubles(a.nmax, CPLX, MW), a.nmax, CPLX, MW);
-    if constexpr (MW > 32) {
-        // The La Budde table's entries left of column 0 must read as zero; nothing ever writes them.
-        for (int i = lane; i < (MW + 1) * (MW + 1); i += 32) w.C[i] = 0.0;
-        __syncwarp();
-    }
     const int wslot = blockIdx.x * cw + wib;
     const uint64_t W = (uint64_t)a.warps_per_inst;
     dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
