@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <tuple>
 
 #include "egg_internal.cuh"
@@ -58,6 +59,9 @@ int create_streams(Context &c, int device)
 
 int smem_limit_at_least(const void *k, size_t bytes)
 {
+    // Own lock: the entry point that allocates nothing reaches this without the library's lock.
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
     static std::map<const void *, size_t> done;
     auto it = done.find(k);
     if (it != done.end() && it->second >= bytes) return EGG_OK;
@@ -68,6 +72,8 @@ int smem_limit_at_least(const void *k, size_t bytes)
 
 int blocks_per_sm(const void *k, int threads, size_t smem, int *out)
 {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
     static std::map<std::tuple<const void *, int, size_t>, int> done;
     const auto key = std::make_tuple(k, threads, smem);
     auto it = done.find(key);

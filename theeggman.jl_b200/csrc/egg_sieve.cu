@@ -755,10 +755,13 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         ps.p[k] = nullptr;
         ps.w[k] = 0;
     }
-    // Side launches go round robin over the side streams, the exact kernel first.
-    const bool ex_side = run_ex && fast_ok;  // the exact kernel only takes the terms too large for the tiles
+    // Side launches go round robin over the library's side streams, the exact kernel first.  With
+    // caller-provided scratch (the entry point that allocates nothing) everything stays on the
+    // caller's stream: that path uses nothing of the library's context.
+    const bool side_ok = fixed == nullptr;
+    const bool ex_side = side_ok && run_ex && fast_ok;  // the exact kernel only takes the terms too large for the tiles
     int nside = ex_side ? 1 : 0;
-    for (const FastLaunch &L : fl) nside += L.side ? 1 : 0;
+    for (const FastLaunch &L : fl) nside += (side_ok && L.side) ? 1 : 0;
     const int nstreams = nside < Context::kSideStreams ? nside : Context::kSideStreams;
     if (nstreams > 0) {
         EGG_CUDA_TRY(cudaEventRecord(c.fork_ev, st));
@@ -791,7 +794,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         for (const FastLaunch &L : fl) {
             a.warps_per_inst = L.bx * L.cw;
             cudaStream_t ls = st;
-            if (L.side) ls = c.side[next_side++ % Context::kSideStreams];
+            if (side_ok && L.side) ls = c.side[next_side++ % Context::kSideStreams];
             rc = cplx ? level_launch_cplx(a, dstr, (int)B, L.level, part, L.bx, ls)
                       : level_launch_real(a, dstr, (int)B, L.level, part, L.bx, ls);
             if (rc) return rc;

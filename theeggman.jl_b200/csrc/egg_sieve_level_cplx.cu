@@ -1,4 +1,6 @@
 // egg_sieve_level_cplx.cu -- popcount-level sieve kernels for ComplexF64 terms, m = 2 .. 32.
+#include <mutex>
+
 #include "egg_sieve_level.cuh"
 
 namespace egg {
@@ -20,6 +22,8 @@ int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, 
 
 int level_shape_cplx(int nmax, int k, int *warps_per_block, int *blocks_per_sm)
 {
+    static std::mutex mu;  // the entry point that allocates nothing reaches this without the library's lock
+    std::lock_guard<std::mutex> lk(mu);
     static int cache[kLevelMaxCplx + 1][2];
     if (k >= 1 && k <= kLevelMaxCplx && cache[k][1] > 0) {
         *warps_per_block = cache[k][0];

@@ -1,4 +1,6 @@
 // egg_sieve_level_real_hi.cu -- popcount-level sieve kernels for Float64 terms, m = 34 .. 48 (two rows per lane).
+#include <mutex>
+
 #include "egg_sieve_level.cuh"
 
 namespace egg {
@@ -20,6 +22,8 @@ int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int 
 
 int level_shape_real_hi(int nmax, int k, int *warps_per_block, int *blocks_per_sm)
 {
+    static std::mutex mu;  // the entry point that allocates nothing reaches this without the library's lock
+    std::lock_guard<std::mutex> lk(mu);
     static int cache[kLevelMaxReal + 1][2];
     if (k >= 1 && k <= kLevelMaxReal && cache[k][1] > 0) {
         *warps_per_block = cache[k][0];
