@@ -663,7 +663,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     // the terms too large for the tiles.
     struct FastLaunch {
         int level, cw, bx;
-        bool side;
+        bool side, narrow;
     };
     std::vector<FastLaunch> fl;
     int64_t f_parts = 0;  // sum over launches of partials (one per block) per instance
@@ -685,12 +685,17 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             }
             for (int k = 1; k <= kmax && k <= si.E; ++k) lvl[(size_t)k] += cnt[(size_t)k];
         }
+        // Tiles of up to 16 rows take two terms per warp when every odometer instance has at most 16
+        // edges (one lane per digit); distinct-row instances need no digits.
+        int64_t e_odo = 0;
+        for (const SieveInst &si : inst) e_odo = (!si.subset && si.E > e_odo) ? si.E : e_odo;
         for (int k = 1; k <= kmax; ++k) {
             if (lvl[(size_t)k] <= 0.0) continue;
+            const bool narrow = 2 * k <= 16 && e_odo <= 16;
             int cw = 0, bps = 0;
-            int rc0 = cplx ? level_shape_cplx(nmax, k, &cw, &bps) : level_shape_real(nmax, k, &cw, &bps);
+            int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, &cw, &bps) : level_shape_real(nmax, k, narrow, &cw, &bps);
             if (rc0) return rc0;
-            if (bps < 1 || (size_t)cw * fast_ws_bytes(nmax, cplx, 2 * k) > 220 * 1024)
+            if (bps < 1 || (size_t)cw * (narrow ? 2 : 1) * fast_ws_bytes(nmax, cplx, 2 * k) > 220 * 1024)
                 return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
             // Distinct-row levels deal equal shares: one wave.  Odometer runs are only balanced on
             // average and instances differ in size, so those levels get about four waves of blocks
@@ -700,7 +705,8 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             const int64_t cap = (maxsteps + cw - 1) / cw;  // no more warps than terms
             if (per > cap) per = cap;
             if (per < 1) per = 1;
-            fl.push_back(FastLaunch{k, cw, (int)per, lvl[(size_t)k] <= 2.0 * (double)(num_sms * bps * cw)});
+            const double slots = (double)num_sms * bps * cw * (narrow ? 2 : 1);  // terms in flight
+            fl.push_back(FastLaunch{k, cw, (int)per, lvl[(size_t)k] <= 2.0 * slots, narrow});
             f_parts += per;
         }
     }
@@ -795,8 +801,8 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             a.warps_per_inst = L.bx * L.cw;
             cudaStream_t ls = st;
             if (side_ok && L.side) ls = c.side[next_side++ % Context::kSideStreams];
-            rc = cplx ? level_launch_cplx(a, dstr, (int)B, L.level, part, L.bx, ls)
-                      : level_launch_real(a, dstr, (int)B, L.level, part, L.bx, ls);
+            rc = cplx ? level_launch_cplx(a, dstr, (int)B, L.level, L.narrow, part, L.bx, ls)
+                      : level_launch_real(a, dstr, (int)B, L.level, L.narrow, part, L.bx, ls);
             if (rc) return rc;
             ps.p[slot] = part;
             ps.w[slot] = L.bx;

@@ -31,13 +31,17 @@ constexpr int kLevelMaxReal = 24, kLevelMaxCplx = 16;
 constexpr int kMaxPartials = 26;  // the exact kernel and up to 25 level launches
 size_t fast_ws_bytes(int nmax, int cplx, int mhi);  // one warp's scratch for a tile of mhi columns
 // Launches level k on a grid of blocks_x x B blocks; a.warps_per_inst must be blocks_x times the
-// level's warps per block.  Each block writes one partial (re, im) per instance.
-int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, dd *partial, int blocks_x, cudaStream_t st);
-int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int k, dd *partial, int blocks_x, cudaStream_t st);
-int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, dd *partial, int blocks_x, cudaStream_t st);
+// level's warps per block.  Each block writes one partial (re, im) per instance.  `narrow` puts
+// two terms in each warp for tiles of up to 16 rows (odometer instances then need E <= 16).
+int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
+                      cudaStream_t st);
+int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
+                         cudaStream_t st);
+int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
+                      cudaStream_t st);
 // The level's block size in warps and how many of its blocks one SM holds.
-int level_shape_real(int nmax, int k, int *warps_per_block, int *blocks_per_sm);
-int level_shape_real_hi(int nmax, int k, int *warps_per_block, int *blocks_per_sm);
-int level_shape_cplx(int nmax, int k, int *warps_per_block, int *blocks_per_sm);
+int level_shape_real(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm);
+int level_shape_real_hi(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm);
+int level_shape_cplx(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm);
 
 }  // namespace egg

@@ -147,9 +147,9 @@ __device__ inline FastWs fast_carve(double *base, int nmax, int cplx, int mhi)
 // computed too but never read by the columns <= n.  The depth sum runs over all i: entries left of
 // column 0 are exact zeros.  Diagonal 32 (only C[32][0] = 1, never read) has no lane.
 // q_j = C[m][j] (j = 1..min(m, n)) goes to q[j] for the series.
-template <int MW>
+template <int MW, int G>
 __device__ __forceinline__ void labudde_diag(const double *__restrict__ cft, const double *__restrict__ hk, double *q,
-                                             int m, int n, int lane)
+                                             int m, int n, int lane, unsigned gm)
 {
     double D[MW + 1];
     D[0] = lane == 0 ? 1.0 : 0.0;
@@ -158,7 +158,7 @@ __device__ __forceinline__ void labudde_diag(const double *__restrict__ cft, con
 #pragma unroll
     for (int k = 1; k <= MW; ++k) {
         if (k > m) break;
-        double up = __shfl_up_sync(FULL, D[k - 1], 1);
+        double up = __shfl_up_sync(gm, D[k - 1], 1, G);
         if (lane == 0) up = 0.0;
         const double *row = cft + cft_row_real(k);
         double s0 = 0.0, s1 = 0.0;
@@ -221,9 +221,9 @@ __device__ __forceinline__ void labudde_diag2(const double *__restrict__ cft, co
     }
 }
 
-template <int MW>
+template <int MW, int G>
 __device__ __forceinline__ void labudde_diag_c(const cd *__restrict__ cft, const cd *__restrict__ hk, cd *q, int m, int n,
-                                               int lane)
+                                               int lane, unsigned gm)
 {
     double Dr[MW + 1], Di[MW + 1];
     Dr[0] = lane == 0 ? 1.0 : 0.0;
@@ -236,7 +236,7 @@ __device__ __forceinline__ void labudde_diag_c(const cd *__restrict__ cft, const
 #pragma unroll
     for (int k = 1; k <= MW; ++k) {
         if (k > m) break;
-        double ur = __shfl_up_sync(FULL, Dr[k - 1], 1), ui = __shfl_up_sync(FULL, Di[k - 1], 1);
+        double ur = __shfl_up_sync(gm, Dr[k - 1], 1, G), ui = __shfl_up_sync(gm, Di[k - 1], 1, G);
         if (lane == 0) {
             ur = 0.0;
             ui = 0.0;
@@ -263,43 +263,67 @@ __device__ __forceinline__ void labudde_diag_c(const cd *__restrict__ cft, const
     }
 }
 
-// [lambda^n] det(I - lambda H)^(-1/2) from q_1..q_min(m,n), push-style: lane t accumulates
-// S_t = sum_j (2t-j) q_j f_{t-j} as the f's become known; f_t = -S_t / (2t).  All lanes return f_n.
-__device__ __forceinline__ double series_q(const double *q, int m, int n, int lane)
+// [lambda^n] det(I - lambda H)^(-1/2) from q_1..q_min(m,n), push-style: the lane of coefficient t
+// accumulates S_t = sum_j (2t-j) q_j f_{t-j} as the f's become known; f_t = -S_t / (2t).  In a
+// group of G lanes, lane l holds t = l + G c for c < 32 / G (n <= 31).  All lanes return f_n.
+template <int G>
+__device__ __forceinline__ double series_q(const double *q, int m, int n, int lane, unsigned gm)
 {
-    double S = 0.0, fs = 1.0;
+    constexpr int NC = 32 / G;
+    double S[NC], fs = 1.0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) S[c] = 0.0;
     for (int s = 0; s < n; ++s) {
-        const int j = lane - s;
-        if (j >= 1 && j <= m && lane <= n) S = fma((double)(lane + s) * q[j], fs, S);
-        fs = __shfl_sync(FULL, S, s + 1) * c_neg_inv_2t[s + 1];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int t = lane + G * c, j = t - s;
+            if (j >= 1 && j <= m && t <= n) S[c] = fma((double)(t + s) * q[j], fs, S[c]);
+        }
+        const int t1 = s + 1;
+        const double own = (NC > 1 && t1 >= G) ? S[NC - 1] : S[0];
+        fs = __shfl_sync(gm, own, t1 & (G - 1), G) * c_neg_inv_2t[t1];
     }
     return fs;
 }
 
-__device__ __forceinline__ cd series_q_c(const cd *q, int m, int n, int lane)
+template <int G>
+__device__ __forceinline__ cd series_q_c(const cd *q, int m, int n, int lane, unsigned gm)
 {
-    double Sr = 0.0, Si = 0.0, fr = 1.0, fi = 0.0;
+    constexpr int NC = 32 / G;
+    double Sr[NC], Si[NC], fr = 1.0, fi = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        Sr[c] = 0.0;
+        Si[c] = 0.0;
+    }
     for (int s = 0; s < n; ++s) {
-        const int j = lane - s;
-        if (j >= 1 && j <= m && lane <= n) {
-            const double w = (double)(lane + s);
-            const cd qj = q[j];
-            const double ar = w * qj.re, ai = w * qj.im;
-            Sr = fma(ar, fr, fma(-ai, fi, Sr));
-            Si = fma(ar, fi, fma(ai, fr, Si));
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int t = lane + G * c, j = t - s;
+            if (j >= 1 && j <= m && t <= n) {
+                const double w = (double)(t + s);
+                const cd qj = q[j];
+                const double ar = w * qj.re, ai = w * qj.im;
+                Sr[c] = fma(ar, fr, fma(-ai, fi, Sr[c]));
+                Si[c] = fma(ar, fi, fma(ai, fr, Si[c]));
+            }
         }
-        const double c = c_neg_inv_2t[s + 1];
-        fr = __shfl_sync(FULL, Sr, s + 1) * c;
-        fi = __shfl_sync(FULL, Si, s + 1) * c;
+        const int t1 = s + 1;
+        const double c1 = c_neg_inv_2t[t1];
+        const double ownr = (NC > 1 && t1 >= G) ? Sr[NC - 1] : Sr[0];
+        const double owni = (NC > 1 && t1 >= G) ? Si[NC - 1] : Si[0];
+        fr = __shfl_sync(gm, ownr, t1 & (G - 1), G) * c1;
+        fi = __shfl_sync(gm, owni, t1 & (G - 1), G) * c1;
     }
     return cd{fr, fi};
 }
 
 // ---- one real term, m <= 32 * RPL, register tile of MW columns ----------------------------------
-template <int MW, int RPL>
+template <int MW, int RPL, int G>
 __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int lda, int E, int mE, int n,
-                                            const FastWs &ws, int lane)
+                                            const FastWs &ws, int lane, unsigned gm)
 {
+    static_assert(G == 32 || (G == 16 && RPL == 1 && MW <= 16), "a group of 16 lanes holds up to 16 rows");
     const int m = 2 * mE;
     double *prow = ws.prow, *wv = ws.wv;
     double R[RPL][MW];
@@ -334,13 +358,13 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
                 const unsigned k2 = pivot_key(fabs(pc[q]), lane + 32 * q);
                 key = k2 > key ? k2 : key;
             }
-        const unsigned best = __reduce_max_sync(FULL, key);
+        const unsigned best = __reduce_max_sync(gm, key);
         const int pslot = 63 - (int)(best & 63u);
         const int plane = pslot & 31, pq = pslot >> 5;
         const double pcp = (RPL > 1 && pq == 1) ? pc[RPL - 1] : pc[0];
         const int labp = (RPL > 1 && pq == 1) ? lab[RPL - 1] : lab[0];
-        const double x = __shfl_sync(FULL, pcp, plane);
-        const int plab = __shfl_sync(FULL, labp, plane);
+        const double x = __shfl_sync(gm, pcp, plane, G);
+        const int plab = __shfl_sync(gm, labp, plane, G);
         // -- column s-1 is final for rows with label <= s-1 plus the pivot: store La Budde's order
         //    k = s coefficients for labudde_diag, which runs once the reduction is done
 #pragma unroll
@@ -367,7 +391,7 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
                     if (j == pslot) v = R[q][j];
                 pc[q] = v;
             }
-            __syncwarp();
+            __syncwarp(gm);
             continue;
         }
         const double rx = recip(x);
@@ -385,7 +409,7 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
             const int r = lane + 32 * q;
             if (r < MW) wv[r] = r == pslot ? 1.0 : mult[q];
         }
-        __syncwarp();
+        __syncwarp(gm);
         // -- row update: M[i, :] -= mult_i * M[piv, :]
 #pragma unroll
         for (int j = 0; j < MW; j += 2) {
@@ -413,7 +437,7 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
             }
             pc[q] = (a0 + a1) + (a2 + a3);
         }
-        __syncwarp();
+        __syncwarp(gm);
     }
     // Last two columns: m-2 is `pc`, m-1 is the physical slot carrying label m-1.  Feed La Budde
     // steps k = m-1 and k = m (for m == 2 the loop above did not run and k = 1, 2 remain).
@@ -423,7 +447,7 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
 #pragma unroll
         for (int q = 0; q < RPL; ++q)
             if (lab[q] == m - 1) mine = lane + 32 * q;
-        lastslot = (int)__reduce_max_sync(FULL, (unsigned)(mine + 1)) - 1;
+        lastslot = (int)__reduce_max_sync(gm, (unsigned)(mine + 1)) - 1;
     }
     double colm1[RPL];
 #pragma unroll
@@ -441,7 +465,7 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
         double sub = xprev;
         if (last && k >= 2) {
             const double cand = (RPL > 1 && (lastslot >> 5) == 1) ? pc[RPL - 1] : pc[0];
-            sub = __shfl_sync(FULL, cand, lastslot & 31);
+            sub = __shfl_sync(gm, cand, lastslot & 31, G);
         }
 #pragma unroll
         for (int q = 0; q < RPL; ++q) {
@@ -454,18 +478,19 @@ __device__ __forceinline__ double term_real(const double *__restrict__ Ax, int l
             if (lab[q] == k - 1) ws.hk[k] = colv;
         }
     }
-    __syncwarp();
-    if constexpr (RPL == 1) labudde_diag<MW>(ws.cft, ws.hk, ws.q, m, n, lane);
+    __syncwarp(gm);
+    if constexpr (RPL == 1) labudde_diag<MW, G>(ws.cft, ws.hk, ws.q, m, n, lane, gm);
     else labudde_diag2<MW>(ws.cft, ws.hk, ws.q, m, n, lane);
-    __syncwarp();
-    return series_q(ws.q, m, n, lane);
+    __syncwarp(gm);
+    return series_q<G>(ws.q, m, n, lane, gm);
 }
 
 // ---- one complex term, m <= 32 --------------------------------------------------------------------
-template <int MW>
+template <int MW, int G>
 __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int E, int mE, int n, const FastWs &ws,
-                                        int lane)
+                                        int lane, unsigned gm)
 {
+    static_assert(G == 32 || (G == 16 && MW <= 16), "a group of 16 lanes holds up to 16 rows");
     const int m = 2 * mE;
     double Rr[MW], Ri[MW];
     int lab = lane;
@@ -505,10 +530,10 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
     for (int s = 1; s <= m - 2; ++s) {
         unsigned key = 0;
         if (lab >= s && lab < m) key = pivot_key(fma(pcr, pcr, pci * pci), lane);
-        const unsigned best = __reduce_max_sync(FULL, key);
+        const unsigned best = __reduce_max_sync(gm, key);
         const int plane = 63 - (int)(best & 63u);
-        const double xr = __shfl_sync(FULL, pcr, plane), xi = __shfl_sync(FULL, pci, plane);
-        const int plab = __shfl_sync(FULL, lab, plane);
+        const double xr = __shfl_sync(gm, pcr, plane, G), xi = __shfl_sync(gm, pci, plane, G);
+        const int plab = __shfl_sync(gm, lab, plane, G);
         feed(s, pcr, pci, xprev);
         if (lab == s) lab = plab;
         else if (lab == plab) lab = s;
@@ -543,7 +568,7 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
             wvr[lane] = lane == plane ? 1.0 : mr;
             wvi[lane] = lane == plane ? 0.0 : mi;
         }
-        __syncwarp();
+        __syncwarp(gm);
 #pragma unroll
         for (int j = 0; j < MW; j += 2) {
             const double2 ar = *reinterpret_cast<const double2 *>(prr + j);
@@ -565,9 +590,9 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
         }
         pcr = sr0 + sr1;
         pci = si0 + si1;
-        __syncwarp();
+        __syncwarp(gm);
     }
-    const int lastslot = (int)__reduce_max_sync(FULL, lab == m - 1 ? (unsigned)(lane + 1) : 0u) - 1;
+    const int lastslot = (int)__reduce_max_sync(gm, lab == m - 1 ? (unsigned)(lane + 1) : 0u) - 1;
     double cr = 0.0, ci = 0.0;
 #pragma unroll
     for (int j = 0; j < MW; ++j)
@@ -577,14 +602,14 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
         }
     for (int k = (m >= 3 ? m - 1 : 1); k <= m; ++k) {
         cd sub = xprev;
-        if (k == m && k >= 2) sub = cd{__shfl_sync(FULL, pcr, lastslot), __shfl_sync(FULL, pci, lastslot)};
+        if (k == m && k >= 2) sub = cd{__shfl_sync(gm, pcr, lastslot, G), __shfl_sync(gm, pci, lastslot, G)};
         if (k == m) feed(k, cr, ci, sub);
         else feed(k, pcr, pci, sub);
     }
-    __syncwarp();
-    labudde_diag_c<MW>(cft, hk, (cd *)ws.q, m, n, lane);
-    __syncwarp();
-    return series_q_c((const cd *)ws.q, m, n, lane);
+    __syncwarp(gm);
+    labudde_diag_c<MW, G>(cft, hk, (cd *)ws.q, m, n, lane, gm);
+    __syncwarp(gm);
+    return series_q_c<G>((const cd *)ws.q, m, n, lane, gm);
 }
 
 static int upload_fast_tables(cudaStream_t st);

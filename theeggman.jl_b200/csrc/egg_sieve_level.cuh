@@ -21,135 +21,182 @@ namespace egg {
 
 // 128-thread blocks; resident blocks per SM from the tile's register need (65536 / (128 * blocks)
 // registers per thread): a real tile holds m doubles per row, a complex one 2m.
-template <bool CPLX, int K>
+template <bool CPLX, int K, int G = 32>
 struct LevelShape {
     static constexpr int MW = 2 * K;
     static constexpr int threads = 128;
-    static constexpr int min_blocks =
+    static constexpr int full =
         CPLX ? (MW <= 8 ? 6 : (MW <= 10 ? 5 : (MW <= 16 ? 4 : (MW <= 24 ? 3 : 2))))
              : (MW <= 8 ? 8 : (MW <= 12 ? 7 : (MW <= 18 ? 6 : (MW <= 26 ? 5 : (MW <= 32 ? 4 : 2)))));
+    // Two terms per warp need more registers per thread (the series holds two coefficients per
+    // lane); one block fewer still keeps more terms in flight.
+    static constexpr int min_blocks = G == 32 ? full : (full > 2 ? full - 1 : 1);
 };
 
-template <bool CPLX, int K>
-__global__ void __launch_bounds__(LevelShape<CPLX, K>::threads, LevelShape<CPLX, K>::min_blocks)
+// Lanes per term: tiles of up to 16 rows (m <= 16) run two terms per warp, one per half-warp group
+// of 16 lanes, so that the lanes beyond m are not left idle.  Every shuffle, vote, reduction and
+// warp barrier of a term names only its group's lanes.
+template <int K>
+constexpr int level_group(bool narrow)
+{
+    return (narrow && 2 * K <= 16) ? 16 : 32;
+}
+
+template <bool CPLX, int K, int G>
+__global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CPLX, K, G>::min_blocks)
     sieve_level_kernel(SieveArgs a, const int64_t *__restrict__ strides, dd *partial)
 {
     constexpr int MW = 2 * K;
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
+    constexpr int NG = 32 / G;   // groups per warp
+    constexpr int GB = cw * NG;  // groups per block
     extern __shared__ double smem[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int grp = threadIdx.x / G, gl = threadIdx.x & (G - 1);
+    const int gbase = (threadIdx.x & 31) & ~(G - 1);  // the group's first lane within its warp
+    const unsigned gm = G == 32 ? FULL : (0xFFFFu << gbase);
     const int b = blockIdx.y;
     const SieveInst in = a.inst[b];
     const int E = in.E, n = in.n;
-    const FastWs w = fast_carve(smem + (size_t)wib * fast_ws_doubles(a.nmax, CPLX, MW), a.nmax, CPLX, MW);
-    const int wslot = blockIdx.x * cw + wib;
-    const uint64_t W = (uint64_t)a.warps_per_inst;
+    const FastWs w = fast_carve(smem + (size_t)grp * fast_ws_doubles(a.nmax, CPLX, MW), a.nmax, CPLX, MW);
+    const int gslot = blockIdx.x * GB + grp;
+    const uint64_t W = (uint64_t)a.warps_per_inst * NG;  // groups per instance
     dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
     // One term: the surviving edges are compacted into w.eidx / w.kval (K of them) by the caller.
     auto eval_term = [&](double prefac) {
         if constexpr (!CPLX) {
-            const double val = term_real<MW, (MW > 32 ? 2 : 1)>((const double *)a.Ax + in.ax_off, in.lda, E, K, n, w,
-                                                                lane);
-            if (lane == 0) dd_add(acc_re, prefac * val);
+            const double val = term_real<MW, (MW > 32 ? 2 : 1), G>((const double *)a.Ax + in.ax_off, in.lda, E, K, n, w,
+                                                                   gl, gm);
+            if (gl == 0) dd_add(acc_re, prefac * val);
         } else {
-            const cd val = term_cplx<MW>((const cd *)a.Ax + in.ax_off, in.lda, E, K, n, w, lane);
-            if (lane == 0) {
+            const cd val = term_cplx<MW, G>((const cd *)a.Ax + in.ax_off, in.lda, E, K, n, w, gl, gm);
+            if (gl == 0) {
                 dd_add(acc_re, prefac * val.re);
                 dd_add(acc_im, prefac * val.im);
             }
         }
     };
+    // The group's lanes of a warp vote, as bits 0..G-1.
+    auto group_ballot = [&](bool p) -> unsigned {
+        const unsigned v = __ballot_sync(gm, p);
+        return G == 32 ? v : (v >> gbase) & 0xFFFFu;
+    };
+    // Each round every group first finds its next term, then the warp evaluates them together (the
+    // groups of a warp stay converged through the term), until no group of the warp has one left.
     if (in.subset && K <= E) {
         const uint64_t cnt = c_binom[E * 33 + K];
-        const uint64_t lo = (uint64_t)wslot * cnt / W, hi = ((uint64_t)wslot + 1) * cnt / W;
+        const uint64_t lo = (uint64_t)gslot * cnt / W, hi = ((uint64_t)gslot + 1) * cnt / W;
         const double prefac = ((n - K) & 1) ? -1.0 : 1.0;  // (-1)^(n - k), every binomial factor 1
         uint32_t S = lo < hi ? subset_unrank(E, K, (uint32_t)lo) : 0u;
-        for (uint64_t rk = lo; rk < hi; ++rk) {
-            if (rk > lo) S = subset_next(S);
-            if (lane < E && ((S >> lane) & 1u)) {
-                const int pos = __popc(S & ((1u << lane) - 1u));
-                w.eidx[pos] = lane;
-                w.kval[pos] = 1.0;
+        for (uint64_t rk = lo;; ++rk) {
+            const bool has = rk < hi;
+            if (!__any_sync(FULL, has)) break;
+            if (has) {
+                if (rk > lo) S = subset_next(S);
+                for (int e = gl; e < E; e += G)
+                    if ((S >> e) & 1u) {
+                        const int pos = __popc(S & ((1u << e) - 1u));
+                        w.eidx[pos] = e;
+                        w.kval[pos] = 1.0;
+                    }
+                __syncwarp(gm);
+                eval_term(prefac);
+                __syncwarp(gm);
             }
-            __syncwarp();
-            eval_term(prefac);
-            __syncwarp();
         }
     } else if (K <= E) {
-        // Mixed-radix odometer (src/hafnian.jl:542-580): lane i holds digit i (edge E-1 least
-        // significant), digit 0 clipped to its lower half under Glynn.  Runs of kRunTerms
-        // consecutive indices are dealt round robin: a term's size is set by its digits, and a long
-        // contiguous range fixes the high digits, so contiguous ranges would hand some warps most of
-        // a level and others none of it.
+        // Mixed-radix odometer (src/hafnian.jl:542-580): lane i of the group holds digit i (edge
+        // E-1 least significant; E <= G here), digit 0 clipped to its lower half under Glynn.  Runs
+        // of kRunTerms consecutive indices are dealt round robin: a term's size is set by its
+        // digits, and a long contiguous range fixes the high digits, so contiguous ranges would hand
+        // some groups most of a level and others none of it.
         const int *reps = a.reps + in.reps_off;
         const int mr1 = a.maxrep + 1;
         const bool unit = a.maxrep <= 1;  // all multiplicities <= 1: every binomial factor is 1
         int r = 0, base = 1, digit = 0;
-        if (lane < E) {
-            r = reps[lane];
-            base = (in.glynn && lane == 0) ? (r + 2) / 2 : r + 1;
+        if (gl < E) {
+            r = reps[gl];
+            base = (in.glynn && gl == 0) ? (r + 2) / 2 : r + 1;
         }
         constexpr int64_t kRunTerms = 16;
-        for (int64_t j0 = (int64_t)wslot * kRunTerms; j0 < in.steps; j0 += (int64_t)W * kRunTerms) {
-            const int64_t j1 = j0 + kRunTerms < in.steps ? j0 + kRunTerms : in.steps;
-            if (lane < E) digit = (int)((j0 / strides[in.reps_off + lane]) % base);
-            for (int64_t j = j0; j < j1; ++j) {
-                if (j > j0) {
-                    const unsigned notmax = __ballot_sync(FULL, lane < E && digit != base - 1);
+        int64_t j0 = (int64_t)gslot * kRunTerms;
+        int64_t j = j0, j1 = j0 < in.steps ? (j0 + kRunTerms < in.steps ? j0 + kRunTerms : in.steps) : j0;
+        if (gl < E && j0 < in.steps) digit = (int)((j0 / strides[in.reps_off + gl]) % base);
+        for (;;) {
+            bool has = false;
+            double prefac = 0.0;
+            while (j < j1) {
+                const int kk = gl < E ? (in.glynn ? 2 * digit - r : digit) : 0;
+                const bool nz = gl < E && kk != 0;
+                const unsigned mask = group_ballot(nz);
+                const bool hit = __popc(mask) == K;
+                if (hit) {
+                    const int esum = __reduce_add_sync(gm, gl < E ? digit : 0);
+                    double bp = 1.0;
+                    if (!unit) {
+                        bp = gl < E ? a.binoms[r + digit * mr1] : 1.0;
+                        for (int off = G / 2; off > 0; off >>= 1) bp *= __shfl_xor_sync(gm, bp, off, G);
+                    }
+                    prefac = ((n - esum) & 1) ? -bp : bp;
+                    const int k0 = __shfl_sync(gm, kk, 0, G);
+                    if (in.glynn && k0 == 0) prefac *= 0.5;  // the mirror's fixed point (:570-573)
+                    if (nz) {
+                        const int pos = __popc(mask & ((1u << gl) - 1u));
+                        w.eidx[pos] = gl;
+                        w.kval[pos] = (double)kk;
+                    }
+                    has = true;
+                }
+                // Move to index j + 1: the next odometer value, or the start of the group's next run.
+                ++j;
+                if (j < j1) {
+                    const unsigned notmax = group_ballot(gl < E && digit != base - 1);
                     const int h = 31 - __clz(notmax);
-                    if (lane == h) ++digit;
-                    else if (lane > h && lane < E) digit = 0;
+                    if (gl == h) ++digit;
+                    else if (gl > h && gl < E) digit = 0;
+                } else {
+                    j0 += (int64_t)W * kRunTerms;
+                    if (j0 < in.steps) {
+                        j = j0;
+                        j1 = j0 + kRunTerms < in.steps ? j0 + kRunTerms : in.steps;
+                        if (gl < E) digit = (int)((j0 / strides[in.reps_off + gl]) % base);
+                    }
                 }
-                const int kk = lane < E ? (in.glynn ? 2 * digit - r : digit) : 0;
-                const bool nz = lane < E && kk != 0;
-                const unsigned mask = __ballot_sync(FULL, nz);
-                if (__popc(mask) != K) continue;  // another level
-                const int esum = __reduce_add_sync(FULL, lane < E ? digit : 0);
-                double bp = 1.0;
-                if (!unit) {
-                    bp = lane < E ? a.binoms[r + digit * mr1] : 1.0;
-                    for (int off = 16; off > 0; off >>= 1) bp *= __shfl_xor_sync(FULL, bp, off);
-                }
-                double prefac = ((n - esum) & 1) ? -bp : bp;
-                const int k0 = __shfl_sync(FULL, kk, 0);
-                if (in.glynn && k0 == 0) prefac *= 0.5;  // the mirror's fixed point (:570-573)
-                if (nz) {
-                    const int pos = __popc(mask & ((1u << lane) - 1u));
-                    w.eidx[pos] = lane;
-                    w.kval[pos] = (double)kk;
-                }
-                __syncwarp();
+                if (hit) break;
+            }
+            if (!__any_sync(FULL, has)) break;
+            if (has) {
+                __syncwarp(gm);
                 eval_term(prefac);
-                __syncwarp();
+                __syncwarp(gm);
             }
         }
     }
-    // The block's warps summed in a fixed order: one partial per block.
-    __shared__ dd red[2 * cw];
-    if (lane == 0) {
-        red[2 * wib] = acc_re;
-        red[2 * wib + 1] = acc_im;
+    // The block's groups summed in a fixed order: one partial per block.
+    __shared__ dd red[2 * GB];
+    if (gl == 0) {
+        red[2 * grp] = acc_re;
+        red[2 * grp + 1] = acc_im;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        dd r = red[0], i = red[1];
+        dd re = red[0], im = red[1];
 #pragma unroll
-        for (int q = 1; q < cw; ++q) {
-            dd_add(r, red[2 * q]);
-            dd_add(i, red[2 * q + 1]);
+        for (int q = 1; q < GB; ++q) {
+            dd_add(re, red[2 * q]);
+            dd_add(im, red[2 * q + 1]);
         }
         dd *out = partial + ((size_t)b * gridDim.x + blockIdx.x) * 2;
-        out[0] = r;
-        out[1] = i;
+        out[0] = re;
+        out[1] = im;
     }
 }
 
-template <bool CPLX, int K>
+template <bool CPLX, int K, int G>
 static int level_launch_k(const SieveArgs &a, const int64_t *strides, int B, dd *partial, int blocks_x, cudaStream_t st)
 {
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
-    const size_t smem = (size_t)cw * fast_ws_doubles(a.nmax, CPLX, 2 * K) * sizeof(double);
-    auto k = sieve_level_kernel<CPLX, K>;
+    const size_t smem = (size_t)cw * (32 / G) * fast_ws_doubles(a.nmax, CPLX, 2 * K) * sizeof(double);
+    auto k = sieve_level_kernel<CPLX, K, G>;
     int rc = smem_limit_at_least((const void *)k, smem);
     if (rc) return rc;
     k<<<dim3((unsigned)blocks_x, (unsigned)B), cw * 32, smem, st>>>(a, strides, partial);
@@ -158,12 +205,12 @@ static int level_launch_k(const SieveArgs &a, const int64_t *strides, int B, dd 
     return EGG_OK;
 }
 
-template <bool CPLX, int K>
+template <bool CPLX, int K, int G>
 static int level_shape_k(int nmax, int *warps_per_block, int *blocks_per_sm)
 {
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
-    const size_t smem = (size_t)cw * fast_ws_doubles(nmax, CPLX, 2 * K) * sizeof(double);
-    auto k = sieve_level_kernel<CPLX, K>;
+    const size_t smem = (size_t)cw * (32 / G) * fast_ws_doubles(nmax, CPLX, 2 * K) * sizeof(double);
+    auto k = sieve_level_kernel<CPLX, K, G>;
     int nb = 0;
     int rc = smem_limit_at_least((const void *)k, smem);
     if (!rc) rc = egg::blocks_per_sm((const void *)k, cw * 32, smem, &nb);

@@ -5,12 +5,19 @@
 
 namespace egg {
 
-#define EGG_LVL_LAUNCH(CPLX, K) \
-    case K: return level_launch_k<CPLX, K>(a, strides, B, partial, blocks_x, st);
-#define EGG_LVL_SHAPE(CPLX, K) \
-    case K: rc = level_shape_k<CPLX, K>(nmax, warps_per_block, blocks_per_sm); break;
+// Level K with groups of 16 lanes when `narrow` and the tile allows it, else whole warps.
+#define EGG_LVL_LAUNCH(CPLX, K)                                                                     \
+    case K:                                                                                          \
+        return narrow ? level_launch_k<CPLX, K, level_group<K>(true)>(a, strides, B, partial, blocks_x, st) \
+                      : level_launch_k<CPLX, K, 32>(a, strides, B, partial, blocks_x, st);
+#define EGG_LVL_SHAPE(CPLX, K)                                                                       \
+    case K:                                                                                          \
+        rc = narrow ? level_shape_k<CPLX, K, level_group<K>(true)>(nmax, warps_per_block, blocks_per_sm) \
+                    : level_shape_k<CPLX, K, 32>(nmax, warps_per_block, blocks_per_sm);              \
+        break;
 
-int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int k, dd *partial, int blocks_x, cudaStream_t st)
+int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
+                         cudaStream_t st)
 {
     int rc = upload_fast_tables_once(st);
     if (rc) return rc;
@@ -20,14 +27,15 @@ int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int 
     return fail(EGG_ERR_ARGUMENT, "no such sieve level");
 }
 
-int level_shape_real_hi(int nmax, int k, int *warps_per_block, int *blocks_per_sm)
+int level_shape_real_hi(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm)
 {
     static std::mutex mu;  // the entry point that allocates nothing reaches this without the library's lock
     std::lock_guard<std::mutex> lk(mu);
-    static int cache[kLevelMaxReal + 1][2];
-    if (k >= 1 && k <= kLevelMaxReal && cache[k][1] > 0) {
-        *warps_per_block = cache[k][0];
-        *blocks_per_sm = cache[k][1];
+    static int cache[kLevelMaxReal + 1][2][2];
+    int *slot = (k >= 1 && k <= kLevelMaxReal) ? cache[k][narrow ? 1 : 0] : nullptr;
+    if (slot && slot[1] > 0) {
+        *warps_per_block = slot[0];
+        *blocks_per_sm = slot[1];
         return EGG_OK;
     }
     int rc = fail(EGG_ERR_ARGUMENT, "no such sieve level");
@@ -35,8 +43,10 @@ int level_shape_real_hi(int nmax, int k, int *warps_per_block, int *blocks_per_s
         EGG_LEVEL_CASES_HI(false, EGG_LVL_SHAPE)
     }
     if (rc) return rc;
-    cache[k][0] = *warps_per_block;
-    cache[k][1] = *blocks_per_sm;
+    if (slot) {
+        slot[0] = *warps_per_block;
+        slot[1] = *blocks_per_sm;
+    }
     return EGG_OK;
 }
 
