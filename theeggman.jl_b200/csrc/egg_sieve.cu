@@ -8,9 +8,13 @@
 // (:618-622), each warp keeps a double-double accumulator; the per-warp partials are then summed
 // in a fixed tree, so results do not depend on scheduling.
 //
-// Work layout.  Instance b's terms j = 0..steps-1 are dealt round-robin to that instance's warps
-// (grid.y = instance).  The mixed-radix odometer (edge E least significant, the leading digit
-// clipped to its lower half under Glynn, :655-657) is decoded per term.
+// Work layout of this exact kernel.  Instance b's terms are dealt to that instance's warps
+// (grid.y = instance): round robin over j = 0..steps-1, decoding the mixed-radix odometer per term
+// (edge E least significant, the leading digit clipped to its lower half under Glynn, :655-657),
+// or, for distinct-row inclusion-exclusion, as equal shares of each popcount level.  The fast
+// register-tile kernels (egg_sieve_fast.cuh, egg_sieve_level*.cu) take every term that fits their
+// tiles unless the exact mode is asked for; this driver launches both and the fixed-order
+// reduction.
 #include <cstring>
 
 #include "egg_sieve.cuh"
@@ -655,10 +659,11 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     } else if (run_ex) {
         ex_bx = per_inst_blocks(ex_wpb);
     }
-    // The fast launches: one per popcount level with terms, each one wave of its resident blocks
-    // across the machine, shared among the instances (every warp gets the same share of the level's
-    // terms, so a second, partial wave would leave most of the machine idle while it ran).  A level
-    // whose terms number at most two per resident warp is latency-bound: it runs on the side
+    // The fast launches: one per popcount level with terms.  A level of distinct-row instances runs
+    // as one wave of its resident blocks across the machine, shared among the instances (every
+    // group of lanes gets the same share of the level's terms, so a second, partial wave would
+    // leave most of the machine idle while it ran); odometer levels get about four waves.  A level
+    // whose terms number at most two per resident term slot is latency-bound: it runs on a side
     // stream, overlapping the main stream's launches, as does the exact kernel when it only takes
     // the terms too large for the tiles.
     struct FastLaunch {

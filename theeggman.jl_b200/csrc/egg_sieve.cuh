@@ -19,7 +19,7 @@ struct SieveArgs {
     const double *binoms;  // (maxrep+1) x (maxrep+1), binoms[a + b*(maxrep+1)] = C(a, b)
     const uint32_t *binom32;  // C(x, k) at [x * 65 + k], exact for x <= 32
     const SieveInst *inst;
-    dd *partial;           // [B][warps_per_inst][2]
+    dd *partial;           // exact kernel: [B][warps_per_inst][2]
     double *terms;         // if set (one instance, exact kernel only): term j's value at j (complex: 2j, 2j+1)
     int maxrep, warps_per_inst, Emax, nmax;
     int skip_le;           // the exact kernel leaves terms with m <= skip_le to the fast kernels
