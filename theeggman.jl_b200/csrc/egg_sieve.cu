@@ -530,13 +530,6 @@ __global__ void __launch_bounds__(kReduceThreads) sieve_reduce_kernel(PartialSet
 
 // ---- host side ---------------------------------------------------------------------------------
 
-static uint64_t binom_u64(int64_t n, int64_t k)
-{
-    uint64_t r = 1;
-    for (int64_t i = 1; i <= k; ++i) r = r * (uint64_t)(n - k + i) / (uint64_t)i;  // exact at each step
-    return r;
-}
-
 static int64_t maxrep_of(const int64_t *reps, int64_t E)
 {
     int64_t m = 0;
@@ -692,7 +685,9 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         }
         // Tiles of up to 16 rows take two terms per warp when every odometer instance has at most 16
         // edges (one lane per digit); distinct-row instances need no digits.
-        int64_t e_odo = 0;
+        int64_t e_odo = 0, tot_steps = 0;
+        for (const SieveInst &si : inst) tot_steps += si.steps;
+        const int64_t avg_steps = B > 0 ? tot_steps / B : 0;
         for (const SieveInst &si : inst) e_odo = (!si.subset && si.E > e_odo) ? si.E : e_odo;
         for (int k = 1; k <= kmax; ++k) {
             if (lvl[(size_t)k] <= 0.0) continue;
@@ -703,9 +698,11 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             if (bps < 1 || (size_t)cw * (narrow ? 2 : 1) * fast_ws_bytes(nmax, cplx, 2 * k) > 220 * 1024)
                 return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
             // Distinct-row levels deal equal shares: one wave.  Odometer runs are only balanced on
-            // average and instances differ in size, so those levels get about four waves of blocks
-            // for the block scheduler to even out.
-            const int64_t waves = all_subset ? 1 : 4;
+            // average and instances differ in size, so those levels get several waves of blocks for
+            // the block scheduler to even out: four for long odometers, two for short ones (a
+            // batch of 1,458-term instances ran 6 % faster on two, one of 90 k-term instances 23 %
+            // faster on four), where each block's fixed costs weigh more.
+            const int64_t waves = all_subset ? 1 : (avg_steps >= 16384 ? 4 : 2);
             int64_t per = ((int64_t)num_sms * bps * waves + B - 1) / B;
             const int64_t cap = (maxsteps + cw - 1) / cw;  // no more warps than terms
             if (per > cap) per = cap;
