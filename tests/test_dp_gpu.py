@@ -208,6 +208,20 @@ def test_level_kernel_batches(egg, nat, orc, W, K, B):
         assert got[b] == orc.haf_dp_pairs(np.ascontiguousarray(P[b]), plan, orc.F64), b
 
 
+def test_small_call_graph_replay(egg, orc, W):
+    """Small single-instance calls run eagerly once, are recorded into a graph the second time and
+    replayed after that: every call must still read its own matrix and match the reference's DP
+    bit for bit, in several element types, and again after the cache (and its graphs) is cleared."""
+    for N in (12, 20):
+        for rep in range(2):
+            for i in range(5):
+                A = W.dense_real(N, 9000 + 10 * N + i)
+                assert egg.hafnian(A, method="dp") == orc.haf_dp(A), (N, i)
+                C = W.dense_complex(N, 9100 + 10 * N + i, 0.5)
+                assert complex(egg.hafnian(C, method="dp")) == complex(orc.haf_dp(C)), (N, i)
+            egg.empty_gpu_cache()
+
+
 def test_cache_accounting(egg, nat, W):
     # test/gpu.jl:96-108
     egg.empty_gpu_cache()
