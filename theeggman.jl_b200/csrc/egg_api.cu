@@ -57,41 +57,6 @@ int create_streams(Context &c, int device)
     return EGG_OK;
 }
 
-// Small host calls of egg_dp_batch (one or a few instances): the copy in from the page-locked
-// buffer, the DP and the copy out run eagerly the first time a shape is seen, are recorded into a
-// graph the second time and replayed after that, which takes one runtime call instead of several.
-// The key names every buffer the graph touches; callers hold the library's lock.
-struct SmallDpGraph {
-    const DevPlan *plan;
-    int dtype, prec;
-    int64_t B;
-    std::vector<const void *> ptrs;
-    int seen;
-    cudaGraphExec_t exec;
-    long long nodes;
-};
-static std::vector<SmallDpGraph> g_small_graphs;
-static constexpr size_t kMaxSmallGraphs = 16;
-
-void small_dp_graphs_clear()
-{
-    for (SmallDpGraph &g : g_small_graphs)
-        if (g.exec) cudaGraphExecDestroy(g.exec);
-    g_small_graphs.clear();
-}
-
-static SmallDpGraph &small_dp_graph(const DevPlan *plan, int dtype, int prec, int64_t B, const std::vector<const void *> &ptrs)
-{
-    for (SmallDpGraph &g : g_small_graphs)
-        if (g.plan == plan && g.dtype == dtype && g.prec == prec && g.B == B && g.ptrs == ptrs) return g;
-    if (g_small_graphs.size() >= kMaxSmallGraphs) {
-        if (g_small_graphs.front().exec) cudaGraphExecDestroy(g_small_graphs.front().exec);
-        g_small_graphs.erase(g_small_graphs.begin());
-    }
-    g_small_graphs.push_back(SmallDpGraph{plan, dtype, prec, B, ptrs, 0, nullptr, 0});
-    return g_small_graphs.back();
-}
-
 int smem_limit_at_least(const void *k, size_t bytes)
 {
     // Own lock: the entry point that allocates nothing reaches this without the library's lock.
@@ -262,7 +227,6 @@ int egg_cache_clear(void)
     Context &c = ctx();
     if (c.device >= 0) cudaStreamSynchronize(c.stream);
     mix_graphs_clear();
-    small_dp_graphs_clear();
     for (auto &kv : c.plans)
         if (kv.second.trans) cudaFree(kv.second.trans);
     c.plans.clear();
@@ -480,48 +444,13 @@ int egg_dp_batch(int K, int idx_bytes, int dtype, int prec, const void *P, int64
         // A small call: both transfers through the page-locked staging buffer.
         if (!c.pinned) EGG_CUDA_TRY(cudaHostAlloc(&c.pinned, Context::kPinnedBytes, cudaHostAllocDefault));
         char *pin_in = (char *)c.pinned, *pin_out = pin_in + ((in_bytes + 255) / 256) * 256;
-        if (in_bytes) std::memcpy(pin_in, P, in_bytes);
-        if (!binom32_device(c.stream, &rc)) return rc;  // uploaded before any recording
-        std::vector<const void *> ptrs;
-        for (const DevBuf &b : c.scratch) ptrs.push_back(b.ptr);
-        SmallDpGraph &g = small_dp_graph(plan, dtype, prec, B, ptrs);
-        if (g.exec) {
-            EGG_CUDA_TRY(cudaGraphLaunch(g.exec, c.stream));
-            count_launch(g.nodes);
-        } else {
-            const bool record = g.seen >= 1;
-            ++g.seen;
-            const long long launches0 = g_launches.load();
-            if (record) EGG_CUDA_TRY(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
-            cudaError_t ce = in_bytes ? cudaMemcpyAsync(c.scratch[1].ptr, pin_in, in_bytes, cudaMemcpyHostToDevice, c.stream)
-                                      : cudaSuccess;
-            rc = ce == cudaSuccess ? dp_run(*plan, dtype, prec, c.scratch[1].ptr, B, c.scratch[2].ptr, c.stream)
-                                   : fail(EGG_ERR_CUDA, std::string("copy in: ") + cudaGetErrorString(ce));
-            if (!rc) {
-                ce = cudaMemcpyAsync(pin_out, c.scratch[2].ptr, out_bytes, cudaMemcpyDeviceToHost, c.stream);
-                if (ce != cudaSuccess) rc = fail(EGG_ERR_CUDA, std::string("copy out: ") + cudaGetErrorString(ce));
-            }
-            if (record) {
-                cudaGraph_t graph = nullptr;
-                const cudaError_t e = cudaStreamEndCapture(c.stream, &graph);
-                if (rc || e != cudaSuccess) {
-                    if (graph) cudaGraphDestroy(graph);
-                    cudaGetLastError();
-                    return rc ? rc : fail(EGG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-                }
-                cudaGraphExec_t exec = nullptr;
-                const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
-                cudaGraphDestroy(graph);
-                if (ei != cudaSuccess) return fail(EGG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
-                g.exec = exec;
-                g.nodes = g_launches.load() - launches0;
-                g_launches.fetch_sub(g.nodes);  // counted when the graph runs, not when it is recorded
-                EGG_CUDA_TRY(cudaGraphLaunch(exec, c.stream));
-                count_launch(g.nodes);
-            } else if (rc) {
-                return rc;
-            }
+        if (in_bytes) {
+            std::memcpy(pin_in, P, in_bytes);
+            EGG_CUDA_TRY(cudaMemcpyAsync(c.scratch[1].ptr, pin_in, in_bytes, cudaMemcpyHostToDevice, c.stream));
         }
+        rc = dp_run(*plan, dtype, prec, c.scratch[1].ptr, B, c.scratch[2].ptr, c.stream);
+        if (rc) return rc;
+        EGG_CUDA_TRY(cudaMemcpyAsync(pin_out, c.scratch[2].ptr, out_bytes, cudaMemcpyDeviceToHost, c.stream));
         EGG_CUDA_TRY(cudaStreamSynchronize(c.stream));
         std::memcpy(out, pin_out, out_bytes);
         return EGG_OK;

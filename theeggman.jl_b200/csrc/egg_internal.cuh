@@ -204,8 +204,6 @@ int mix_tuned(int K, int dtype, int prec, int *batched, int64_t *group);
 int mix_set_tuning(int K, int dtype, int prec, int batched, int64_t group);
 // Drop the mixed-degree batch's recorded graphs (they hold the library's buffer addresses).
 void mix_graphs_clear();
-// egg_api.cu: the graphs of small egg_dp_batch calls (they name buffers that cache clearing frees).
-void small_dp_graphs_clear();
 
 // egg_sieve.cu
 // A caller-provided device region for the sieve's tables and partial sums (used instead of the
