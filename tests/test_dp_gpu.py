@@ -208,10 +208,10 @@ def test_level_kernel_batches(egg, nat, orc, W, K, B):
         assert got[b] == orc.haf_dp_pairs(np.ascontiguousarray(P[b]), plan, orc.F64), b
 
 
-def test_small_call_graph_replay(egg, orc, W):
-    """Small single-instance calls run eagerly once, are recorded into a graph the second time and
-    replayed after that: every call must still read its own matrix and match the reference's DP
-    bit for bit, in several element types, and again after the cache (and its graphs) is cleared."""
+def test_small_calls_repeated(egg, orc, W):
+    """Many small single-instance calls of a few shapes, through the page-locked staging buffer:
+    every call must read its own matrix and match the reference's DP bit for bit, in two element
+    types, and again after the cache is cleared."""
     for N in (12, 20):
         for rep in range(2):
             for i in range(5):
