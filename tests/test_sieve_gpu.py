@@ -187,6 +187,40 @@ def test_two_rows_per_lane_tiles(egg, orc, W, glynn):
     assert rel(got, dd) <= 4 * N * EPS * kappa(orc, Ax, [1] * E, glynn, dd) + 1e-15, (got, dd)
 
 
+def test_device_entry_point_orders_with_the_caller_stream(egg, W):
+    """egg_sieve_device forks its latency-bound launches (small levels, and the exact kernel's share
+    of terms too large for the register tiles) onto the library's side streams, and joins them back
+    before the reduction.  So a matrix written on the caller's stream just before the call, and a
+    copy of the result queued just after it, with no synchronisation in between, must give the host
+    entry point's result to the bit."""
+    import torch
+
+    from theeggman_b200 import _native as nat
+
+    L = nat.lib()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    for N, cplx in ((20, False), (40, False), (36, True)):
+        E = N // 2
+        A = W.dense_complex(N, 600 + N, 0.5) if cplx else W.dense_real(N, 600 + N, scale=1.0 / np.sqrt(N))
+        Ax = A[np.ix_(np.array(distinct_x(E)) - 1, np.array(distinct_x(E)) - 1)]
+        host = egg.sieve(Ax, [1] * E)
+        src = torch.from_numpy(np.ascontiguousarray(Ax.T)).to(dev)  # column-major bytes
+        dA = torch.zeros_like(src)
+        out = torch.full((2,), float("nan"), dtype=torch.float64, device=dev)
+        reps = np.ones(E, dtype=np.int64)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            dA.copy_(src)  # queued on the caller's stream, not yet done when the sieve is queued
+            rc = L.egg_sieve_device(nat.EGG_C128 if cplx else nat.EGG_F64, 1, dA.data_ptr(), E, reps.ctypes.data, 0,
+                                    out.data_ptr(), stream.cuda_stream)
+            got = out.clone()  # queued right after
+        stream.synchronize()
+        assert rc == 0, L.egg_last_error()
+        val = complex(got[0].item(), got[1].item()) if cplx else got[0].item()
+        assert val == (complex(host) if cplx else float(host)), (N, val, host)
+
+
 def test_config2_full_size_cross_check(egg, W):
     """N = 40 (E = 20, 2^20 inclusion-exclusion terms / 2^19 Glynn terms), both kernels: Glynn agrees
     with the device DP (machine precision, no cancellation) within the metric's 1e-10 (the
