@@ -173,6 +173,35 @@ def test_batch_mixes_subset_and_odometer_instances(egg, orc, W, cplx):
         assert rel(v, egg.sieve(Ax, er, glynn=g)) <= 1e-15
 
 
+@pytest.mark.parametrize("cplx", [False, True])
+def test_batch_sharing_multiplicity_patterns(egg, orc, W, cplx):
+    """A batch whose repeated-row instances share multiplicity patterns (several matrices with one
+    rpt, under each variant) takes their terms from one list per pattern and level; beside them a
+    pattern held by one instance only, and a distinct-row instance.  Each result is the scalar
+    call's, and within 4 N eps kappa of the oracle's double-double sum."""
+    from theeggman_b200.hafnian import _sieve_device_batch
+
+    T = np.dtype(np.complex128 if cplx else np.float64)
+    Axs, reps, gs = [], [], []
+    for i, rpt in enumerate([[2] * 8] * 6 + [[1, 3, 2, 2, 4]] * 4 + [[3, 1, 2, 2]]):
+        d = len(rpt)
+        A = W.dense_complex(d, 900 + i, 0.5) if cplx else W.dense_real(d, 900 + i)
+        x, er = orc.matched_reps(rpt)
+        Axs.append(orc.permuted(A, x))
+        reps.append(er)
+        gs.append(i % 2 == 1)
+    A = W.dense_complex(14, 990, 0.5) if cplx else W.dense_real(14, 990)
+    Axs.append(orc.permuted(A, distinct_x(7)))
+    reps.append([1] * 7)
+    gs.append(False)
+    vals = _sieve_device_batch(T, Axs, reps, gs, "fma")
+    for Ax, er, g, v in zip(Axs, reps, gs, vals):
+        dd = orc.calc_hafnian(Ax, er, g, sum_mode=1)
+        tol = 4 * 2 * sum(er) * EPS * kappa(orc, Ax, er, g, dd) + 1e-15
+        assert rel(v, dd) <= tol, (er, g, v, dd)
+        assert rel(v, egg.sieve(Ax, er, glynn=g)) <= 1e-14
+
+
 @pytest.mark.parametrize("glynn", [False, True])
 def test_two_rows_per_lane_tiles(egg, orc, W, glynn):
     """Real terms with 32 < m <= 48 run on tiles of two rows per lane (La Budde's table by two

@@ -15,7 +15,9 @@
 // register-tile kernels (egg_sieve_fast.cuh, egg_sieve_level*.cu) take every term that fits their
 // tiles unless the exact mode is asked for; this driver launches both and the fixed-order
 // reduction.
+#include <cmath>
 #include <cstring>
+#include <map>
 
 #include "egg_sieve.cuh"
 
@@ -589,6 +591,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         if (n > 63) return fail(EGG_ERR_TOO_LARGE, "the device sieve extracts coefficients up to lambda^63");
         s.n = (int)n;
         s.subset = (!s.glynn && s.E > 0 && s.E <= 32 && n == s.E && maxrep_of(edge_reps + b * Emax, s.E) == 1) ? 1 : 0;
+        s.pattern = -1;
         nmax = s.n > nmax ? s.n : nmax;
         s.steps = term_count(edge_reps + b * Emax, s.E, s.glynn);
         if (s.steps < 0) return fail(EGG_ERR_TOO_LARGE, "the sieve's term count overflows Int64");
@@ -623,6 +626,76 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     bool all_subset = true;
     for (const SieveInst &si : inst) all_subset = all_subset && si.subset;
     const int fast_hi = cplx ? 32 : 48;
+
+    // Term lists for the fast kernels: instances that share a multiplicity pattern (a batch of
+    // hafnian_repeated(B, rpt) with one rpt) share one list per level of their terms' digits, so
+    // that the level kernels deal the terms evenly instead of walking the whole odometer at every
+    // level.  Only patterns of at least two instances, small ones (E <= 16 edges, digits below 16,
+    // all lists within 2^22 terms), and not with caller-provided scratch, whose size must not depend
+    // on this.
+    std::vector<uint64_t> lists;
+    std::vector<int64_t> list_off;
+    const int list_stride = (int)Emax + 2;
+    if (fast_ok && !fixed && B > 1) {
+        constexpr int64_t kListTerms = (int64_t)1 << 22;
+        auto list_key = [&](int64_t b, std::vector<int64_t> &key) -> bool {
+            const SieveInst &si = inst[(size_t)b];
+            const int64_t *er = edge_reps + b * Emax;
+            if (si.subset || si.E == 0 || si.E > 16 || maxrep_of(er, si.E) > 15) return false;
+            key.assign(er, er + si.E);
+            key.push_back(si.glynn);
+            return true;
+        };
+        // Only patterns that at least two instances share: a list costs a host walk of the odometer.
+        std::map<std::vector<int64_t>, int> uses;
+        std::vector<int64_t> key;
+        for (int64_t b = 0; b < B; ++b)
+            if (list_key(b, key)) ++uses[key];
+        std::map<std::vector<int64_t>, int> pid;
+        for (int64_t b = 0; b < B; ++b) {
+            SieveInst &si = inst[(size_t)b];
+            const int64_t *er = edge_reps + b * Emax;
+            if (!list_key(b, key) || uses[key] < 2) continue;
+            auto it = pid.find(key);
+            if (it != pid.end()) {
+                si.pattern = it->second;
+                continue;
+            }
+            if ((int64_t)lists.size() + si.steps > kListTerms) continue;
+            // Walk the odometer once (edge E-1 least significant, digit 0 clipped under Glynn).
+            const int E = si.E;
+            std::vector<int> d((size_t)E, 0), base((size_t)E), r((size_t)E);
+            for (int i = 0; i < E; ++i) {
+                r[(size_t)i] = (int)er[i];
+                base[(size_t)i] = (si.glynn && i == 0) ? (r[(size_t)i] + 2) / 2 : r[(size_t)i] + 1;
+            }
+            std::vector<std::vector<uint64_t>> lvl((size_t)E + 1);
+            for (int64_t j = 0; j < si.steps; ++j) {
+                uint64_t word = 0;
+                int k = 0;
+                for (int i = 0; i < E; ++i) {
+                    word |= (uint64_t)d[(size_t)i] << (4 * i);
+                    const int kk = si.glynn ? 2 * d[(size_t)i] - r[(size_t)i] : d[(size_t)i];
+                    k += kk != 0;
+                }
+                lvl[(size_t)k].push_back(word);
+                for (int i = E - 1; i >= 0; --i) {
+                    if (++d[(size_t)i] < base[(size_t)i]) break;
+                    d[(size_t)i] = 0;
+                }
+            }
+            const int p = (int)pid.size();
+            pid[key] = p;
+            list_off.resize((size_t)(p + 1) * list_stride, 0);
+            for (int k = 0; k < list_stride; ++k) {
+                list_off[(size_t)p * list_stride + k] = (int64_t)lists.size();
+                if (k <= E) lists.insert(lists.end(), lvl[(size_t)k].begin(), lvl[(size_t)k].end());
+            }
+            si.pattern = p;
+        }
+    }
+    bool all_balanced = true;  // every instance's terms dealt in equal shares (subsets or lists)
+    for (const SieveInst &si : inst) all_balanced = all_balanced && (si.subset || si.pattern >= 0);
     const bool run_ex = !fast_ok || mmax_all > fast_hi || mmax_all == 0;
     const int skip_le = fast_ok ? fast_hi : 0;
 
@@ -704,6 +777,25 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             // faster on four), where each block's fixed costs weigh more.
             const int64_t waves = all_subset ? 1 : (avg_steps >= 16384 ? 4 : 2);
             int64_t per = ((int64_t)num_sms * bps * waves + B - 1) / B;
+            if (all_balanced && B > 1) {
+                // Equal shares within each instance: the only loss is a last, partial wave of
+                // blocks, so take the fewest blocks per instance whose waves end at least 90 % full.
+                const double res = (double)num_sms * bps;
+                int64_t best = 1;
+                double best_eff = 0.0;
+                for (int64_t p = 1; p <= 8; ++p) {
+                    const double w = (double)(B * p) / res, eff = w / std::ceil(w);
+                    if (eff > best_eff + 1e-9) {
+                        best = p;
+                        best_eff = eff;
+                    }
+                    if (eff >= 0.9) {
+                        best = p;
+                        break;
+                    }
+                }
+                per = best;
+            }
             const int64_t cap = (maxsteps + cw - 1) / cw;  // no more warps than terms
             if (per > cap) per = cap;
             if (per < 1) per = 1;
@@ -720,6 +812,8 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     const int64_t off_reps = off; off = align256(off + (int64_t)((reps.size() + 1) * sizeof(int)));
     const int64_t off_str = off; off = align256(off + (int64_t)((strides.size() + 1) * sizeof(int64_t)));
     const int64_t off_bin = off; off = align256(off + (int64_t)(binoms.size() * sizeof(double)));
+    const int64_t off_loff = off; off = align256(off + (int64_t)((list_off.size() + 1) * sizeof(int64_t)));
+    const int64_t off_lst = off; off = align256(off + (int64_t)((lists.size() + 1) * sizeof(uint64_t)));
     const int64_t off_pex = off; off = align256(off + (run_ex ? B * ex_bx * ex_wpb * 2 * (int64_t)sizeof(dd) : 0));
     const int64_t off_pf = off; off = align256(off + B * f_parts * 2 * (int64_t)sizeof(dd));
     char *base;
@@ -736,14 +830,16 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         base = (char *)c.scratch[5].ptr;
     }
     {
-        // The instance table, reps, strides and binomials in their device layout, sent as one copy
-        // (each copy from pageable memory has a fixed staging cost).
-        const size_t img = (size_t)(off_bin + (int64_t)(binoms.size() * sizeof(double)));
+        // The instance table, reps, strides, binomials and term lists in their device layout, sent
+        // as one copy (each copy from pageable memory has a fixed staging cost).
+        const size_t img = (size_t)(off_lst + (int64_t)(lists.size() * sizeof(uint64_t)));
         std::vector<char> h(img, 0);
         std::memcpy(h.data() + off_inst, inst.data(), inst.size() * sizeof(SieveInst));
         if (!reps.empty()) std::memcpy(h.data() + off_reps, reps.data(), reps.size() * sizeof(int));
         if (!strides.empty()) std::memcpy(h.data() + off_str, strides.data(), strides.size() * sizeof(int64_t));
         std::memcpy(h.data() + off_bin, binoms.data(), binoms.size() * sizeof(double));
+        if (!list_off.empty()) std::memcpy(h.data() + off_loff, list_off.data(), list_off.size() * sizeof(int64_t));
+        if (!lists.empty()) std::memcpy(h.data() + off_lst, lists.data(), lists.size() * sizeof(uint64_t));
         EGG_CUDA_TRY(cudaMemcpyAsync(base, h.data(), img, cudaMemcpyHostToDevice, st));
     }
     SieveArgs a;
@@ -753,6 +849,9 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.binom32 = binom32_device(st, &rc);
     if (!a.binom32) return rc;
     a.inst = (const SieveInst *)(base + off_inst);
+    a.lists = (const uint64_t *)(base + off_lst);
+    a.list_off = (const int64_t *)(base + off_loff);
+    a.list_stride = list_stride;
     a.maxrep = maxrep;
     a.Emax = Ews;
     a.nmax = nmax;

@@ -11,6 +11,7 @@ struct SieveInst {
     int64_t reps_off;   // offset into the reps / strides arrays
     int E, n, glynn, lda;
     int subset;         // all multiplicities 1 under inclusion-exclusion: term j is the edge subset j
+    int pattern;        // >= 0: the instance's terms are listed per level (SieveArgs::lists), else -1
 };
 
 struct SieveArgs {
@@ -23,6 +24,12 @@ struct SieveArgs {
     double *terms;         // if set (one instance, exact kernel only): term j's value at j (complex: 2j, 2j+1)
     int maxrep, warps_per_inst, Emax, nmax;
     int skip_le;           // the exact kernel leaves terms with m <= skip_le to the fast kernels
+    // Term lists of repeated multiplicity patterns: the digits of each term of pattern p and level k
+    // (4 bits per edge, edge i at bits 4i..4i+3) at lists[list_off[p * list_stride + k] ..
+    // list_off[p * list_stride + k + 1]), in odometer order.
+    const uint64_t *lists;
+    const int64_t *list_off;
+    int list_stride;
 };
 
 // Register-tile path (egg_sieve_fast.cuh, egg_sieve_level*.cu): level k evaluates the terms with

@@ -9,8 +9,10 @@
 //     variant for distinct rows, src/hafnian.jl:1139-1146): term j is the subset of edges whose
 //     digit is 1, so the level's terms are the k-subsets.  Every warp takes an equal share of them
 //     (one colex unrank, then Gosper successors), and the level runs as one balanced wave.
-//   * Any other multiplicities (hafnian_repeated, Glynn): each warp walks runs of 16 consecutive
-//     odometer indices, dealt round robin, and evaluates the terms of its level among them.
+//   * Any other multiplicities (hafnian_repeated, Glynn): when instances of the batch share a small
+//     pattern, its terms come listed per level (digits packed 4 bits per edge) and are dealt in
+//     equal shares; otherwise each group walks runs of 16 consecutive odometer indices, dealt round
+//     robin, and evaluates the terms of its level among them.
 //
 // Each block writes one partial (re, im) per instance: its warps' double-double sums added in a
 // fixed order.
@@ -98,6 +100,46 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
                         w.eidx[pos] = e;
                         w.kval[pos] = 1.0;
                     }
+                __syncwarp(gm);
+                eval_term(prefac);
+                __syncwarp(gm);
+            }
+        }
+    } else if (in.pattern >= 0 && K <= E) {
+        // The level's terms listed by digits (a multiplicity pattern shared by instances of the
+        // batch): every group takes an equal share of the list, as for subsets.  Lane i of the group
+        // takes digit i (E <= 16 here), and the term is set up as on the odometer below.
+        const int64_t lrow = (int64_t)in.pattern * a.list_stride + K;
+        const int64_t lb = a.list_off[lrow];
+        const uint64_t cnt = (uint64_t)(a.list_off[lrow + 1] - lb);
+        const uint64_t lo = (uint64_t)gslot * cnt / W, hi = ((uint64_t)gslot + 1) * cnt / W;
+        const int *reps = a.reps + in.reps_off;
+        const int mr1 = a.maxrep + 1;
+        const bool unit = a.maxrep <= 1;
+        const int r = gl < E ? reps[gl] : 0;
+        for (uint64_t rk = lo;; ++rk) {
+            const bool has = rk < hi;
+            if (!__any_sync(FULL, has)) break;
+            if (has) {
+                const uint64_t word = a.lists[lb + (int64_t)rk];
+                const int digit = gl < E ? (int)((word >> (4 * gl)) & 15u) : 0;
+                const int kk = gl < E ? (in.glynn ? 2 * digit - r : digit) : 0;
+                const bool nz = gl < E && kk != 0;
+                const unsigned mask = group_ballot(nz);
+                const int esum = __reduce_add_sync(gm, gl < E ? digit : 0);
+                double bp = 1.0;
+                if (!unit) {
+                    bp = gl < E ? a.binoms[r + digit * mr1] : 1.0;
+                    for (int off = G / 2; off > 0; off >>= 1) bp *= __shfl_xor_sync(gm, bp, off, G);
+                }
+                double prefac = ((n - esum) & 1) ? -bp : bp;
+                const int k0 = __shfl_sync(gm, kk, 0, G);
+                if (in.glynn && k0 == 0) prefac *= 0.5;  // the mirror's fixed point (:570-573)
+                if (nz) {
+                    const int pos = __popc(mask & ((1u << gl) - 1u));
+                    w.eidx[pos] = gl;
+                    w.kval[pos] = (double)kk;
+                }
                 __syncwarp(gm);
                 eval_term(prefac);
                 __syncwarp(gm);
