@@ -227,8 +227,7 @@ int egg_cache_clear(void)
     Context &c = ctx();
     if (c.device >= 0) cudaStreamSynchronize(c.stream);
     mix_graphs_clear();
-    for (auto &kv : c.plans)
-        if (kv.second.trans) cudaFree(kv.second.trans);
+    for (auto &kv : c.plans) release_plan_memory(kv.second);
     c.plans.clear();
     for (auto &b : c.scratch) {
         if (b.ptr) cudaFree(b.ptr);
@@ -403,7 +402,7 @@ int egg_plan_release(int K, int idx_bytes)
     auto it = ctx().plans.find({K, idx_bytes});
     if (it == ctx().plans.end()) return fail(EGG_ERR_NO_PLAN, "no resident plan for degree " + std::to_string(K));
     cudaStreamSynchronize(ctx().stream);
-    cudaFree(it->second.trans);
+    release_plan_memory(it->second);
     ctx().plans.erase(it);
     return EGG_OK;
 }

@@ -19,7 +19,9 @@
 // contracts each multiply-add as the reference's GPU kernel does.  EGG_PREC_MIXED multiplies in
 // FP32 and accumulates each state in FP64.  Integer inputs run exactly in Int128.
 #include <cooperative_groups.h>
+#include <map>
 #include <type_traits>
+#include <utility>
 
 #include "egg_dp_common.cuh"
 
@@ -523,6 +525,179 @@ __global__ void __launch_bounds__(MAXT) dpc_small_kernel(const uint32_t *__restr
     }
 }
 
+// Largest degree and cluster size of the one-instance cluster kernel (a level's states fit in 13
+// bits beside an 8-bit pair index up to K = 22).
+static constexpr int kClusterMaxK = 22;
+static constexpr int kClusterMaxLevels = kClusterMaxK / 2 + 1;
+
+// One state's transitions as (child << 8) | pair, in plan order: walk_state's index arithmetic
+// without the loads.
+template <class M>
+__device__ __forceinline__ void list_state(M m, const uint2 *TP, int ld, int c, int K, int m0, uint32_t *ent)
+{
+    const int e1 = low_bit<M>(m);
+    M rest = m & (m - 1);
+    const int e2 = low_bit<M>(rest);
+    rest &= rest - 1;
+    uint32_t suf = 0;
+    {
+        M r = rest;
+        for (int x = 3; x <= c; ++x) {
+            const int e = low_bit<M>(r);
+            r &= r - 1;
+            suf += TP[(e - 1) * ld + (x - 2)].x;
+        }
+    }
+    const int ib = e1 + m0 + 1;
+    const int pb = (ib - 1) * K - (ib * (ib + 1)) / 2 + m0;
+    uint32_t pre = 0, padd = TP[(e2 - 1) * ld].y;
+    int ej = e2;
+    for (int x = 2; x <= c; ++x) {
+        ent[x - 2] = ((pre + suf) << 8) | (uint32_t)(pb + ej);
+        pre += padd;
+        if (x < c) {
+            const int en = low_bit<M>(rest);
+            rest &= rest - 1;
+            const uint2 t = TP[(en - 1) * ld + (x - 1)];
+            suf -= t.x;
+            padd = t.y;
+            ej = en;
+        }
+    }
+}
+
+// CTA `rank`'s share of a closed-form plan in an nr-CTA cluster: its states of level L (c = 2L >= 4)
+// are s = rank + nr j, j < cnt(L); unit_lo[L] numbers them level after level and ent_lo[L] their
+// transition entries (c - 1 per state).  Entries [2, nlev] are set.
+__device__ __forceinline__ void cluster_layout(const uint2 *TP, int ld, int K, int nr, int rank, int *unit_lo, int *ent_lo)
+{
+    const int nlev = K / 2 + 1;
+    int u = 0, e = 0;
+    for (int L = 2; L < nlev; ++L) {
+        const int c = 2 * L, U = K - (K - c) / 2;
+        const int n = (int)TP[U * ld + c].x;
+        const int cnt = n > rank ? (n - 1 - rank) / nr + 1 : 0;
+        unit_lo[L] = u;
+        ent_lo[L] = e;
+        u += cnt;
+        e += cnt * (c - 1);
+    }
+    unit_lo[nlev] = u;
+    ent_lo[nlev] = e;
+}
+
+// The transition lists of dpc_cluster_kernel for one degree and cluster size, built once and kept
+// with the plan: CTA r's list is ent[r * stride ...].  blockIdx.x is the CTA, blockIdx.y a slice of
+// its states.
+__global__ void __launch_bounds__(256) cluster_list_kernel(const uint32_t *__restrict__ binom, uint32_t *ent, int64_t stride,
+                                                           int K, int nr)
+{
+    __shared__ uint2 TP[(kClusterMaxK + 1) * (kClusterMaxK + 1)];
+    __shared__ int unit_lo[kClusterMaxLevels + 1], ent_lo[kClusterMaxLevels + 1];
+    const int ld = K + 1, rank = blockIdx.x, nlev = K / 2 + 1;
+    fill_pair_table(TP, binom, ld, ld, threadIdx.x, blockDim.x);
+    __syncthreads();
+    if (threadIdx.x == 0) cluster_layout(TP, ld, K, nr, rank, unit_lo, ent_lo);
+    __syncthreads();
+    uint32_t *mine = ent + (int64_t)rank * stride;
+    for (int u = blockIdx.y * blockDim.x + threadIdx.x; u < unit_lo[nlev]; u += gridDim.y * blockDim.x) {
+        int L = 2;
+        while (u >= unit_lo[L + 1]) ++L;
+        const int c = 2 * L, m0 = (K - c) / 2, U = K - m0;
+        const int j = u - unit_lo[L];
+        const uint32_t m = colex_unrank<uint32_t>(TP, ld, U, c, (uint32_t)(rank + nr * j));
+        list_state<uint32_t>(m, TP, ld, c, K, m0, mine + ent_lo[L] + j * (c - 1));
+    }
+}
+
+// One instance of a small degree on a cluster of nr CTAs (nr a power of two).  State s of a level
+// belongs to CTA s mod nr, which keeps its value at s / nr of its own two level buffers in shared
+// memory; a state's children are read from their owners through distributed shared memory, and a
+// cluster barrier separates the levels.  Each CTA first copies its transition list (built once per
+// degree by cluster_list_kernel) into shared memory, so a level is only loads and the ordered sum.
+// The walk's order and arithmetic are dpc_small_kernel's: the result is bit for bit the same.
+template <class Op, class PT, class HT, class AT, int MAXT>
+__global__ void __launch_bounds__(MAXT) dpc_cluster_kernel(const uint32_t *__restrict__ binom, const uint32_t *__restrict__ gent,
+                                                           int64_t stride, const PT *__restrict__ P, HT *__restrict__ out,
+                                                           int K, int lmax)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    const int nr = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const int lg = __ffs(nr) - 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int unit_lo[kClusterMaxLevels + 1], ent_lo[kClusterMaxLevels + 1];
+    HT *H0 = reinterpret_cast<HT *>(smem_raw);
+    HT *H1 = H0 + lmax;
+    PT *Ps = reinterpret_cast<PT *>(H1 + lmax);
+    const int npairs = K * (K - 1) / 2;
+    const int ld = K + 1;
+    const size_t tp_off = (((size_t)2 * lmax * sizeof(HT) + (size_t)npairs * sizeof(PT) + 15) / 16) * 16;
+    uint2 *TP = reinterpret_cast<uint2 *>(smem_raw + tp_off);
+    uint32_t *ENT = reinterpret_cast<uint32_t *>(smem_raw + tp_off + (((size_t)ld * ld * sizeof(uint2) + 15) / 16) * 16);
+    const int nlev = K / 2 + 1;  // levels L = 0..K/2, popcount c = 2L
+    fill_pair_table(TP, binom, ld, ld, threadIdx.x, blockDim.x);
+    for (int q = threadIdx.x; q < npairs; q += blockDim.x) Ps[q] = P[q];
+    __syncthreads();
+    if (threadIdx.x == 0) cluster_layout(TP, ld, K, nr, rank, unit_lo, ent_lo);
+    {
+        const int n = (K / 2 + 1) * (K / 2) / 2;  // level c = 2, into H1
+        for (int j = threadIdx.x; rank + nr * j < n; j += blockDim.x)
+            H1[j] = first_level_value<Op, PT, HT, AT>(rank + nr * j, K, Ps, 1, 0);
+    }
+    __syncthreads();
+    {
+        // The list, in 16-byte pieces (the stride and this buffer are padded to 4 entries).
+        const uint4 *src = reinterpret_cast<const uint4 *>(gent + (int64_t)rank * stride);
+        uint4 *dst = reinterpret_cast<uint4 *>(ENT);
+        const int n4 = (ent_lo[nlev] + 3) / 4;
+        for (int i = threadIdx.x; i < n4; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    // Every CTA has started, copied its list and written level c = 2.
+    cl.sync();
+    for (int L = 2; L < nlev; ++L) {
+        const int c = 2 * L;
+        const HT *prev = (L & 1) ? H0 : H1;
+        HT *cur = (L & 1) ? H1 : H0;
+        const int cnt = unit_lo[L + 1] - unit_lo[L];
+        for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+            const uint32_t *e = ENT + ent_lo[L] + j * (c - 1);
+            AT acc = zero_of<AT>();
+            for (int x0 = 0; x0 < c - 1; x0 += kBatch) {
+                HT hv[kBatch];
+                PT pv[kBatch];
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u)
+                    if (x0 + u < c - 1) {
+                        const uint32_t t = e[x0 + u];
+                        const uint32_t child = t >> 8;
+                        hv[u] = *cl.map_shared_rank(prev + (child >> lg), child & (uint32_t)(nr - 1));
+                        pv[u] = Ps[t & 255u];
+                    }
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u)
+                    if (x0 + u < c - 1) acc = madd(Op{}, acc, pv[u], hv[u]);
+            }
+            HT v;
+            store(v, acc);
+            if (L == nlev - 1) out[0] = v;  // the last level has the one state, on CTA 0
+            else cur[j] = v;
+        }
+        // The level is complete everywhere before any CTA reads it, and before any CTA overwrites
+        // the buffer this level read; the last barrier also keeps every CTA's shared memory alive
+        // until all remote reads are done.
+        cl.sync();
+    }
+}
+
+// Entries per CTA of the cluster lists: the most any CTA of an nr-CTA cluster lists (CTA 0's),
+// rounded up to 4 so that lists are copied in 16-byte pieces.
+static int64_t cluster_stride(const DevPlan &plan, int nr)
+{
+    int64_t e = 0;
+    for (int L = 2; L < (int)plan.levels.size(); ++L) e += (plan.levels[L].n + nr - 1) / nr * (2 * L - 1);
+    return (e + 3) / 4 * 4;
+}
+
 template <class HT>
 __global__ void fill_one_kernel(HT *H, int64_t B)
 {
@@ -706,9 +881,90 @@ static int launch_span(const uint32_t *bt, const DevPlan &plan, const PT *P, HT 
     return EGG_OK;
 }
 
+// One instance of a small degree on one cluster (dpc_cluster_kernel) of 8 CTAs, or of 16 where
+// 8 CTAs' shared memory cannot hold their states and lists.  Returns kNoCluster, with nothing launched, when the
+// degree is out of its range or the device cannot place such a cluster.
+static constexpr int kNoCluster = -1;
+static constexpr size_t kClusterSmemMax = 200 * 1024;
+
+template <class Op, class PT, class HT, class AT>
+static int launch_cluster(const uint32_t *bt, const DevPlan &plan, const PT *P, HT *out, cudaStream_t st)
+{
+    const int K = plan.K;
+    if (K < 4 || K > kClusterMaxK || (int)plan.levels.size() != K / 2 + 1) return kNoCluster;
+    constexpr int kMaxT = 1024;
+    auto k = dpc_cluster_kernel<Op, PT, HT, AT, kMaxT>;
+    const int64_t maxlev = max_level(plan);
+    const int64_t npairs = (int64_t)K * (K - 1) / 2;
+    auto smem_for = [&](int nr) {
+        const int64_t lmax = (maxlev + nr - 1) / nr;
+        return (((size_t)2 * lmax * sizeof(HT) + (size_t)npairs * sizeof(PT) + 15) / 16) * 16 +
+               (((size_t)(K + 1) * (K + 1) * sizeof(uint2) + 15) / 16) * 16 +
+               (size_t)cluster_stride(plan, nr) * sizeof(uint32_t);
+    };
+    int nr = 8;
+    size_t smem = smem_for(nr);
+    if (smem > kClusterSmemMax) {
+        nr = 16;
+        smem = smem_for(nr);
+        if (smem > kClusterSmemMax) return kNoCluster;
+    }
+    const int lmax = (int)((maxlev + nr - 1) / nr);
+    // Whether a cluster of this shape can be placed, per (cluster size, shared memory); callers hold
+    // the library's lock.
+    static std::map<std::pair<int, size_t>, bool> placeable;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)nr;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)nr);
+    cfg.blockDim = dim3(kMaxT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const auto key = std::make_pair(nr, smem);
+    auto it = placeable.find(key);
+    if (it == placeable.end()) {
+        int rc = smem_limit_at_least((const void *)k, smem);
+        if (rc) return rc;
+        if (nr > 8) EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        int nclusters = 0;
+        EGG_CUDA_TRY(cudaOccupancyMaxActiveClusters(&nclusters, k, &cfg));
+        it = placeable.emplace(key, nclusters > 0).first;
+    }
+    if (!it->second) return kNoCluster;
+    const int slot = nr == 8 ? 0 : 1;
+    const int64_t stride = cluster_stride(plan, nr);
+    if (!plan.cluster_lists[slot]) {
+        const size_t bytes = (size_t)nr * stride * sizeof(uint32_t);
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return kNoCluster;
+        }
+        cluster_list_kernel<<<dim3((unsigned)nr, 8), 256, 0, st>>>(bt, (uint32_t *)p, stride, K, nr);
+        count_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            cudaFree(p);
+            return fail(EGG_ERR_CUDA, std::string("cluster lists: ") + cudaGetErrorString(e));
+        }
+        plan.cluster_lists[slot] = p;
+        plan.cluster_list_bytes[slot] = (int64_t)bytes;
+    }
+    const uint32_t *gent = (const uint32_t *)plan.cluster_lists[slot];
+    EGG_CUDA_TRY(cudaLaunchKernelEx(&cfg, k, bt, gent, stride, P, out, K, lmax));
+    count_launch();
+    return EGG_OK;
+}
+
 // A closed-form plan: one launch for small degrees, else one launch per level with the last level
-// written straight into `out` when the state type is the output type.  For one instance, the runs of
-// small levels at either end of the plan each take one span launch.
+// written straight into `out` when the state type is the output type.  For one instance of a larger
+// degree, the runs of small levels at either end of the plan each take one span launch.
 template <class Op, class PT, class HT, class AT>
 static int run_closed(const DevPlan &plan, const PT *P, HT *h0, HT *h1, HT *out, bool out_direct, int64_t B,
                       cudaStream_t st)
@@ -717,10 +973,14 @@ static int run_closed(const DevPlan &plan, const PT *P, HT *h0, HT *h1, HT *out,
     const uint32_t *bt = binom32_device(st, &rc);
     if (!bt) return rc;
     const int K = plan.K;
-    // Batches of small degrees: one CTA per instance, the whole plan in shared memory.  A single
-    // instance runs as spans across the machine instead (below), which finishes sooner.
-    const size_t small = (out_direct && B > 1) ? closed_small_smem<PT, HT>(plan) : 0;
-    if (small) {
+    // A single instance of a small degree: one cluster of CTAs.  A batch of small degrees, whose two
+    // largest levels fit in shared memory: one CTA per instance with the whole plan inside it.
+    const size_t small = out_direct ? closed_small_smem<PT, HT>(plan) : 0;
+    if (out_direct && B == 1) {
+        rc = launch_cluster<Op, PT, HT, AT>(bt, plan, P, out, st);
+        if (rc != kNoCluster) return rc;
+    }
+    if (small && B > 1) {
         constexpr int kMaxT = sizeof(HT) <= 8 ? 1024 : 512;
         auto k = dpc_small_kernel<Op, PT, HT, AT, kMaxT>;
         rc = smem_limit_at_least((const void *)k, small);

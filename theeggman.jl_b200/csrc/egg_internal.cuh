@@ -118,9 +118,28 @@ struct DevPlan {
     void *trans = nullptr;        // device, ntrans entries of idx_bytes; null for a closed-form plan
     std::vector<Level> levels;    // levels[0] is the empty set
     std::vector<int64_t> level_starts;  // the reference's 1-based `levels` vector
+    // The one-instance cluster kernel's transition lists for clusters of 8 and of 16 CTAs (closed-form
+    // plans of small degrees), built on first use and kept with the plan.
+    mutable void *cluster_lists[2] = {nullptr, nullptr};
+    mutable int64_t cluster_list_bytes[2] = {0, 0};
     bool closed_form() const { return trans == nullptr; }
-    int64_t bytes() const { return trans ? ntrans * (int64_t)idx_bytes : 0; }
+    int64_t bytes() const
+    {
+        return (trans ? ntrans * (int64_t)idx_bytes : 0) + cluster_list_bytes[0] + cluster_list_bytes[1];
+    }
 };
+
+// Frees a plan's device memory (its transition array and its cluster lists).
+inline void release_plan_memory(DevPlan &p)
+{
+    if (p.trans) cudaFree(p.trans);
+    p.trans = nullptr;
+    for (int i = 0; i < 2; ++i) {
+        if (p.cluster_lists[i]) cudaFree(p.cluster_lists[i]);
+        p.cluster_lists[i] = nullptr;
+        p.cluster_list_bytes[i] = 0;
+    }
+}
 
 struct DevBuf {
     void *ptr = nullptr;
