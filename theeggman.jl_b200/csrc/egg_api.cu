@@ -441,8 +441,22 @@ int egg_dp_batch(int K, int idx_bytes, int dtype, int prec, const void *P, int64
     const size_t in_bytes = (size_t)B * npairs * es, out_bytes = (size_t)B * oes;
     if (chunk == B && in_bytes + out_bytes + 256 <= Context::kPinnedBytes) {
         // A small call: both transfers through the page-locked staging buffer.
-        if (!c.pinned) EGG_CUDA_TRY(cudaHostAlloc(&c.pinned, Context::kPinnedBytes, cudaHostAllocDefault));
+        if (!c.pinned) {
+            EGG_CUDA_TRY(cudaHostAlloc(&c.pinned, Context::kPinnedBytes, cudaHostAllocMapped));
+            EGG_CUDA_TRY(cudaHostGetDevicePointer(&c.pinned_dev, c.pinned, 0));
+        }
         char *pin_in = (char *)c.pinned, *pin_out = pin_in + ((in_bytes + 255) / 256) * 256;
+        if (B == 1) {
+            // One instance of a small degree: its pairs travel in the launch and its value is
+            // written straight into the mapped staging buffer, so neither copy is needed.
+            rc = dp_run_one_host(*plan, dtype, prec, P, (char *)c.pinned_dev + (pin_out - pin_in), c.stream);
+            if (rc == EGG_OK) {
+                EGG_CUDA_TRY(cudaStreamSynchronize(c.stream));
+                std::memcpy(out, pin_out, out_bytes);
+                return EGG_OK;
+            }
+            if (rc != kDpNotHere) return rc;
+        }
         if (in_bytes) {
             std::memcpy(pin_in, P, in_bytes);
             EGG_CUDA_TRY(cudaMemcpyAsync(c.scratch[1].ptr, pin_in, in_bytes, cudaMemcpyHostToDevice, c.stream));

@@ -19,6 +19,7 @@
 // contracts each multiply-add as the reference's GPU kernel does.  EGG_PREC_MIXED multiplies in
 // FP32 and accumulates each state in FP64.  Integer inputs run exactly in Int128.
 #include <cooperative_groups.h>
+#include <cstring>
 #include <map>
 #include <type_traits>
 #include <utility>
@@ -529,6 +530,16 @@ __global__ void __launch_bounds__(MAXT) dpc_small_kernel(const uint32_t *__restr
 // bits beside an 8-bit pair index up to K = 22).
 static constexpr int kClusterMaxK = 22;
 static constexpr int kClusterMaxLevels = kClusterMaxK / 2 + 1;
+static constexpr int kClusterMaxPairs = kClusterMaxK * (kClusterMaxK - 1) / 2;
+
+// The pairs of a one-instance cluster launch: in device memory (ptr), or, for a call from host
+// memory, carried in the launch's own parameters (ptr null), so no copy precedes the launch.  At most
+// 231 pairs of 16 bytes, within the 4 KB of kernel parameters.
+template <class PT>
+struct ClusterPairs {
+    const PT *ptr;
+    PT v[kClusterMaxPairs];
+};
 
 // One state's transitions as (child << 8) | pair, in plan order: walk_state's index arithmetic
 // without the loads.
@@ -618,8 +629,8 @@ __global__ void __launch_bounds__(256) cluster_list_kernel(const uint32_t *__res
 // The walk's order and arithmetic are dpc_small_kernel's: the result is bit for bit the same.
 template <class Op, class PT, class HT, class AT, int MAXT>
 __global__ void __launch_bounds__(MAXT) dpc_cluster_kernel(const uint32_t *__restrict__ binom, const uint32_t *__restrict__ gent,
-                                                           int64_t stride, const PT *__restrict__ P, HT *__restrict__ out,
-                                                           int K, int lmax)
+                                                           int64_t stride, const __grid_constant__ ClusterPairs<PT> P,
+                                                           HT *__restrict__ out, int K, int lmax)
 {
     cg::cluster_group cl = cg::this_cluster();
     const int nr = (int)cl.num_blocks(), rank = (int)cl.block_rank();
@@ -636,7 +647,7 @@ __global__ void __launch_bounds__(MAXT) dpc_cluster_kernel(const uint32_t *__res
     uint32_t *ENT = reinterpret_cast<uint32_t *>(smem_raw + tp_off + (((size_t)ld * ld * sizeof(uint2) + 15) / 16) * 16);
     const int nlev = K / 2 + 1;  // levels L = 0..K/2, popcount c = 2L
     fill_pair_table(TP, binom, ld, ld, threadIdx.x, blockDim.x);
-    for (int q = threadIdx.x; q < npairs; q += blockDim.x) Ps[q] = P[q];
+    for (int q = threadIdx.x; q < npairs; q += blockDim.x) Ps[q] = P.ptr ? P.ptr[q] : P.v[q];
     __syncthreads();
     if (threadIdx.x == 0) cluster_layout(TP, ld, K, nr, rank, unit_lo, ent_lo);
     {
@@ -888,10 +899,11 @@ static constexpr int kNoCluster = -1;
 static constexpr size_t kClusterSmemMax = 200 * 1024;
 
 template <class Op, class PT, class HT, class AT>
-static int launch_cluster(const uint32_t *bt, const DevPlan &plan, const PT *P, HT *out, cudaStream_t st)
+static int launch_cluster(const uint32_t *bt, const DevPlan &plan, const PT *P, HT *out, cudaStream_t st,
+                          bool host_pairs = false)
 {
     const int K = plan.K;
-    if (K < 4 || K > kClusterMaxK || (int)plan.levels.size() != K / 2 + 1) return kNoCluster;
+    if (K < 4 || K > kClusterMaxK || (int)plan.levels.size() != K / 2 + 1 || !plan.closed_form()) return kNoCluster;
     constexpr int kMaxT = 1024;
     auto k = dpc_cluster_kernel<Op, PT, HT, AT, kMaxT>;
     const int64_t maxlev = max_level(plan);
@@ -957,7 +969,10 @@ static int launch_cluster(const uint32_t *bt, const DevPlan &plan, const PT *P, 
         plan.cluster_list_bytes[slot] = (int64_t)bytes;
     }
     const uint32_t *gent = (const uint32_t *)plan.cluster_lists[slot];
-    EGG_CUDA_TRY(cudaLaunchKernelEx(&cfg, k, bt, gent, stride, P, out, K, lmax));
+    ClusterPairs<PT> pa;
+    pa.ptr = host_pairs ? nullptr : P;
+    if (host_pairs) std::memcpy(pa.v, P, (size_t)npairs * sizeof(PT));
+    EGG_CUDA_TRY(cudaLaunchKernelEx(&cfg, k, bt, gent, stride, pa, out, K, lmax));
     count_launch();
     return EGG_OK;
 }
@@ -1263,6 +1278,39 @@ int dp_run_grouped(const DevPlan &plan, int dtype, int prec, const void *dP, int
                                                                         (__int128 *)h1, maxlev, (__int128 *)dout, st);
     }
     return fail(EGG_ERR_ARGUMENT, "unknown dtype");
+}
+
+int dp_run_one_host(const DevPlan &plan, int dtype, int prec, const void *P, void *dout, cudaStream_t st)
+{
+    if (prec == EGG_PREC_MIXED) return kDpNotHere;
+    int rc = EGG_OK;
+    const uint32_t *bt = binom32_device(st, &rc);
+    if (!bt) return rc;
+    const bool fma_mode = prec == EGG_PREC_FMA;
+    switch (dtype) {
+    case EGG_F64:
+        rc = fma_mode ? launch_cluster<FmaOp, double, double, double>(bt, plan, (const double *)P, (double *)dout, st, true)
+                      : launch_cluster<ExactOp, double, double, double>(bt, plan, (const double *)P, (double *)dout, st, true);
+        break;
+    case EGG_C128:
+        rc = fma_mode ? launch_cluster<FmaOp, cd, cd, cd>(bt, plan, (const cd *)P, (cd *)dout, st, true)
+                      : launch_cluster<ExactOp, cd, cd, cd>(bt, plan, (const cd *)P, (cd *)dout, st, true);
+        break;
+    case EGG_F32:
+        rc = fma_mode ? launch_cluster<FmaOp, float, float, float>(bt, plan, (const float *)P, (float *)dout, st, true)
+                      : launch_cluster<ExactOp, float, float, float>(bt, plan, (const float *)P, (float *)dout, st, true);
+        break;
+    case EGG_C64:
+        rc = fma_mode ? launch_cluster<FmaOp, cf, cf, cf>(bt, plan, (const cf *)P, (cf *)dout, st, true)
+                      : launch_cluster<ExactOp, cf, cf, cf>(bt, plan, (const cf *)P, (cf *)dout, st, true);
+        break;
+    case EGG_I64:
+        rc = launch_cluster<IntOp, int64_t, __int128, __int128>(bt, plan, (const int64_t *)P, (__int128 *)dout, st, true);
+        break;
+    default:
+        return kDpNotHere;
+    }
+    return rc == kNoCluster ? kDpNotHere : rc;
 }
 
 int dp_run(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t B, void *dout, cudaStream_t st)

@@ -157,7 +157,8 @@ struct Context {
     cudaEvent_t fork_ev = nullptr, join_ev[kSideStreams] = {};
     // Page-locked host staging for small transfers: a copy from pageable memory is staged by the
     // driver at a fixed cost of several microseconds, a copy from page-locked memory is not.
-    void *pinned = nullptr;
+    void *pinned = nullptr;      // mapped: pinned_dev is its device address
+    void *pinned_dev = nullptr;
     static constexpr size_t kPinnedBytes = 128 * 1024;
     int num_sms = 0;
     std::map<std::pair<int, int>, DevPlan> plans;
@@ -205,6 +206,11 @@ const uint32_t *binom32_device(cudaStream_t st, int *rc);
 // made resident (closed form) if absent.
 DevPlan *dp_plan_for(int K, int *rc);
 int dp_run(const DevPlan &plan, int dtype, int prec, const void *dP, int64_t B, void *dout, cudaStream_t st);
+// One instance whose pairs are in host memory, carried in the launch's parameters (small degrees on
+// one cluster); dout is device-visible.  Returns kDpNotHere, with nothing launched, when that
+// kernel does not take the call.
+constexpr int kDpNotHere = -1;
+int dp_run_one_host(const DevPlan &plan, int dtype, int prec, const void *P, void *dout, cudaStream_t st);
 size_t dp_scratch_bytes(const DevPlan &plan, int dtype, int prec, int64_t B);
 // G instances of a closed-form plan side by side, each evaluated as a single instance: P is
 // instance-major (instance g's pairs at g * npairs), out receives G values.  Degrees 4..40, for
