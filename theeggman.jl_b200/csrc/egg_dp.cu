@@ -892,9 +892,9 @@ static int launch_span(const uint32_t *bt, const DevPlan &plan, const PT *P, HT 
     return EGG_OK;
 }
 
-// One instance of a small degree on one cluster (dpc_cluster_kernel) of 8 CTAs, or of 16 where
-// 8 CTAs' shared memory cannot hold their states and lists.  Returns kNoCluster, with nothing launched, when the
-// degree is out of its range or the device cannot place such a cluster.
+// One instance of a small degree on one cluster (dpc_cluster_kernel) of 16 CTAs, or of 8 where 16
+// cannot be placed.  Returns kNoCluster, with nothing launched, when the degree is out of its range
+// or the device cannot place such a cluster.
 static constexpr int kNoCluster = -1;
 static constexpr size_t kClusterSmemMax = 200 * 1024;
 
@@ -914,40 +914,48 @@ static int launch_cluster(const uint32_t *bt, const DevPlan &plan, const PT *P, 
                (((size_t)(K + 1) * (K + 1) * sizeof(uint2) + 15) / 16) * 16 +
                (size_t)cluster_stride(plan, nr) * sizeof(uint32_t);
     };
-    int nr = 8;
-    size_t smem = smem_for(nr);
-    if (smem > kClusterSmemMax) {
-        nr = 16;
-        smem = smem_for(nr);
-        if (smem > kClusterSmemMax) return kNoCluster;
-    }
-    const int lmax = (int)((maxlev + nr - 1) / nr);
     // Whether a cluster of this shape can be placed, per (cluster size, shared memory); callers hold
     // the library's lock.
     static std::map<std::pair<int, size_t>, bool> placeable;
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = (unsigned)nr;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3((unsigned)nr);
     cfg.blockDim = dim3(kMaxT);
-    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    const auto key = std::make_pair(nr, smem);
-    auto it = placeable.find(key);
-    if (it == placeable.end()) {
-        int rc = smem_limit_at_least((const void *)k, smem);
-        if (rc) return rc;
-        if (nr > 8) EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        int nclusters = 0;
-        EGG_CUDA_TRY(cudaOccupancyMaxActiveClusters(&nclusters, k, &cfg));
-        it = placeable.emplace(key, nclusters > 0).first;
+    // 16 CTAs where they can be placed (each level's remote reads spread over twice the SMs), else 8.
+    int nr = 0;
+    size_t smem = 0;
+    for (int cand : {16, 8}) {
+        const size_t sm = smem_for(cand);
+        if (sm > kClusterSmemMax) continue;
+        at[0].val.clusterDim.x = (unsigned)cand;
+        cfg.gridDim = dim3((unsigned)cand);
+        cfg.dynamicSmemBytes = sm;
+        const auto key = std::make_pair(cand, sm);
+        auto it = placeable.find(key);
+        if (it == placeable.end()) {
+            int rc = smem_limit_at_least((const void *)k, sm);
+            if (rc) return rc;
+            if (cand > 8) EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, k, &cfg) != cudaSuccess) {
+                cudaGetLastError();
+                nclusters = 0;
+            }
+            it = placeable.emplace(key, nclusters > 0).first;
+        }
+        if (it->second) {
+            nr = cand;
+            smem = sm;
+            break;
+        }
     }
-    if (!it->second) return kNoCluster;
+    if (!nr) return kNoCluster;
+    const int lmax = (int)((maxlev + nr - 1) / nr);
     const int slot = nr == 8 ? 0 : 1;
     const int64_t stride = cluster_stride(plan, nr);
     if (!plan.cluster_lists[slot]) {
