@@ -738,7 +738,23 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     };
     std::vector<FastLaunch> fl;
     int64_t f_parts = 0;  // sum over launches of partials (one per block) per instance
-    if (fast_ok) {
+    // One small distinct-row instance: all its terms in one launch (every nonzero edge subset on the
+    // tile of its largest size) instead of a launch per popcount level, whose fixed costs would
+    // outweigh its few terms.
+    const bool fused = fast_ok && B == 1 && all_subset && inst[0].E >= 1 && inst[0].E <= kFusedMaxE;
+    if (fused) {
+        const int k = inst[0].E;
+        const bool narrow = 2 * k <= 16;
+        int cw = 0, bps = 0;
+        int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, &cw, &bps) : level_shape_real(nmax, k, narrow, &cw, &bps);
+        if (rc0) return rc0;
+        if (bps < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
+        const int64_t terms_all = ((int64_t)1 << k) - 1, per_block = (int64_t)cw * (narrow ? 2 : 1);
+        int64_t bx = (terms_all + per_block - 1) / per_block;
+        if (bx > (int64_t)num_sms * bps) bx = (int64_t)num_sms * bps;
+        fl.push_back(FastLaunch{k, cw, (int)bx, false, narrow});
+        f_parts += bx;
+    } else if (fast_ok) {
         // Terms per level over all instances: the `counts` recursion of the cost model
         // (src/hafnian.jl:855-884), per instance.
         const int kmax = (int)(Emax < fast_hi / 2 ? Emax : fast_hi / 2);
@@ -852,6 +868,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.lists = (const uint64_t *)(base + off_lst);
     a.list_off = (const int64_t *)(base + off_loff);
     a.list_stride = list_stride;
+    a.all_levels = fused ? 1 : 0;
     a.maxrep = maxrep;
     a.Emax = Ews;
     a.nmax = nmax;

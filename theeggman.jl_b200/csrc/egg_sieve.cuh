@@ -30,7 +30,12 @@ struct SieveArgs {
     const uint64_t *lists;
     const int64_t *list_off;
     int list_stride;
+    // Set for one distinct-row instance of at most kFusedMaxE edges, launched at level k = E: the
+    // launch takes every nonzero edge subset, each on the tile of m = 2E columns.
+    int all_levels;
 };
+
+constexpr int kFusedMaxE = 10;
 
 // Register-tile path (egg_sieve_fast.cuh, egg_sieve_level*.cu): level k evaluates the terms with
 // k surviving edges, m = 2k <= 48 (real) or 32 (complex), for any multiplicities.

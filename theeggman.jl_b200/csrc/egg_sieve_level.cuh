@@ -63,14 +63,15 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
     const int gslot = blockIdx.x * GB + grp;
     const uint64_t W = (uint64_t)a.warps_per_inst * NG;  // groups per instance
     dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
-    // One term: the surviving edges are compacted into w.eidx / w.kval (K of them) by the caller.
-    auto eval_term = [&](double prefac) {
+    // One term: the surviving edges are compacted into w.eidx / w.kval (mE of them, mE = K except
+    // in the all-levels mode) by the caller.
+    auto eval_term = [&](double prefac, int mE) {
         if constexpr (!CPLX) {
-            const double val = term_real<MW, (MW > 32 ? 2 : 1), G>((const double *)a.Ax + in.ax_off, in.lda, E, K, n, w,
+            const double val = term_real<MW, (MW > 32 ? 2 : 1), G>((const double *)a.Ax + in.ax_off, in.lda, E, mE, n, w,
                                                                    gl, gm);
             if (gl == 0) dd_add(acc_re, prefac * val);
         } else {
-            const cd val = term_cplx<MW, G>((const cd *)a.Ax + in.ax_off, in.lda, E, K, n, w, gl, gm);
+            const cd val = term_cplx<MW, G>((const cd *)a.Ax + in.ax_off, in.lda, E, mE, n, w, gl, gm);
             if (gl == 0) {
                 dd_add(acc_re, prefac * val.re);
                 dd_add(acc_im, prefac * val.im);
@@ -84,7 +85,29 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
     };
     // Each round every group first finds its next term, then the warp evaluates them together (the
     // groups of a warp stay converged through the term), until no group of the warp has one left.
-    if (in.subset && K <= E) {
+    if (in.subset && a.all_levels) {
+        // Every nonzero edge subset of the one instance (E <= K): subset r + 1 for r = gslot,
+        // gslot + W, ...; a term of k edges has m = 2k <= MW rows.
+        const uint64_t cnt = ((uint64_t)1 << E) - 1;
+        for (uint64_t r = gslot;; r += W) {
+            const bool has = r < cnt;
+            if (!__any_sync(FULL, has)) break;
+            if (has) {
+                const uint32_t S = (uint32_t)r + 1u;
+                const int k = __popc(S);
+                const double prefac = ((n - k) & 1) ? -1.0 : 1.0;
+                for (int e = gl; e < E; e += G)
+                    if ((S >> e) & 1u) {
+                        const int pos = __popc(S & ((1u << e) - 1u));
+                        w.eidx[pos] = e;
+                        w.kval[pos] = 1.0;
+                    }
+                __syncwarp(gm);
+                eval_term(prefac, k);
+                __syncwarp(gm);
+            }
+        }
+    } else if (in.subset && K <= E) {
         const uint64_t cnt = c_binom[E * 33 + K];
         const uint64_t lo = (uint64_t)gslot * cnt / W, hi = ((uint64_t)gslot + 1) * cnt / W;
         const double prefac = ((n - K) & 1) ? -1.0 : 1.0;  // (-1)^(n - k), every binomial factor 1
@@ -101,7 +124,7 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
                         w.kval[pos] = 1.0;
                     }
                 __syncwarp(gm);
-                eval_term(prefac);
+                eval_term(prefac, K);
                 __syncwarp(gm);
             }
         }
@@ -141,7 +164,7 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
                     w.kval[pos] = (double)kk;
                 }
                 __syncwarp(gm);
-                eval_term(prefac);
+                eval_term(prefac, K);
                 __syncwarp(gm);
             }
         }
@@ -208,7 +231,7 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
             if (!__any_sync(FULL, has)) break;
             if (has) {
                 __syncwarp(gm);
-                eval_term(prefac);
+                eval_term(prefac, K);
                 __syncwarp(gm);
             }
         }
