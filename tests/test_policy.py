@@ -176,3 +176,21 @@ def test_dp_batch_bytes(egg, pol):
     ns, _ = pol._dp_counts(20)
     assert egg.dp_batch_bytes(20, np.complex128, 1) == (ns + 190) * 16
     assert egg.dp_batch_bytes(20, np.complex64, 8) == 8 * (ns + 190) * 8
+
+
+def test_permuted_distinct_is_permuted(egg, W):
+    """The one-gather permutation of the distinct-row sieve equals _permuted(T, A, x) with
+    x = [1, 3, ..., 2, 4, ...] (src/hafnian.jl:786-792, :1140-1145), entry for entry, for row- and
+    column-major inputs that are not symmetric, and comes out column-major."""
+    import importlib
+
+    H = importlib.import_module("theeggman_b200.hafnian")
+    for N in (2, 4, 20, 40):
+        for dt in (np.float64, np.complex128, np.float32):
+            A = np.asarray(W.dense_real(N, 5 + N), dtype=dt)
+            A[0, 1] += 0.25
+            want = H._permuted(np.dtype(dt), A, H._distinct_x(N // 2))
+            for src in (A, np.asfortranarray(A)):
+                got = H._permuted_distinct(np.dtype(dt), src)
+                assert got.dtype == want.dtype and got.flags.f_contiguous
+                assert np.array_equal(got, want)

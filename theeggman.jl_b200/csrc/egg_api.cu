@@ -409,6 +409,22 @@ int egg_plan_release(int K, int idx_bytes)
 
 static size_t state_out_size(int dtype) { return dtype == EGG_I64 ? 16 : dtype_size(dtype); }
 
+// The page-locked staging buffer of small synchronous calls, mapped into the device's address
+// space (pinned_dev), allocated on first use.
+static int ensure_pinned()
+{
+    Context &c = ctx();
+    if (c.pinned) return EGG_OK;
+    EGG_CUDA_TRY(cudaHostAlloc(&c.pinned, Context::kPinnedBytes, cudaHostAllocMapped));
+    cudaError_t e = cudaHostGetDevicePointer(&c.pinned_dev, c.pinned, 0);
+    if (e != cudaSuccess) {
+        cudaFreeHost(c.pinned);
+        c.pinned = nullptr;
+        return fail(EGG_ERR_CUDA, std::string("mapping the staging buffer: ") + cudaGetErrorString(e));
+    }
+    return EGG_OK;
+}
+
 int egg_dp_batch(int K, int idx_bytes, int dtype, int prec, const void *P, int64_t B, int64_t max_batch, void *out)
 {
     EGG_GUARD();
@@ -441,10 +457,8 @@ int egg_dp_batch(int K, int idx_bytes, int dtype, int prec, const void *P, int64
     const size_t in_bytes = (size_t)B * npairs * es, out_bytes = (size_t)B * oes;
     if (chunk == B && in_bytes + out_bytes + 256 <= Context::kPinnedBytes) {
         // A small call: both transfers through the page-locked staging buffer.
-        if (!c.pinned) {
-            EGG_CUDA_TRY(cudaHostAlloc(&c.pinned, Context::kPinnedBytes, cudaHostAllocMapped));
-            EGG_CUDA_TRY(cudaHostGetDevicePointer(&c.pinned_dev, c.pinned, 0));
-        }
+        rc = ensure_pinned();
+        if (rc) return rc;
         char *pin_in = (char *)c.pinned, *pin_out = pin_in + ((in_bytes + 255) / 256) * 256;
         if (B == 1) {
             // One instance of a small degree: its pairs travel in the launch and its value is
@@ -513,6 +527,24 @@ int egg_sieve(int dtype, int prec, const void *Ax, int64_t E, const int64_t *edg
     if (rc) return rc;
     rc = ensure_buf(c.scratch[4], 64);
     if (rc) return rc;
+    if (abytes + 512 <= Context::kPinnedBytes / 2) {
+        // A small call: the matrix and the launch's tables go through the page-locked staging
+        // buffer, and the result is written straight into it (it is mapped), so no copy follows.
+        rc = ensure_pinned();
+        if (rc) return rc;
+        char *pin = (char *)c.pinned;
+        const size_t out_off = Context::kPinnedBytes - 256, stage_off = ((abytes + 255) / 256) * 256;
+        if (abytes) {
+            std::memcpy(pin, Ax, abytes);
+            EGG_CUDA_TRY(cudaMemcpyAsync(c.scratch[3].ptr, pin, abytes, cudaMemcpyHostToDevice, c.stream));
+        }
+        rc = sieve_run(dtype, prec, c.scratch[3].ptr, E, edge_reps, glynn, (char *)c.pinned_dev + out_off, c.stream,
+                       pin + stage_off, out_off - stage_off);
+        if (rc) return rc;
+        EGG_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        std::memcpy(out, pin + out_off, es);
+        return EGG_OK;
+    }
     if (abytes) EGG_CUDA_TRY(cudaMemcpyAsync(c.scratch[3].ptr, Ax, abytes, cudaMemcpyHostToDevice, c.stream));
     rc = sieve_run(dtype, prec, c.scratch[3].ptr, E, edge_reps, glynn, c.scratch[4].ptr, c.stream);
     if (rc) return rc;

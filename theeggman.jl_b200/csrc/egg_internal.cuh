@@ -238,11 +238,14 @@ struct FixedScratch {
     size_t bytes;
     int num_sms;
 };
+// stage (optional, synchronous callers only): page-locked host memory of stage_cap bytes through
+// which the launch's small tables are copied, when they fit.
 int sieve_run(int dtype, int prec, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, void *dout,
-              cudaStream_t st);
+              cudaStream_t st, void *stage = nullptr, size_t stage_cap = 0);
 int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
                     const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st,
-                    const FixedScratch *fixed = nullptr, double *terms = nullptr);
+                    const FixedScratch *fixed = nullptr, double *terms = nullptr, void *stage = nullptr,
+                    size_t stage_cap = 0);
 // One sieve summed as the reference sums it (_sieve_sum, src/hafnian.jl:713-738): every term in the
 // reference's arithmetic, then plain FP64 sums over `nchunks` equal chunks of the term range, each
 // in term order, and the chunk sums left to right.  Host edge_reps, device Ax and out.

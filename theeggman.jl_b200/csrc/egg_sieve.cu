@@ -557,7 +557,7 @@ static int64_t align256(int64_t x) { return (x + 255) & ~(int64_t)255; }
 
 int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
                     const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st,
-                    const FixedScratch *fixed, double *terms)
+                    const FixedScratch *fixed, double *terms, void *stage, size_t stage_cap)
 {
     // terms: instead of summing, store every term of the single instance (exact kernel).
     if (terms && (B != 1 || prec != EGG_PREC_EXACT)) return fail(EGG_ERR_ARGUMENT, "term output needs one instance in exact mode");
@@ -848,15 +848,24 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     {
         // The instance table, reps, strides, binomials and term lists in their device layout, sent
         // as one copy (each copy from pageable memory has a fixed staging cost).
+        // A synchronous caller's page-locked stage takes the image when it fits.
         const size_t img = (size_t)(off_lst + (int64_t)(lists.size() * sizeof(uint64_t)));
-        std::vector<char> h(img, 0);
-        std::memcpy(h.data() + off_inst, inst.data(), inst.size() * sizeof(SieveInst));
-        if (!reps.empty()) std::memcpy(h.data() + off_reps, reps.data(), reps.size() * sizeof(int));
-        if (!strides.empty()) std::memcpy(h.data() + off_str, strides.data(), strides.size() * sizeof(int64_t));
-        std::memcpy(h.data() + off_bin, binoms.data(), binoms.size() * sizeof(double));
-        if (!list_off.empty()) std::memcpy(h.data() + off_loff, list_off.data(), list_off.size() * sizeof(int64_t));
-        if (!lists.empty()) std::memcpy(h.data() + off_lst, lists.data(), lists.size() * sizeof(uint64_t));
-        EGG_CUDA_TRY(cudaMemcpyAsync(base, h.data(), img, cudaMemcpyHostToDevice, st));
+        std::vector<char> hv;
+        char *h;
+        if (stage && img <= stage_cap) {
+            h = (char *)stage;
+            std::memset(h, 0, img);
+        } else {
+            hv.assign(img, 0);
+            h = hv.data();
+        }
+        std::memcpy(h + off_inst, inst.data(), inst.size() * sizeof(SieveInst));
+        if (!reps.empty()) std::memcpy(h + off_reps, reps.data(), reps.size() * sizeof(int));
+        if (!strides.empty()) std::memcpy(h + off_str, strides.data(), strides.size() * sizeof(int64_t));
+        std::memcpy(h + off_bin, binoms.data(), binoms.size() * sizeof(double));
+        if (!list_off.empty()) std::memcpy(h + off_loff, list_off.data(), list_off.size() * sizeof(int64_t));
+        if (!lists.empty()) std::memcpy(h + off_lst, lists.data(), lists.size() * sizeof(uint64_t));
+        EGG_CUDA_TRY(cudaMemcpyAsync(base, h, img, cudaMemcpyHostToDevice, st));
     }
     SieveArgs a;
     a.Ax = dAx;
@@ -944,13 +953,13 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
 }
 
 int sieve_run(int dtype, int prec, const void *dAx, int64_t E, const int64_t *edge_reps, int glynn, void *dout,
-              cudaStream_t st)
+              cudaStream_t st, void *stage, size_t stage_cap)
 {
     int32_t g = glynn ? 1 : 0;
     int64_t e = E;
     std::vector<int64_t> reps(edge_reps, edge_reps + E);
     if (reps.empty()) reps.push_back(0);
-    return sieve_batch_run(dtype, prec, 1, E, dAx, &e, reps.data(), &g, dout, st, nullptr);
+    return sieve_batch_run(dtype, prec, 1, E, dAx, &e, reps.data(), &g, dout, st, nullptr, nullptr, stage, stage_cap);
 }
 
 // ---- the reference's summation ------------------------------------------------------------------

@@ -315,6 +315,24 @@ def _permuted(T, A: np.ndarray, x: list[int]) -> np.ndarray:
     return np.asarray(A)[np.ix_(xi, xi)].astype(T, copy=False)
 
 
+@lru_cache(maxsize=None)
+def _distinct_flat(N: int) -> np.ndarray:
+    """Flat (row-major) indices into an N x N matrix such that A.ravel().take(f).reshape(N, N).T is
+    _permuted(T, A, _distinct_x(N // 2)) in column-major layout: entry (a, b) of the transpose is
+    A[x[b], x[a]].  Cached per degree; read-only."""
+    xi = np.asarray(_distinct_x(N // 2), dtype=np.int64) - 1
+    f = (xi[None, :] * N + xi[:, None]).ravel()
+    f.setflags(write=False)
+    return f
+
+
+def _permuted_distinct(T, A: np.ndarray) -> np.ndarray:
+    """_permuted(T, A, _distinct_x(N / 2)) as one gather, already in the column-major layout the
+    sieve takes."""
+    N = A.shape[0]
+    return A.ravel().take(_distinct_flat(N)).reshape(N, N).T.astype(T, copy=False)
+
+
 def _expanded_indices(rpt, total: int) -> np.ndarray:
     """Row i repeated rpt[i] times, 0-based (src/hafnian.jl:1014-1021)."""
     return np.repeat(np.arange(len(rpt), dtype=np.int64), np.asarray(rpt, dtype=np.int64))
@@ -370,7 +388,7 @@ def hafnian(A, *, nthreads: int | None = None, glynn: bool | None = None, method
         P = _gather_pairs_one(T, A)
         v = _dp_device(T, P, N, _dp_prec(prec), None, exact_int)[0]
         return v if exact_int else T.type(v)
-    return _sieve_one(T, _permuted(T, A, _distinct_x(E)), [1] * E, use_glynn, prec, nthreads)
+    return _sieve_one(T, _permuted_distinct(T, A), [1] * E, use_glynn, prec, nthreads)
 
 
 def hafnian_repeated(A, rpt, *, nthreads: int | None = None, glynn: bool | None = None, method: str = "auto",
