@@ -673,11 +673,14 @@ __global__ void __launch_bounds__(MAXT) dpc_cluster_kernel(const uint32_t *__res
         for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
             const uint32_t *e = ENT + ent_lo[L] + j * (c - 1);
             AT acc = zero_of<AT>();
-            for (int x0 = 0; x0 < c - 1; x0 += kBatch) {
-                HT hv[kBatch];
-                PT pv[kBatch];
+            // A remote read takes about as long as a level's arithmetic, so as many of the state's
+            // children as the registers hold are requested before the first is used.
+            constexpr int kCB = sizeof(HT) <= 8 ? kClusterMaxK - 1 : (kClusterMaxK + 1) / 2;
+            for (int x0 = 0; x0 < c - 1; x0 += kCB) {
+                HT hv[kCB];
+                PT pv[kCB];
 #pragma unroll
-                for (int u = 0; u < kBatch; ++u)
+                for (int u = 0; u < kCB; ++u)
                     if (x0 + u < c - 1) {
                         const uint32_t t = e[x0 + u];
                         const uint32_t child = t >> 8;
@@ -685,7 +688,7 @@ __global__ void __launch_bounds__(MAXT) dpc_cluster_kernel(const uint32_t *__res
                         pv[u] = Ps[t & 255u];
                     }
 #pragma unroll
-                for (int u = 0; u < kBatch; ++u)
+                for (int u = 0; u < kCB; ++u)
                     if (x0 + u < c - 1) acc = madd(Op{}, acc, pv[u], hv[u]);
             }
             HT v;
@@ -904,7 +907,7 @@ static int launch_cluster(const uint32_t *bt, const DevPlan &plan, const PT *P, 
 {
     const int K = plan.K;
     if (K < 4 || K > kClusterMaxK || (int)plan.levels.size() != K / 2 + 1 || !plan.closed_form()) return kNoCluster;
-    constexpr int kMaxT = 1024;
+    constexpr int kMaxT = 512;  // a level holds at most 8008 / 16 states per CTA at N = 22
     auto k = dpc_cluster_kernel<Op, PT, HT, AT, kMaxT>;
     const int64_t maxlev = max_level(plan);
     const int64_t npairs = (int64_t)K * (K - 1) / 2;

@@ -828,6 +828,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     const int64_t off_reps = off; off = align256(off + (int64_t)((reps.size() + 1) * sizeof(int)));
     const int64_t off_str = off; off = align256(off + (int64_t)((strides.size() + 1) * sizeof(int64_t)));
     const int64_t off_bin = off; off = align256(off + (int64_t)(binoms.size() * sizeof(double)));
+    const int64_t off_done = off; off = align256(off + (int64_t)sizeof(unsigned));  // zero in the image
     const int64_t off_loff = off; off = align256(off + (int64_t)((list_off.size() + 1) * sizeof(int64_t)));
     const int64_t off_lst = off; off = align256(off + (int64_t)((lists.size() + 1) * sizeof(uint64_t)));
     const int64_t off_pex = off; off = align256(off + (run_ex ? B * ex_bx * ex_wpb * 2 * (int64_t)sizeof(dd) : 0));
@@ -878,6 +879,8 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.list_off = (const int64_t *)(base + off_loff);
     a.list_stride = list_stride;
     a.all_levels = fused ? 1 : 0;
+    a.fused_out = fused ? dout : nullptr;
+    a.done = (unsigned *)(base + off_done);
     a.maxrep = maxrep;
     a.Emax = Ews;
     a.nmax = nmax;
@@ -941,7 +944,8 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         EGG_CUDA_TRY(cudaEventRecord(c.join_ev[i], c.side[i]));
         EGG_CUDA_TRY(cudaStreamWaitEvent(st, c.join_ev[i], 0));
     }
-    if (terms) {
+    if (terms || fused) {
+        // (The all-levels launch sums its own partials.)
         EGG_CUDA_TRY(cudaGetLastError());
         return EGG_OK;
     }

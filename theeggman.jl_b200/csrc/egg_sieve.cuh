@@ -31,8 +31,12 @@ struct SieveArgs {
     const int64_t *list_off;
     int list_stride;
     // Set for one distinct-row instance of at most kFusedMaxE edges, launched at level k = E: the
-    // launch takes every nonzero edge subset, each on the tile of m = 2E columns.
+    // launch takes every nonzero edge subset, each on the tile of m = 2E columns, and its last
+    // block to finish sums the blocks' partials into fused_out (done counts finished blocks and
+    // starts at zero).
     int all_levels;
+    void *fused_out;
+    unsigned *done;
 };
 
 constexpr int kFusedMaxE = 10;

@@ -254,6 +254,51 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
         out[0] = re;
         out[1] = im;
     }
+    if (a.all_levels) {
+        // The last block to finish sums all blocks' partials in a fixed order (thread t takes
+        // partials t, t + 128, ...; then the warps' lanes pairwise; then the warps in order) and
+        // writes the value, so no reduction launch follows.
+        __shared__ bool last;
+        if (threadIdx.x == 0) {
+            __threadfence();
+            last = atomicAdd(a.done, 1u) == gridDim.x - 1;
+        }
+        __syncthreads();
+        if (last) {
+            __threadfence();
+            dd re{0.0, 0.0}, im{0.0, 0.0};
+            for (unsigned p = threadIdx.x; p < gridDim.x; p += blockDim.x) {
+                const dd *q = partial + (size_t)p * 2;
+                dd_add(re, dd{__ldcg(&q[0].hi), __ldcg(&q[0].lo)});
+                if (CPLX) dd_add(im, dd{__ldcg(&q[1].hi), __ldcg(&q[1].lo)});
+            }
+            const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+            for (int off = 16; off > 0; off >>= 1) {
+                const dd ro{__shfl_down_sync(FULL, re.hi, off), __shfl_down_sync(FULL, re.lo, off)};
+                const dd io{__shfl_down_sync(FULL, im.hi, off), __shfl_down_sync(FULL, im.lo, off)};
+                if (lane < off) {
+                    dd_add(re, ro);
+                    if (CPLX) dd_add(im, io);
+                }
+            }
+            __syncthreads();  // red[] is free again
+            if (lane == 0) {
+                red[2 * wid] = re;
+                red[2 * wid + 1] = im;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                dd fr = red[0], fi = red[1];
+                for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+                    dd_add(fr, red[2 * w]);
+                    if (CPLX) dd_add(fi, red[2 * w + 1]);
+                }
+                const double hr = __dadd_rn(fr.hi, fr.lo);
+                if (CPLX) ((cd *)a.fused_out)[0] = cd{hr, __dadd_rn(fi.hi, fi.lo)};
+                else ((double *)a.fused_out)[0] = hr;
+            }
+        }
+    }
 }
 
 template <bool CPLX, int K, int G>
