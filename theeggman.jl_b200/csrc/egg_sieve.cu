@@ -878,7 +878,6 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.lists = (const uint64_t *)(base + off_lst);
     a.list_off = (const int64_t *)(base + off_loff);
     a.list_stride = list_stride;
-    a.all_levels = fused ? 1 : 0;
     a.fused_out = fused ? dout : nullptr;
     a.done = (unsigned *)(base + off_done);
     a.maxrep = maxrep;
@@ -931,8 +930,12 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             a.warps_per_inst = L.bx * L.cw;
             cudaStream_t ls = st;
             if (side_ok && L.side) ls = c.side[next_side++ % Context::kSideStreams];
-            rc = cplx ? level_launch_cplx(a, dstr, (int)B, L.level, L.narrow, part, L.bx, ls)
-                      : level_launch_real(a, dstr, (int)B, L.level, L.narrow, part, L.bx, ls);
+            if (fused)
+                rc = cplx ? level_launch_all_cplx(a, L.level, L.narrow, part, L.bx, ls)
+                          : level_launch_all_real(a, L.level, L.narrow, part, L.bx, ls);
+            else
+                rc = cplx ? level_launch_cplx(a, dstr, (int)B, L.level, L.narrow, part, L.bx, ls)
+                          : level_launch_real(a, dstr, (int)B, L.level, L.narrow, part, L.bx, ls);
             if (rc) return rc;
             ps.p[slot] = part;
             ps.w[slot] = L.bx;

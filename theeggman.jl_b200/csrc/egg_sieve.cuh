@@ -30,11 +30,8 @@ struct SieveArgs {
     const uint64_t *lists;
     const int64_t *list_off;
     int list_stride;
-    // Set for one distinct-row instance of at most kFusedMaxE edges, launched at level k = E: the
-    // launch takes every nonzero edge subset, each on the tile of m = 2E columns, and its last
-    // block to finish sums the blocks' partials into fused_out (done counts finished blocks and
-    // starts at zero).
-    int all_levels;
+    // The all-levels launch (level_launch_all_*): its last block to finish sums the blocks'
+    // partials into fused_out; done counts finished blocks and starts at zero.
     void *fused_out;
     unsigned *done;
 };
@@ -53,6 +50,11 @@ int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, 
                       cudaStream_t st);
 int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
                          cudaStream_t st);
+// One distinct-row instance (B = 1) of k <= kFusedMaxE edges in one launch: every nonzero edge
+// subset, each on the tile of m = 2k columns, the blocks' partials summed inside the launch into
+// a.fused_out.  A separate instantiation of the level kernel, so the level launches are unchanged.
+int level_launch_all_real(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st);
+int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st);
 int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
                       cudaStream_t st);
 // The level's block size in warps and how many of its blocks one SM holds.

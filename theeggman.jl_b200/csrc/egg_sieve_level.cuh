@@ -44,7 +44,9 @@ constexpr int level_group(bool narrow)
     return (narrow && 2 * K <= 16) ? 16 : 32;
 }
 
-template <bool CPLX, int K, int G>
+// ALL: the all-levels mode of one small distinct-row instance (level_launch_all_*), a separate
+// instantiation.
+template <bool CPLX, int K, int G, bool ALL = false>
 __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CPLX, K, G>::min_blocks)
     sieve_level_kernel(SieveArgs a, const int64_t *__restrict__ strides, dd *partial)
 {
@@ -67,11 +69,11 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
     // in the all-levels mode) by the caller.
     auto eval_term = [&](double prefac, int mE) {
         if constexpr (!CPLX) {
-            const double val = term_real<MW, (MW > 32 ? 2 : 1), G>((const double *)a.Ax + in.ax_off, in.lda, E, mE, n, w,
-                                                                   gl, gm);
+            const double val = term_real<MW, (MW > 32 ? 2 : 1), G>((const double *)a.Ax + in.ax_off, in.lda, E,
+                                                                   ALL ? mE : K, n, w, gl, gm);
             if (gl == 0) dd_add(acc_re, prefac * val);
         } else {
-            const cd val = term_cplx<MW, G>((const cd *)a.Ax + in.ax_off, in.lda, E, mE, n, w, gl, gm);
+            const cd val = term_cplx<MW, G>((const cd *)a.Ax + in.ax_off, in.lda, E, ALL ? mE : K, n, w, gl, gm);
             if (gl == 0) {
                 dd_add(acc_re, prefac * val.re);
                 dd_add(acc_im, prefac * val.im);
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
     };
     // Each round every group first finds its next term, then the warp evaluates them together (the
     // groups of a warp stay converged through the term), until no group of the warp has one left.
-    if (in.subset && a.all_levels) {
+    if constexpr (ALL) {
         // Every nonzero edge subset of the one instance (E <= K): subset r + 1 for r = gslot,
         // gslot + W, ...; a term of k edges has m = 2k <= MW rows.
         const uint64_t cnt = ((uint64_t)1 << E) - 1;
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
         out[0] = re;
         out[1] = im;
     }
-    if (a.all_levels) {
+    if constexpr (ALL) {
         // The last block to finish sums all blocks' partials in a fixed order (thread t takes
         // partials t, t + 128, ...; then the warps' lanes pairwise; then the warps in order) and
         // writes the value, so no reduction launch follows.
@@ -316,6 +318,20 @@ static int level_launch_k(const SieveArgs &a, const int64_t *strides, int B, dd 
 }
 
 template <bool CPLX, int K, int G>
+static int level_launch_all_k(const SieveArgs &a, dd *partial, int blocks_x, cudaStream_t st)
+{
+    constexpr int cw = LevelShape<CPLX, K>::threads / 32;
+    const size_t smem = (size_t)cw * (32 / G) * fast_ws_doubles(a.nmax, CPLX, 2 * K) * sizeof(double);
+    auto k = sieve_level_kernel<CPLX, K, G, true>;
+    int rc = smem_limit_at_least((const void *)k, smem);
+    if (rc) return rc;
+    k<<<dim3((unsigned)blocks_x, 1u), cw * 32, smem, st>>>(a, nullptr, partial);
+    count_launch();
+    EGG_CUDA_TRY(cudaGetLastError());
+    return EGG_OK;
+}
+
+template <bool CPLX, int K, int G>
 static int level_shape_k(int nmax, int *warps_per_block, int *blocks_per_sm)
 {
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
@@ -336,5 +352,13 @@ static int level_shape_k(int nmax, int *warps_per_block, int *blocks_per_sm)
 #define EGG_LEVEL_CASES(CPLX, X)                                                                   \
     X(CPLX, 1) X(CPLX, 2) X(CPLX, 3) X(CPLX, 4) X(CPLX, 5) X(CPLX, 6) X(CPLX, 7) X(CPLX, 8) X(CPLX, 9) \
     X(CPLX, 10) X(CPLX, 11) X(CPLX, 12) X(CPLX, 13) X(CPLX, 14) X(CPLX, 15) X(CPLX, 16)
+// Case K of a switch over the all-levels launches (groups as for the level launch).
+#define EGG_ALL_LAUNCH(CPLX, K)                                                                      \
+    case K:                                                                                          \
+        return narrow ? level_launch_all_k<CPLX, K, level_group<K>(true)>(a, partial, blocks_x, st)  \
+                      : level_launch_all_k<CPLX, K, 32>(a, partial, blocks_x, st);
+#define EGG_FUSED_CASES(CPLX, X)                                                                    \
+    X(CPLX, 1) X(CPLX, 2) X(CPLX, 3) X(CPLX, 4) X(CPLX, 5) X(CPLX, 6) X(CPLX, 7) X(CPLX, 8) X(CPLX, 9) \
+    X(CPLX, 10)
 #define EGG_LEVEL_CASES_HI(CPLX, X)                                                                 \
     X(CPLX, 17) X(CPLX, 18) X(CPLX, 19) X(CPLX, 20) X(CPLX, 21) X(CPLX, 22) X(CPLX, 23) X(CPLX, 24)

@@ -27,6 +27,17 @@ int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, 
     return fail(EGG_ERR_ARGUMENT, "no such sieve level");
 }
 
+int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st)
+{
+    static_assert(kFusedMaxE == 10, "EGG_FUSED_CASES lists the levels 1..kFusedMaxE");
+    int rc = upload_fast_tables_once(st);
+    if (rc) return rc;
+    switch (k) {
+        EGG_FUSED_CASES(true, EGG_ALL_LAUNCH)
+    }
+    return fail(EGG_ERR_ARGUMENT, "no all-levels sieve launch for this edge count");
+}
+
 int level_shape_cplx(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm)
 {
     static std::mutex mu;  // the entry point that allocates nothing reaches this without the library's lock
