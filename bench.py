@@ -60,7 +60,7 @@ def measured_peaks() -> dict:
 # The committed ncu summary (kernel and workload) whose DRAM traffic figure belongs to a workload.
 PROFILE_OF = {"sieve40": "sieve_level_kernel_sieve40.md", "sieve40c": "sieve_level_kernel_sieve40c.md",
               "sieve40g": "sieve_level_kernel_sieve40g.md", "rep14": "sieve_level_kernel_rep14.md",
-              "dp40": "dpc_fixed_kernel_dp40.md"}
+              "dp40": "dpc_fixed_kernel_dp40.md", "dp20": "dpc_cluster_kernel_dp20.md"}
 
 
 def profile_traffic(name: str):
