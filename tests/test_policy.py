@@ -194,3 +194,21 @@ def test_permuted_distinct_is_permuted(egg, W):
                 got = H._permuted_distinct(np.dtype(dt), src)
                 assert got.dtype == want.dtype and got.flags.f_contiguous
                 assert np.array_equal(got, want)
+
+
+def test_gather_pairs_one_is_pair_order(egg, W):
+    """The single-matrix pair gather takes P[q] = A[i, j] for q = _pair_index(i, j, K) in the
+    row-major upper triangle (src/unrolled.jl:60, src/dp.jl:452-477), for row- and column-major
+    inputs that are not symmetric, in the requested element type."""
+    import importlib
+
+    H = importlib.import_module("theeggman_b200.hafnian")
+    for K in (2, 4, 20, 33):
+        A = np.asarray(W.dense_real(K, 70 + K))
+        A[1, 0] += 0.5
+        want = np.array([A[i, j] for i in range(K) for j in range(i + 1, K)])
+        for src in (A, np.asfortranarray(A)):
+            for T in (np.float64, np.complex128, np.float32):
+                got = H._gather_pairs_one(np.dtype(T), src)
+                assert got.shape == (1, K * (K - 1) // 2) and got.dtype == np.dtype(T)
+                assert np.array_equal(got[0], want.astype(T))

@@ -58,6 +58,8 @@ def _dp_plan(K: int, idx_bytes: int | None = None) -> tuple[int, int]:
     """
     ib = pol._dp_index_bytes(K) if idx_bytes is None else idx_bytes
     key = (K, ib)
+    if key in _resident:
+        return key
     with _lock:
         if key not in _resident:
             nat.check(nat.lib().egg_plan_build(K, ib))
@@ -175,10 +177,18 @@ def _triu_pairs(K: int) -> tuple[np.ndarray, np.ndarray]:
     return iu, ju
 
 
+@lru_cache(maxsize=None)
+def _triu_flat(K: int) -> np.ndarray:
+    """Row-major flat indices i * K + j of the pairs, in _pair_index order.  Cached; read-only."""
+    iu, ju = _triu_pairs(K)
+    f = iu * K + ju
+    f.setflags(write=False)
+    return f
+
+
 def _gather_pairs_one(T: np.dtype, A: np.ndarray) -> np.ndarray:
-    """The 1 x npairs P of a single K x K matrix (the rows taken in order)."""
-    iu, ju = _triu_pairs(A.shape[0])
-    return A[iu, ju].astype(T, copy=False).reshape(1, -1)
+    """The 1 x npairs P of a single K x K matrix (the rows taken in order), as one gather."""
+    return A.ravel().take(_triu_flat(A.shape[0])).astype(T, copy=False).reshape(1, -1)
 
 
 def _gather_pairs_batch(T: np.dtype, mats: np.ndarray, idxs: np.ndarray, K: int) -> np.ndarray:
