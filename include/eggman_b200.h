@@ -11,7 +11,10 @@
  *   - Matrices are column-major (Julia order); complex values are interleaved (re, im) pairs of
  *     the real type, exactly as Julia lays out Complex{Float64}/Complex{Float32}.
  *   - One device context per process and one internal lock, mirroring the reference's
- *     _DEVICE_PLAN_LOCK (src/dp.jl:542): calls are serialised and synchronous to the caller.
+ *     _DEVICE_PLAN_LOCK (src/dp.jl:542): calls are serialised, and the host-pointer calls are
+ *     synchronous to the caller.  The _device calls return once their work is enqueued; it uses
+ *     the library's own work buffers, so _device calls whose work could run on the GPU at the
+ *     same time (different streams, not ordered by events) race.
  *   - The library never falls back to a CPU implementation.
  */
 #ifndef EGGMAN_B200_H
