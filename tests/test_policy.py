@@ -212,3 +212,46 @@ def test_gather_pairs_one_is_pair_order(egg, W):
                 got = H._gather_pairs_one(np.dtype(T), src)
                 assert got.shape == (1, K * (K - 1) // 2) and got.dtype == np.dtype(T)
                 assert np.array_equal(got[0], want.astype(T))
+
+
+def test_sieve_batch_pack_layout(egg, W):
+    """The batched sieve's host packing: instance b's matrix column-major in the leading 2E_b block
+    of slab[b], its multiplicities zero-padded, its variant as 0/1.  Checked against a plain
+    element-by-element packing for one-size batches (whose stacking buffers are reused: two calls
+    in a row with different matrices) and for mixed sizes, real and complex, with inputs that are
+    not symmetric and of either memory order."""
+    import importlib
+
+    H = importlib.import_module("theeggman_b200.hafnian")
+    rng = np.random.default_rng(11)
+
+    def plain(CT, Axs, reps_list, glynns):
+        B = len(Axs)
+        Emax = max((len(r) for r in reps_list), default=0)
+        lda = max(2 * Emax, 1)
+        slab = np.zeros((B, lda, lda), CT)
+        reps = np.zeros((B, max(Emax, 1)), np.int64)
+        for b, (A, r) in enumerate(zip(Axs, reps_list)):
+            m = 2 * len(r)
+            for i in range(m):
+                for j in range(m):
+                    slab[b].reshape(-1)[i + j * lda] = A[i, j]  # column-major within the block
+            reps[b, : len(r)] = r
+        return slab, np.array([len(r) for r in reps_list], np.int64), reps, \
+            np.array([1 if x else 0 for x in glynns], np.int32), Emax
+
+    for CT in (np.float64, np.complex128):
+        for sizes in ([3, 3, 3, 3], [3, 3, 3, 3], [1, 4, 2, 4, 0]):
+            Axs, reps_list, glynns = [], [], []
+            for k, E in enumerate(sizes):
+                A = rng.standard_normal((2 * E, 2 * E)).astype(CT)
+                if CT is np.complex128:
+                    A = A + 1j * rng.standard_normal((2 * E, 2 * E))
+                Axs.append(np.asfortranarray(A) if k % 2 else A)
+                reps_list.append(list(rng.integers(1, 4, size=E)))
+                glynns.append(bool(k % 2))
+            got = H._sieve_batch_pack(CT, Axs, reps_list, glynns)
+            want = plain(CT, Axs, reps_list, glynns)
+            assert got[4] == want[4]
+            for a, b in zip(got[:4], want[:4]):
+                assert a.dtype == b.dtype and a.shape == b.shape and np.array_equal(a, b)

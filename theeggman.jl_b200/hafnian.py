@@ -244,30 +244,50 @@ def _sieve_prec(prec) -> int:
     return nat.PREC["exact"] if prec in ("exact", "reference") else nat.PREC["fma"]
 
 
+# The last equal-size batch shape's stacking buffers, reused (under _lock) so that a batch does not
+# pay for fresh pages on every call.
+_slab_bufs: dict = {}
+
+
+def _sieve_batch_pack(CT, Axs: list, reps_list: list, glynns: list):
+    """(slab, E, reps, glynn, Emax) of one egg_sieve_batch call: slab[b] holds instance b's matrix
+    column-major in its leading 2E_b x 2E_b block, reps[b] its multiplicities (zero-padded).  For
+    a batch of one size the slab is a reused buffer: call under _lock and use it before releasing."""
+    B = len(Axs)
+    lens = list(map(len, reps_list))
+    E = np.array(lens, dtype=np.int64)
+    Emax = max(lens) if B else 0
+    g = np.array([1 if x else 0 for x in glynns], dtype=np.int32)
+    if B and Emax and min(lens) == Emax:
+        # Every instance the same size (a batch of one pattern): one stack, one transposing copy.
+        m = 2 * Emax
+        key = (B, m, np.dtype(CT))
+        bufs = _slab_bufs.get(key)
+        if bufs is None:
+            _slab_bufs.clear()
+            bufs = (np.empty((B, m, m), CT), np.empty((B, m, m), CT))
+            _slab_bufs[key] = bufs
+        np.stack(Axs, out=bufs[0])
+        np.copyto(bufs[1], bufs[0].transpose(0, 2, 1))
+        return bufs[1], E, np.array(reps_list, dtype=np.int64).reshape(B, Emax), g, Emax
+    lda = max(2 * Emax, 1)
+    slab = np.zeros((B, lda, lda), dtype=CT)  # per instance: column-major leading block
+    for b, (Ax, r) in enumerate(zip(Axs, reps_list)):
+        m = 2 * len(r)
+        if m:
+            slab[b, :m, :m] = np.asarray(Ax, dtype=CT).T  # store transposed so memory is column-major
+    reps = np.zeros((B, max(Emax, 1)), dtype=np.int64)
+    for b, r in enumerate(reps_list):
+        reps[b, : len(r)] = r
+    return slab, E, reps, g, Emax
+
+
 def _sieve_device_batch(T: np.dtype, Axs: list[np.ndarray], reps_list: list[list[int]], glynns: list[bool],
                         prec=None) -> np.ndarray:
     """One egg_sieve_batch call over instances of possibly different edge counts."""
     B = len(Axs)
     cplx = np.dtype(T).kind == "c"
     CT = np.complex128 if cplx else np.float64
-    E = np.fromiter((len(r) for r in reps_list), dtype=np.int64, count=B)
-    Emax = int(E.max()) if B else 0
-    lda = max(2 * Emax, 1)
-    if B and Emax and int(E.min()) == Emax:
-        # Every instance the same size (a batch of one pattern): one stacked transpose, so each
-        # instance's block is column-major.
-        slab = np.ascontiguousarray(np.stack([np.asarray(a) for a in Axs]).astype(CT, copy=False).transpose(0, 2, 1))
-        reps = np.array(reps_list, dtype=np.int64).reshape(B, Emax)
-    else:
-        slab = np.zeros((B, lda, lda), dtype=CT)  # per instance: column-major leading block
-        for b, (Ax, r) in enumerate(zip(Axs, reps_list)):
-            m = 2 * len(r)
-            if m:
-                slab[b, :m, :m] = np.asarray(Ax, dtype=CT).T  # store transposed so memory is column-major
-        reps = np.zeros((B, max(Emax, 1)), dtype=np.int64)
-        for b, r in enumerate(reps_list):
-            reps[b, : len(r)] = r
-    g = np.fromiter((1 if x else 0 for x in glynns), dtype=np.int32, count=B)
     if prec == "reference":
         # The reference's batch loop runs each instance with nthreads = 1, i.e. one chunk
         # (src/hafnian.jl:1297-1300, :1355-1358).
@@ -275,6 +295,7 @@ def _sieve_device_batch(T: np.dtype, Axs: list[np.ndarray], reps_list: list[list
                         dtype=T)
     out = np.zeros(B, CT)
     with _lock:
+        slab, E, reps, g, Emax = _sieve_batch_pack(CT, Axs, reps_list, glynns)
         nat.check(nat.lib().egg_sieve_batch(nat.EGG_C128 if cplx else nat.EGG_F64, _sieve_prec(prec), B, Emax, nat.ptr(slab),
                                             nat.ptr(E), nat.ptr(reps), nat.ptr(g), nat.ptr(out)))
     return out.astype(T, copy=False)
