@@ -255,3 +255,20 @@ def test_sieve_batch_pack_layout(egg, W):
             assert got[4] == want[4]
             for a, b in zip(got[:4], want[:4]):
                 assert a.dtype == b.dtype and a.shape == b.shape and np.array_equal(a, b)
+
+
+def test_gather_pairs_stack_equals_batch_gather(egg, W):
+    """The all-rows pair gather of a (B, K, K) stack equals the general gather of
+    _gather_pairs_batch (src/dp.jl:479-512) with every instance's rows in order, entry for entry,
+    in the column-major layout (instance index fastest), for real, complex and integer inputs."""
+    import importlib
+
+    H = importlib.import_module("theeggman_b200.hafnian")
+    rng = np.random.default_rng(5)
+    for K in (2, 6, 20):
+        for dt in (np.float64, np.complex128, np.int64):
+            S = rng.integers(-9, 9, size=(7, K, K)).astype(dt)
+            want = H._gather_pairs_batch(np.dtype(dt), S, np.tile(np.arange(K), (7, 1)), K)
+            got = H._gather_pairs_stack(np.dtype(dt), S)
+            assert got.dtype == want.dtype and got.flags.f_contiguous
+            assert np.array_equal(got, want)

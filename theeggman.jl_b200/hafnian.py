@@ -119,13 +119,17 @@ def dp_batch_bytes(N: int, T, B: int) -> int:
 
 def _haf_dtype(A: np.ndarray) -> np.dtype:
     """float(eltype(A)) (src/hafnian.jl:744): integers and bools promote to Float64."""
-    if A.dtype.kind in "iub":
+    return _haf_dtype_of(A.dtype)
+
+
+def _haf_dtype_of(dt: np.dtype) -> np.dtype:
+    if dt.kind in "iub":
         return np.dtype(np.float64)
-    if A.dtype in (np.float16,):
+    if dt in (np.float16,):
         return np.dtype(np.float32)
-    if A.dtype not in (np.float64, np.float32, np.complex128, np.complex64):
-        raise ArgumentError(f"unsupported element type {A.dtype}")
-    return A.dtype
+    if dt not in (np.float64, np.float32, np.complex128, np.complex64):
+        raise ArgumentError(f"unsupported element type {dt}")
+    return dt
 
 
 def _checksquare(A: np.ndarray) -> int:
@@ -189,6 +193,14 @@ def _triu_flat(K: int) -> np.ndarray:
 def _gather_pairs_one(T: np.dtype, A: np.ndarray) -> np.ndarray:
     """The 1 x npairs P of a single K x K matrix (the rows taken in order), as one gather."""
     return A.ravel().take(_triu_flat(A.shape[0])).astype(T, copy=False).reshape(1, -1)
+
+
+def _gather_pairs_stack(T: np.dtype, stack: np.ndarray) -> np.ndarray:
+    """P[b, q] = A_b[i, j] for q = _pair_index(i, j, K) of a C-contiguous (B, K, K) stack, every row
+    taken in order, column-major (instance index fastest): one gather of the pairs' rows of the
+    transposed stack."""
+    B, K = stack.shape[0], stack.shape[1]
+    return stack.reshape(B, K * K).T[_triu_flat(K)].T.astype(T, copy=False)
 
 
 def _gather_pairs_batch(T: np.dtype, mats: np.ndarray, idxs: np.ndarray, K: int) -> np.ndarray:
@@ -469,15 +481,17 @@ def _hafnian_batch(As, *, nthreads, glynn, method, check_symmetric, backend, max
     B = len(mats)
     if B == 0:
         return np.zeros(0, dtype=np.float64)
-    exact_int = exact and all(m.dtype.kind in "iub" for m in mats)
-    T = np.dtype(np.int64) if exact_int else np.result_type(*[_haf_dtype(m) for m in mats])
+    dtypes = {m.dtype for m in mats}
+    exact_int = exact and all(d.kind in "iub" for d in dtypes)
+    T = np.dtype(np.int64) if exact_int else np.result_type(*[_haf_dtype_of(d) for d in dtypes])
     N = _checksquare(mats[0])
-    for b, m in enumerate(mats):
-        if _checksquare(m) != N:
-            raise DimensionMismatch(f"matrix {b + 1} is {m.shape[0]}×{m.shape[1]}, expected {N}×{N}; a batch shares "
-                                    "one strategy and one plan")
-        if check_symmetric:
-            _check_symmetric(m)
+    if check_symmetric or len({m.shape for m in mats}) > 1:
+        for b, m in enumerate(mats):
+            if _checksquare(m) != N:
+                raise DimensionMismatch(f"matrix {b + 1} is {m.shape[0]}×{m.shape[1]}, expected {N}×{N}; a batch "
+                                        "shares one strategy and one plan")
+            if check_symmetric:
+                _check_symmetric(m)
     if N == 0:
         return [1] * B if exact_int else np.ones(B, T)
     if N % 2:
@@ -491,10 +505,8 @@ def _hafnian_batch(As, *, nthreads, glynn, method, check_symmetric, backend, max
         # Without a backend the reference loops over hafnian(As[b]; nthreads=1, ...) (:1297-1300);
         # every instance has the same size, so they all choose alike.
         chosen = pol._choose_method_distinct(N, N // 2, 1)[0] if method == "auto" else method
-    stack = np.stack(mats)
     if chosen in ("unrolled", "dp"):
-        idxs = np.tile(np.arange(N, dtype=np.int64), (B, 1))
-        P = _gather_pairs_batch(T, stack, idxs, N)
+        P = _gather_pairs_stack(T, np.stack(mats))
         return _dp_device(T, P, N, _dp_prec(prec), max_batch, exact_int)
     if exact_int:
         raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
