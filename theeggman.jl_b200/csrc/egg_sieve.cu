@@ -14,7 +14,8 @@
 // or, for distinct-row inclusion-exclusion, as equal shares of each popcount level.  The fast
 // register-tile kernels (egg_sieve_fast.cuh, egg_sieve_level*.cu) take every term that fits their
 // tiles unless the exact mode is asked for; this driver launches both and the fixed-order
-// reduction.
+// reduction.  One small distinct-row instance instead takes a single all-levels launch of the
+// register-tile kernel, which sums its own blocks' partials in a fixed order.
 #include <cmath>
 #include <cstring>
 #include <map>
