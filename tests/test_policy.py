@@ -272,3 +272,42 @@ def test_gather_pairs_stack_equals_batch_gather(egg, W):
             got = H._gather_pairs_stack(np.dtype(dt), S)
             assert got.dtype == want.dtype and got.flags.f_contiguous
             assert np.array_equal(got, want)
+
+
+def test_repeated_batch_equal_patterns(egg, W, monkeypatch):
+    """hafnian_repeated(A, rpts) evaluates each distinct pattern once and gives its value to every
+    instance with that pattern, in order; distinct patterns keep the per-pattern strategy choice of
+    the reference's loop (src/hafnian.jl:1355-1358).  The device calls are replaced by stand-ins
+    whose value identifies the instance they were given, so the mapping is checked without a GPU."""
+    import importlib
+
+    H = importlib.import_module("theeggman_b200.hafnian")
+    pol = importlib.import_module("theeggman_b200.policy")
+
+    seen = []
+
+    def fake_sieve(T, Axs, reps_list, glynns, prec=None):
+        seen.extend(tuple(r) for r in reps_list)
+        return np.array([float(np.sum(np.abs(a))) * 1000 + sum(r) + 0.5 * bool(g)
+                         for a, r, g in zip(Axs, reps_list, glynns)], dtype=T)
+
+    def fake_dp(T, P, K, prec, max_batch, exact_int):
+        seen.extend(range(np.asarray(P).shape[0]))
+        return np.array([float(np.sum(np.abs(p))) for p in np.asarray(P)], dtype=T)
+
+    monkeypatch.setattr(H, "_sieve_device_batch", fake_sieve)
+    monkeypatch.setattr(H, "_dp_device", fake_dp)
+    A = W.dense_real(8, 17)
+    pats = [[2, 2, 2, 2, 0, 0, 0, 0], [1, 1, 1, 1, 1, 1, 1, 1], [3, 1, 2, 0, 2, 0, 0, 0], [4, 4, 0, 0, 0, 0, 0, 0]]
+    for method in ("auto", "sieve", "dp"):
+        rpts = [pats[i] for i in (2, 0, 0, 3, 1, 2, 2, 0)]
+        seen.clear()
+        got = H.hafnian_repeated(A, rpts, method=method)
+        assert len(seen) == len(pats)  # one evaluation per distinct pattern
+        assert len(got) == len(rpts)
+        for b, i in enumerate((2, 0, 0, 3, 1, 2, 2, 0)):
+            want = H._hafnian_repeated_batch(A, [pats[i]], nthreads=None, glynn=None, method=method,
+                                             check_symmetric=True, backend=None, max_batch=None, prec=None,
+                                             exact=False)[0]
+            assert got[b] == want, (method, b)
+    assert pol.matched_reps([2, 2, 2, 2, 0, 0, 0, 0]) == tuple(map(list, H._pattern_choice((2, 2, 2, 2, 0, 0, 0, 0), 8)[:2]))

@@ -516,6 +516,16 @@ def _hafnian_batch(As, *, nthreads, glynn, method, check_symmetric, backend, max
     return _sieve_device_batch(T, [_permuted(T, m, x) for m in mats], [[1] * (N // 2)] * B, [use_glynn] * B, prec)
 
 
+@lru_cache(maxsize=4096)
+def _pattern_choice(rp: tuple, total: int):
+    """(x, edge_reps, method, glynn) of one multiplicity pattern: matched_reps (src/hafnian.jl:142-188)
+    and the per-pattern choice of the reference's batch loop, _choose_method(total, edge_reps; nthreads
+    = 1) (:1355-1358).  Both depend on the pattern alone, so they are cached."""
+    x, er = pol.matched_reps(list(rp))
+    sel, sg = pol._choose_method(total, er, 1)
+    return tuple(x), tuple(er), sel, sg  # shared by every caller: immutable
+
+
 def _hafnian_repeated_batch(A, rpts, *, nthreads, glynn, method, check_symmetric, backend, max_batch, prec, exact):
     A = np.asarray(A)
     B = len(rpts)
@@ -541,6 +551,15 @@ def _hafnian_repeated_batch(A, rpts, *, nthreads, glynn, method, check_symmetric
     if total % 2:
         return [0] * B if exact_int else np.zeros(B, T)
     pol._check_method(method, total)
+    # Equal patterns over the one matrix are equal instances: each distinct pattern is evaluated
+    # once (as its own scalar call would be) and its value given to every instance that has it.
+    slot = {}
+    order = [slot.setdefault(tuple(rp), len(slot)) for rp in rpts]
+    if len(slot) < B:
+        uniq = [list(k) for k in slot]
+        vals = _hafnian_repeated_batch(A, uniq, nthreads=nthreads, glynn=glynn, method=method, check_symmetric=False,
+                                       backend=backend, max_batch=max_batch, prec=prec, exact=exact)
+        return [vals[i] for i in order] if exact_int else np.asarray(vals)[order]
     if backend is not None and method in ("auto", "dp") and total <= pol.DP_HARD_MAX:
         idxs = np.stack([_expanded_indices(rp, total) for rp in rpts])
         P = _gather_pairs_batch(T, A, idxs, total)
@@ -550,8 +569,7 @@ def _hafnian_repeated_batch(A, rpts, *, nthreads, glynn, method, check_symmetric
     out = [None] * B
     dp_idx, sv_idx, sv_ax, sv_reps, sv_g = [], [], [], [], []
     for b, rp in enumerate(rpts):
-        x, er = pol.matched_reps(rp)
-        sel, sg = pol._choose_method(total, er, 1)
+        x, er, sel, sg = _pattern_choice(tuple(rp), total)
         chosen = sel if method == "auto" else method
         if chosen != "sieve":
             dp_idx.append(b)
