@@ -311,3 +311,38 @@ def test_repeated_batch_equal_patterns(egg, W, monkeypatch):
                                              exact=False)[0]
             assert got[b] == want, (method, b)
     assert pol.matched_reps([2, 2, 2, 2, 0, 0, 0, 0]) == tuple(map(list, H._pattern_choice((2, 2, 2, 2, 0, 0, 0, 0), 8)[:2]))
+
+
+def test_scalar_sieve_marshalling(egg, W, monkeypatch):
+    """A scalar sieve call hands the C ABI its matrix (column-major), its multiplicities (cached per
+    pattern) and a result buffer (reused), and returns what the library writes there, in the
+    input's type.  A stand-in for egg_sieve reads the arguments through their addresses and writes
+    a value that depends on them, so the plumbing is checked without a GPU."""
+    import ctypes
+    import importlib
+
+    H = importlib.import_module("theeggman_b200.hafnian")
+    nat = importlib.import_module("theeggman_b200._native")
+
+    class Stub:
+        def egg_sieve(self, dtype, prec, ax, E, reps, glynn, out):
+            r = np.ctypeslib.as_array((ctypes.c_int64 * max(E, 1)).from_address(reps))
+            cplx = dtype == nat.EGG_C128
+            n = 2 * E
+            vals = np.ctypeslib.as_array((ctypes.c_double * (n * n * (2 if cplx else 1))).from_address(ax)) if E else []
+            v = float(np.sum(r[:E]) * 1000 + np.sum(vals) + 7 * glynn)
+            (ctypes.c_double * 2).from_address(out)[0] = v
+            if cplx:
+                (ctypes.c_double * 2).from_address(out)[1] = -v
+            return 0
+
+    monkeypatch.setattr(nat, "lib", lambda: Stub())
+    for dt in (np.float64, np.complex128):
+        for reps in ([1, 2, 3], [2, 2], [1, 2, 3]):
+            E = len(reps)
+            Ax = np.arange(4 * E * E, dtype=np.float64).reshape(2 * E, 2 * E).astype(dt)
+            for glynn in (False, True):
+                got = H._sieve_one(np.dtype(dt), Ax, reps, glynn)
+                v = sum(reps) * 1000 + float(np.sum(Ax.view(np.float64))) + 7 * glynn
+                want = complex(v, -v) if dt is np.complex128 else v
+                assert type(got) is np.dtype(dt).type and got == want

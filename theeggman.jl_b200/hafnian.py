@@ -323,12 +323,34 @@ def _sieve_one(T: np.dtype, Ax: np.ndarray, edge_reps: list[int], glynn: bool, p
     CT = np.complex128 if cplx else np.float64
     E = len(edge_reps)
     A = np.asfortranarray(np.asarray(Ax, dtype=CT))
-    reps = np.ascontiguousarray(edge_reps if E else [0], dtype=np.int64)
-    out = np.zeros(1, CT)
+    reps_ptr = _reps_array(tuple(edge_reps))[1]
     with _lock:
+        out, out_ptr = _one_out(CT)
         nat.check(nat.lib().egg_sieve(nat.EGG_C128 if cplx else nat.EGG_F64, _sieve_prec(prec), nat.ptr(A) if E else None, E,
-                                      nat.ptr(reps), 1 if glynn else 0, nat.ptr(out)))
-    return np.dtype(T).type(out[0])
+                                      reps_ptr, 1 if glynn else 0, out_ptr))
+        v = out[0]
+    return np.dtype(T).type(v)
+
+
+@lru_cache(maxsize=256)
+def _reps_array(reps: tuple):
+    """(array, address) of a multiplicity pattern as the C ABI takes it (Int64; one zero for an
+    empty pattern).  Cached per pattern; read-only."""
+    a = np.array(reps if reps else (0,), dtype=np.int64)
+    a.setflags(write=False)
+    return a, a.ctypes.data
+
+
+_one_outs: dict = {}
+
+
+def _one_out(CT):
+    """(array, address) of the one-value result buffer of a scalar call, per type; use under _lock."""
+    r = _one_outs.get(CT)
+    if r is None:
+        a = np.zeros(1, CT)
+        r = _one_outs[CT] = (a, a.ctypes.data)
+    return r
 
 
 def _sieve_reference(T: np.dtype, Ax: np.ndarray, edge_reps: list[int], glynn: bool, nthreads: int):
