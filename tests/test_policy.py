@@ -346,3 +346,50 @@ def test_scalar_sieve_marshalling(egg, W, monkeypatch):
                 v = sum(reps) * 1000 + float(np.sum(Ax.view(np.float64))) + 7 * glynn
                 want = complex(v, -v) if dt is np.complex128 else v
                 assert type(got) is np.dtype(dt).type and got == want
+
+
+def test_scalar_dp_marshalling(egg, W, monkeypatch):
+    """A scalar DP call hands egg_dp_batch the pairs of _pair_index order with B = 1 and returns the
+    value the library writes into the (reused) result buffer, in the input's type; exact integer
+    calls read back a two's-complement Int128.  A stand-in for the library reads the pairs through
+    their address, so the plumbing is checked without a GPU."""
+    import ctypes
+    import importlib
+
+    H = importlib.import_module("theeggman_b200.hafnian")
+    nat = importlib.import_module("theeggman_b200._native")
+    monkeypatch.setattr(H, "_resident", set())
+
+    class Stub:
+        def egg_plan_build(self, K, ib):
+            return 0
+
+        def egg_dp_batch(self, K, ib, dtype, prec, P, B, max_batch, out):
+            assert B == 1 and max_batch == 0
+            npairs = K * (K - 1) // 2
+            if dtype == nat.EGG_I64:
+                p = np.ctypeslib.as_array((ctypes.c_int64 * npairs).from_address(P))
+                v = -int(np.sum(p * np.arange(1, npairs + 1))) - (1 << 70)  # negative, beyond Int64
+                u = v & ((1 << 128) - 1)
+                o = (ctypes.c_uint64 * 2).from_address(out)
+                o[0], o[1] = u & ((1 << 64) - 1), u >> 64
+                return 0
+            cplx = dtype == nat.EGG_C128
+            p = np.ctypeslib.as_array((ctypes.c_double * (npairs * (2 if cplx else 1))).from_address(P))
+            w = np.repeat(np.arange(1, npairs + 1), 2 if cplx else 1)
+            o = (ctypes.c_double * 2).from_address(out)
+            o[0] = float(np.sum(p * w)) + prec
+            if cplx:
+                o[1] = 1.0
+            return 0
+
+    monkeypatch.setattr(nat, "lib", lambda: Stub())
+    A = np.arange(36, dtype=np.float64).reshape(6, 6)
+    pairs = np.array([A[i, j] for i in range(6) for j in range(i + 1, 6)])
+    w = np.arange(1, 16)
+    for dt in (np.float64, np.complex128):
+        got = egg.hafnian(A.astype(dt), method="dp", check_symmetric=False, prec="fma")
+        want = float(np.sum(pairs * w)) + nat.PREC["fma"]
+        assert type(got) is np.dtype(dt).type and got == (complex(want, 1.0) if dt is np.complex128 else want)
+    got = egg.hafnian(A.astype(np.int64), method="dp", check_symmetric=False, exact=True)
+    assert got == -int(np.sum(pairs.astype(np.int64) * w)) - (1 << 70)

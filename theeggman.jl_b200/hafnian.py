@@ -241,6 +241,23 @@ def _dp_device(T: np.dtype, P: np.ndarray, K: int, prec: str, max_batch, exact_i
     return out
 
 
+def _dp_one(T: np.dtype, P: np.ndarray, K: int, prec: str, exact_int: bool):
+    """One hafnian through egg_dp_batch (B = 1), as _dp_device(...)[0], with its value read from a
+    reused result buffer."""
+    key = _dp_plan(K)
+    dtype = nat.EGG_I64 if exact_int else nat.DTYPE_OF[np.dtype(T)]
+    if prec not in nat.PREC:
+        raise ArgumentError(f"prec must be one of {tuple(nat.PREC)}")
+    P = np.ascontiguousarray(P)  # 1 x npairs: both memory orders at once
+    with _lock:
+        out, out_ptr = _one_out(np.dtype(np.uint64), 2) if exact_int else _one_out(np.dtype(T))
+        nat.check(nat.lib().egg_dp_batch(key[0], key[1], dtype, nat.PREC[prec], nat.ptr(P), 1, 0, out_ptr))
+        if exact_int:
+            v = int(out[0]) | (int(out[1]) << 64)
+            return v - (1 << 128) if v >= (1 << 127) else v
+        return out[0]
+
+
 def _dp_prec(prec) -> str:
     """DP rounding: the reference CPU's (exact) unless asked otherwise.  'reference' is 'exact':
     the DP's sum order is fixed by its plan, so its exact kernels already reproduce the reference
@@ -344,12 +361,13 @@ def _reps_array(reps: tuple):
 _one_outs: dict = {}
 
 
-def _one_out(CT):
-    """(array, address) of the one-value result buffer of a scalar call, per type; use under _lock."""
-    r = _one_outs.get(CT)
+def _one_out(CT, n: int = 1):
+    """(array, address) of the result buffer of a scalar call (n values of type CT), kept per kind
+    and reused; use under _lock."""
+    r = _one_outs.get((CT, n))
     if r is None:
-        a = np.zeros(1, CT)
-        r = _one_outs[CT] = (a, a.ctypes.data)
+        a = np.zeros(n, CT)
+        r = _one_outs[(CT, n)] = (a, a.ctypes.data)
     return r
 
 
@@ -451,7 +469,7 @@ def hafnian(A, *, nthreads: int | None = None, glynn: bool | None = None, method
         raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
     if chosen in ("unrolled", "dp"):
         P = _gather_pairs_one(T, A)
-        v = _dp_device(T, P, N, _dp_prec(prec), None, exact_int)[0]
+        v = _dp_one(T, P, N, _dp_prec(prec), exact_int)
         return v if exact_int else T.type(v)
     return _sieve_one(T, _permuted_distinct(T, A), [1] * E, use_glynn, prec, nthreads)
 
