@@ -552,8 +552,8 @@ def _hafnian_batch(As, *, nthreads, glynn, method, check_symmetric, backend, max
         raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
     sel_glynn = pol._choose_method_distinct(N, N // 2, 1 if backend is None else nthreads)[1]
     use_glynn = sel_glynn if glynn is None else glynn
-    x = _distinct_x(N // 2)
-    return _sieve_device_batch(T, [_permuted(T, m, x) for m in mats], [[1] * (N // 2)] * B, [use_glynn] * B, prec)
+    return _sieve_device_batch(T, [_permuted_distinct(T, m) for m in mats], [[1] * (N // 2)] * B, [use_glynn] * B,
+                               prec)
 
 
 @lru_cache(maxsize=4096)
