@@ -67,8 +67,12 @@ const char *egg_last_error(void);
  * the reference. */
 int64_t egg_launch_count(void);
 
-/* Select the CUDA device (idempotent; the first call of any other entry point does this with
- * device 0).  Fails with EGG_ERR_NO_DEVICE if there is none. */
+/* Bind the library to one CUDA device (idempotent; the first call of any other entry point does
+ * this with device 0).  Fails with EGG_ERR_NO_DEVICE if there is none.  The library's streams,
+ * plans and work buffers belong to that device: binding another device in the same process fails
+ * with EGG_ERR_ARGUMENT, and so does any later call made while the calling thread's current device
+ * is a different one.  (egg_sieve_device_noalloc keeps its state per device and is the exception:
+ * it runs on the caller's current device.) */
 int egg_init(int device);
 
 /* Device bytes held by resident plans and reusable work buffers.
@@ -160,8 +164,10 @@ int egg_sieve_device(int dtype, int prec, const void *Ax, int64_t E, const int64
  * device buffers; the sieve's scratch (its instance tables and per-warp partial sums) lives in a
  * fixed 4 MiB array compiled into the library, present on every GPU that loads it until the
  * process exits.  Nothing is allocated or freed.  A sieve needing more scratch than that (edge
- * counts up to 32 fit) is refused with EGG_ERR_TOO_LARGE.  The first call on a device looks up
- * the array's device address, so make it before any stream capture.  All calls share the array:
+ * counts up to 32 fit on a 148-SM B200: the largest need is about 3.8 MB) is refused with
+ * EGG_ERR_TOO_LARGE.  The first call on a device looks up the device addresses of the array and of
+ * the library's binomial table (no upload and no stream work), so make it before any stream
+ * capture.  The call runs on the calling thread's current device.  All calls share the array:
  * calls whose device work overlaps race on it.  There is no counterpart of this entry point in the
  * reference. */
 int egg_sieve_device_noalloc(int dtype, int prec, const void *Ax, int64_t E, const int64_t *edge_reps, int glynn,

@@ -368,6 +368,154 @@ int orc_haf_dp_batch(int dtype, int idx_bytes, const void *starts, const void *t
     return err ? -1 : 0;
 }
 
+/*
+ * The same forward pass without a stored plan, for degrees whose plan would not fit in host memory
+ * (N = 36: 3.2 GB of transitions, N = 40: 24 GB).  It walks exactly the states and transitions
+ * _build_dp_plan (src/dp.jl:223-304) would list, in its order, and sums each state as _dp_states!
+ * (:344-363) does:
+ *   - A non-empty mask S with r = K - |S| bits removed is reachable iff r <= 2(min(S) - 1)
+ *     (src/dp.jl:16-27, 1-based min), so the reachable masks of popcount c are exactly the
+ *     c-subsets of the bits m0..K-1 (0-based) with m0 = (K - c)/2, and sorting by
+ *     (popcount, mask) lists each level in colex order of the element sets shifted down by m0.
+ *     A state is identified by (c, colex rank); only two levels are kept.
+ *   - State S (lowest bit i) has one transition per other bit j, ascending (:283-292), to the
+ *     child S \ {i, j} of level c - 2 with pair index _pair_index(i, j, K) (src/unrolled.jl:60).
+ *     The child's colex rank is found from its elements with the binomial table.
+ * Each state is accumulated by one thread in plan order, so the value is bit-identical to
+ * orc_haf_dp on the stored plan for any thread count; the tests pin this against orc_build_plan
+ * (transition by transition, and value by value) for K <= 28.  Supports ORC_F64, ORC_C128,
+ * ORC_I64 (Int128 states) and ORC_Q_F64.
+ */
+static int64_t g_cbinom[65][65];
+static void cbinom_init(void)
+{
+    if (g_cbinom[0][0] == 1) return;
+    for (int n = 0; n <= 64; ++n)
+        for (int k = 0; k <= 64; ++k) g_cbinom[n][k] = binom_i64(n, k);
+}
+
+/* The colex unrank of r among the c-subsets of {0..U-1}: elements e[1] < ... < e[c]. */
+static void colex_unrank(int64_t r, int c, int U, int *e)
+{
+    int x = U - 1;
+    for (int i = c; i >= 1; --i) {
+        while (g_cbinom[x][i] > r) --x;
+        e[i] = x;
+        r -= g_cbinom[x][i];
+        --x;
+    }
+}
+
+/* The closed-form plan's transitions of degree K, in the stored layout (the test compares them
+ * with orc_build_plan's, entry for entry).  trans_out has ntrans entries of idx_bytes. */
+int orc_closed_trans(int K, int idx_bytes, void *trans_out)
+{
+    if (K < 2 || K > 64 || (K & 1) || (idx_bytes != 4 && idx_bytes != 8)) return -1;
+    cbinom_init();
+    const int bits = pair_bits(idx_bytes);
+    int64_t n = 0, child_lo1 = 1; /* 1-based number of the child level's first state */
+    int64_t level_lo1 = 2;        /* level c = 2 starts after the empty set */
+    for (int c = 2; c <= K; c += 2) {
+        const int m0 = (K - c) / 2, U = K - m0;
+        const int64_t cnt = g_cbinom[U][c];
+        for (int64_t r = 0; r < cnt; ++r) {
+            int e[66];
+            colex_unrank(r, c, U, e);
+            const int64_t i1 = e[1] + m0 + 1;
+            for (int j = 2; j <= c; ++j) {
+                int64_t rank = 0;
+                for (int x = 2; x <= c; ++x) {
+                    if (x == j) continue;
+                    const int pos = x < j ? x - 1 : x - 2; /* position in the child's set */
+                    rank += g_cbinom[e[x] - 1][pos];
+                }
+                const int64_t t = ((child_lo1 + rank) << bits) | orc_pair_index(i1, e[j] + m0 + 1, K);
+                if (idx_bytes == 4) ((int32_t *)trans_out)[n] = (int32_t)t;
+                else ((int64_t *)trans_out)[n] = t;
+                ++n;
+            }
+        }
+        child_lo1 = level_lo1;
+        level_lo1 += cnt;
+    }
+    return 0;
+}
+
+#define CLOSED_LEVEL_BODY(T, ZERO, MULADD)                                                      \
+    _Pragma("omp parallel num_threads(nthreads)")                                              \
+    {                                                                                          \
+        int nt_ = 1, id_ = 0;                                                                  \
+        CLOSED_OMP_IDS(nt_, id_);                                                              \
+        const int64_t r0 = cnt * id_ / nt_, r1 = cnt * (id_ + 1) / nt_;                        \
+        int e[66];                                                                             \
+        int64_t suf[67];                                                                       \
+        if (r0 < r1) colex_unrank(r0, c, U, e);                                                \
+        for (int64_t r = r0; r < r1; ++r) {                                                    \
+            if (r > r0) { /* colex successor: raise the lowest element that can move */        \
+                int x = 1;                                                                     \
+                while (x < c && e[x] + 1 == e[x + 1]) ++x;                                     \
+                e[x] += 1;                                                                     \
+                for (int y = 1; y < x; ++y) e[y] = y - 1;                                      \
+            }                                                                                  \
+            suf[c + 1] = 0;                                                                    \
+            suf[c] = 0;                                                                        \
+            for (int x = c; x >= 3; --x) suf[x - 1] = suf[x] + g_cbinom[e[x] - 1][x - 2];      \
+            int64_t pre = 0;                                                                   \
+            const int64_t i1 = e[1] + m0 + 1;                                                  \
+            T acc = ZERO;                                                                      \
+            for (int j = 2; j <= c; ++j) {                                                     \
+                const int64_t q = orc_pair_index(i1, e[j] + m0 + 1, K);                        \
+                MULADD(acc, P[q - 1], prev[pre + suf[j]]);                                     \
+                pre += g_cbinom[e[j] - 1][j - 1];                                              \
+            }                                                                                  \
+            cur[r] = acc;                                                                      \
+        }                                                                                      \
+    }
+
+#ifdef _OPENMP
+#define CLOSED_OMP_IDS(nt, id) do { nt = omp_get_num_threads(); id = omp_get_thread_num(); } while (0)
+#else
+#define CLOSED_OMP_IDS(nt, id) do { } while (0)
+#endif
+
+int orc_haf_dp_closed(int dtype, int K, const void *Pv, int nthreads, void *out)
+{
+    if (K < 0 || K > 64 || (K & 1)) return -1;
+    if (dtype != ORC_F64 && dtype != ORC_C128 && dtype != ORC_I64 && dtype != ORC_Q_F64) return -1;
+    cbinom_init();
+    const size_t es = dp_elsize(dtype);
+    if (nthreads < 1) nthreads = 1;
+    if (K == 0) { set_one(dtype, out); return 0; }
+    int64_t maxlev = 1;
+    for (int c = 2; c <= K; c += 2) {
+        const int U = K - (K - c) / 2;
+        if (g_cbinom[U][c] > maxlev) maxlev = g_cbinom[U][c];
+    }
+    char *buf0 = (char *)malloc((size_t)maxlev * es), *buf1 = (char *)malloc((size_t)maxlev * es);
+    if (!buf0 || !buf1) { free(buf0); free(buf1); return -2; }
+    set_one(dtype, buf0); /* the empty set */
+    char *pv = buf0, *cv = buf1;
+    for (int c = 2; c <= K; c += 2) {
+        const int m0 = (K - c) / 2, U = K - m0;
+        const int64_t cnt = g_cbinom[U][c];
+        switch (dtype) {
+        case ORC_F64: { const double *P = Pv, *prev = (const double *)pv; double *cur = (double *)cv;
+                        CLOSED_LEVEL_BODY(double, 0.0, MA_REAL) break; }
+        case ORC_C128: { const c128 *P = Pv, *prev = (const c128 *)pv; c128 *cur = (c128 *)cv; const c128 z = {0, 0};
+                         CLOSED_LEVEL_BODY(c128, z, MA_C128) break; }
+        case ORC_I64: { const int64_t *P = Pv; const __int128 *prev = (const __int128 *)pv; __int128 *cur = (__int128 *)cv;
+                        CLOSED_LEVEL_BODY(__int128, 0, MA_I128) break; }
+        case ORC_Q_F64: { const double *P = Pv; const __float128 *prev = (const __float128 *)pv; __float128 *cur = (__float128 *)cv;
+                          CLOSED_LEVEL_BODY(__float128, 0, MA_QR) break; }
+        }
+        char *t = pv; pv = cv; cv = t;
+    }
+    memcpy(out, pv, es); /* the last level holds one state, the full mask */
+    free(buf0);
+    free(buf1);
+    return 0;
+}
+
 /* _gather_pairs!(P, A, idx, K), src/dp.jl:452-462.  A is column-major N x N, idx 1-based. */
 void orc_gather_pairs(int dtype, const void *A, int64_t N, const int64_t *idx, int64_t K, void *P)
 {

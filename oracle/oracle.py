@@ -26,7 +26,29 @@ from math import comb
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "build", "libeggoracle.so")
+
+
+def _host_tag() -> str:
+    """A short name for this host's CPU (model and feature flags): the oracle is compiled with
+    -march=native, so a build made on one host must not be loaded on another."""
+    import hashlib
+
+    model, flags = "", ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name") and not model:
+                    model = line.split(":", 1)[1].strip()
+                elif line.startswith("flags") and not flags:
+                    flags = line.split(":", 1)[1].strip()
+                if model and flags:
+                    break
+    except OSError:
+        pass
+    return hashlib.sha1((model + "|" + flags).encode()).hexdigest()[:10]
+
+
+_LIB_PATH = os.path.join(_HERE, "build", f"libeggoracle-{_host_tag()}.so")
 
 F64, C128, F32, C64, I64, Q_F64, Q_C128 = 0, 1, 2, 3, 4, 5, 6
 
@@ -40,7 +62,7 @@ _DP_PARALLEL_CAP = 4     # src/hafnian.jl:969
 
 def build() -> str:
     """Compile the C oracle (idempotent)."""
-    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    subprocess.run(["make", "-s", "-C", _HERE, "OUT=" + os.path.relpath(_LIB_PATH, _HERE)], check=True)
     return _LIB_PATH
 
 
@@ -63,6 +85,8 @@ def lib() -> ctypes.CDLL:
     L.orc_sieve_terms.argtypes = [i32, vp, vp, i32, i32, i64, i64, vp]
     L.orc_charpoly_check.argtypes = [i32, vp, i32, vp]
     L.orc_max_threads.restype = i32
+    L.orc_closed_trans.argtypes = [i32, i32, vp]
+    L.orc_haf_dp_closed.argtypes = [i32, i32, vp, i32, vp]
     return L
 
 
@@ -146,6 +170,37 @@ def haf_dp_pairs(P: np.ndarray, plan: Plan, dtype: int, nthreads: int = 1):
     if dtype in (Q_F64, Q_C128):
         return out  # raw bytes; callers use quad_to_mpf
     return out[0]
+
+
+def closed_trans(K: int, idx_bytes: int) -> np.ndarray:
+    """The transitions of the degree-K plan as the closed-form walk lists them (orc_closed_trans),
+    in the layout of build_plan's `trans`: the tests compare the two entry for entry."""
+    ns, nt = dp_counts(K)
+    out = np.zeros(max(nt, 1), dtype=np.int32 if idx_bytes == 4 else np.int64)
+    if lib().orc_closed_trans(K, idx_bytes, _ptr(out)) != 0:
+        raise ValueError(f"no closed-form plan for degree {K}")
+    return out[:nt]
+
+
+def haf_dp_closed(P: np.ndarray, K: int, dtype: int, nthreads: int = 1):
+    """_haf_dp's forward pass (src/dp.jl:408-442) on the closed form of the degree-K plan, no stored
+    transitions: the reference's states, transitions and per-state order, for degrees whose plan
+    does not fit in host memory.  dtype F64, C128, I64 (Int128 states; returns a Python int) or
+    Q_F64 (raw bytes)."""
+    src = {F64: np.float64, C128: np.complex128, I64: np.int64, Q_F64: np.float64}[dtype]
+    P = np.ascontiguousarray(P, dtype=src)
+    out = np.zeros(4, np.uint64)
+    rc = lib().orc_haf_dp_closed(dtype, K, _ptr(P), int(nthreads), _ptr(out))
+    if rc != 0:
+        raise RuntimeError(f"orc_haf_dp_closed failed rc={rc}")
+    if dtype == F64:
+        return out.view(np.float64)[0]
+    if dtype == C128:
+        return out.view(np.complex128)[0]
+    if dtype == I64:
+        v = int(out[0]) | (int(out[1]) << 64)
+        return v - (1 << 128) if v >= (1 << 127) else v
+    return out
 
 
 def gather_pairs(A: np.ndarray, idx, K: int) -> np.ndarray:

@@ -54,6 +54,45 @@ def test_noalloc_sieve_matches_allocating_entry_point(egg, W, cplx, prec):
             assert rel(val, expect) <= 1e-15, (N, glynn, call, val, expect)
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_noalloc_at_32_edges_allocates_nothing(egg, W, prec):
+    """The largest edge count the entry point accepts (E = 32, a 64 x 64 matrix), kept cheap with
+    only five nonzero multiplicities (32 terms); the library's own device buffers must not grow."""
+    import torch
+
+    from theeggman_b200 import _native as nat
+
+    L = nat.lib()
+    assert L.egg_init(0) == 0, L.egg_last_error()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(dev)
+    E = 32
+    A = W.dense_real(2 * E, 4321)
+    dA = torch.from_numpy(np.ascontiguousarray(A.T)).to(dev)
+    reps = np.zeros(E, dtype=np.int64)
+    reps[[0, 5, 11, 20, 31]] = 1
+    ref = torch.zeros(1, dtype=torch.float64, device=dev)
+    got = torch.zeros(1, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    assert L.egg_sieve_device(nat.EGG_F64, prec, dA.data_ptr(), E, reps.ctypes.data, 0, ref.data_ptr(),
+                              stream.cuda_stream) == 0, L.egg_last_error()
+    stream.synchronize()
+    # One call first: the first call on a device looks up the fixed array's address.
+    assert L.egg_sieve_device_noalloc(nat.EGG_F64, prec, dA.data_ptr(), E, reps.ctypes.data, 0, got.data_ptr(),
+                                      stream.cuda_stream) == 0, L.egg_last_error()
+    stream.synchronize()
+    held = L.egg_cache_bytes()
+    for call in range(2):
+        got.fill_(float("nan"))
+        torch.cuda.synchronize()
+        rc = L.egg_sieve_device_noalloc(nat.EGG_F64, prec, dA.data_ptr(), E, reps.ctypes.data, 0, got.data_ptr(),
+                                        stream.cuda_stream)
+        assert rc == 0, L.egg_last_error()
+        stream.synchronize()
+        assert rel(got[0].item(), ref[0].item()) <= 1e-15, (call, got[0].item(), ref[0].item())
+    assert L.egg_cache_bytes() == held
+
+
 def test_noalloc_rejects_bad_arguments(egg):
     from theeggman_b200 import _native as nat
 

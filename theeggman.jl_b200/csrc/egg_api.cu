@@ -60,13 +60,17 @@ int create_streams(Context &c, int device)
 int smem_limit_at_least(const void *k, size_t bytes)
 {
     // Own lock: the entry point that allocates nothing reaches this without the library's lock.
+    // A kernel's attribute is set per device, so the record is kept per (device, kernel).
     static std::mutex mu;
     std::lock_guard<std::mutex> lk(mu);
-    static std::map<const void *, size_t> done;
-    auto it = done.find(k);
+    static std::map<std::pair<int, const void *>, size_t> done;
+    int dev = -1;
+    EGG_CUDA_TRY(cudaGetDevice(&dev));
+    const auto key = std::make_pair(dev, k);
+    auto it = done.find(key);
     if (it != done.end() && it->second >= bytes) return EGG_OK;
     EGG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    done[k] = bytes;
+    done[key] = bytes;
     return EGG_OK;
 }
 
@@ -74,8 +78,10 @@ int blocks_per_sm(const void *k, int threads, size_t smem, int *out)
 {
     static std::mutex mu;
     std::lock_guard<std::mutex> lk(mu);
-    static std::map<std::tuple<const void *, int, size_t>, int> done;
-    const auto key = std::make_tuple(k, threads, smem);
+    static std::map<std::tuple<int, const void *, int, size_t>, int> done;
+    int dev = -1;
+    EGG_CUDA_TRY(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, k, threads, smem);
     auto it = done.find(key);
     if (it != done.end()) {
         *out = it->second;
@@ -147,8 +153,22 @@ using namespace egg;
     std::lock_guard<std::recursive_mutex> lk_(ctx().mu);    \
     do {                                                    \
         int rc_ = ensure_init();                            \
+        if (!rc_) rc_ = check_current_device();             \
         if (rc_) return rc_;                                \
     } while (0)
+
+// The library's context (streams, plans, work buffers) belongs to one device, the one egg_init
+// bound (device 0 if egg_init was not called).  A call from a thread whose current device is
+// another one is refused instead of handing that device's kernels this device's memory.
+static int check_current_device()
+{
+    int dev = -1;
+    EGG_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != ctx().device)
+        return fail(EGG_ERR_ARGUMENT, "the library is bound to device " + std::to_string(ctx().device) +
+                                          " but the calling thread's current device is " + std::to_string(dev));
+    return EGG_OK;
+}
 
 static int check_layout(int K, int idx_bytes);
 

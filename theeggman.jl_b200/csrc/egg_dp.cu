@@ -996,7 +996,7 @@ static int run_closed(const DevPlan &plan, const PT *P, HT *h0, HT *h1, HT *out,
                       cudaStream_t st)
 {
     int rc = EGG_OK;
-    const uint32_t *bt = binom32_device(st, &rc);
+    const uint32_t *bt = binom32_device(&rc);
     if (!bt) return rc;
     const int K = plan.K;
     // A single instance of a small degree: one cluster of CTAs.  A batch of small degrees, whose two
@@ -1201,7 +1201,7 @@ template <class Op, class PT, class HT, class AT, class OT>
 static int run_grouped(const DevPlan &plan, const PT *P, int64_t G, HT *h0, HT *h1, int64_t ldh, OT *out, cudaStream_t st)
 {
     int rc = EGG_OK;
-    const uint32_t *bt = binom32_device(st, &rc);
+    const uint32_t *bt = binom32_device(&rc);
     if (!bt) return rc;
     const int K = plan.K;
     const int64_t ldp = (int64_t)K * (K - 1) / 2;
@@ -1295,7 +1295,7 @@ int dp_run_one_host(const DevPlan &plan, int dtype, int prec, const void *P, voi
 {
     if (prec == EGG_PREC_MIXED) return kDpNotHere;
     int rc = EGG_OK;
-    const uint32_t *bt = binom32_device(st, &rc);
+    const uint32_t *bt = binom32_device(&rc);
     if (!bt) return rc;
     const bool fma_mode = prec == EGG_PREC_FMA;
     switch (dtype) {

@@ -199,7 +199,7 @@ int plan_is_closed_form(const DevPlan &p, cudaStream_t st, bool *same);
 int plan_validate_device(const DevPlan &p, cudaStream_t st);
 // Saturated 32-bit binomial table C(n, k), n, k <= 64, row-major with row length 65, in device
 // memory (uploaded once; no allocation).
-const uint32_t *binom32_device(cudaStream_t st, int *rc);
+const uint32_t *binom32_device(int *rc);
 
 // egg_dp.cu
 // The resident plan for degree K in the layout the reference picks for it (Int32 up to K = 32),

@@ -367,7 +367,7 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
     if (rc) return rc;
     // 4. Gather, 5. DP per bin, 6. scatter: eagerly the first time a shape is seen, captured into a
     // graph the second time, replayed after that (not when the caller is capturing the stream).
-    if (!binom32_device(st, &rc)) return rc;
+    if (!binom32_device(&rc)) return rc;
     GraphKey key{dtype, prec, n, B, {}, {dA, drows, dout}};
     for (int k = 0; k < bins.nb; ++k) {
         key.shape.insert(key.shape.end(), {(int64_t)bins.b[k].K, bins.b[k].count, exs[k].batched ? 1 : 0, exs[k].group});

@@ -12,46 +12,52 @@
 //   * The scratch array holds kNoAllocScratchBytes (4 MiB).  It lives on every GPU that loads the
 //     library, for the life of the process.  A sieve whose tables and partials need more is refused
 //     with EGG_ERR_TOO_LARGE and a message giving both sizes (edge counts up to 32 fit).
-//   * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-//     that device current and caches it; make that first call before capturing any stream.
+//   * The first call on a device looks up, with that device current, the device addresses of this
+//     array and of the library's binomial table (cudaGetSymbolAddress; both are module globals with
+//     their contents in the image, so nothing is uploaded and no stream is touched) and caches them
+//     per device; make that first call before capturing any stream.
 //   * Every call uses the same array, and each call overwrites what it reads: the tables are copied
 //     in and every partial-sum slot is written by its warp before the final reduction reads it, so
 //     nothing has to start at zero.  Calls whose device work overlaps (on different streams, or from
 //     different host threads) race on the array and must not be issued.
+#include "egg_perdevice.h"
 #include "egg_sieve.cuh"
 
 namespace egg {
 
 static constexpr size_t kNoAllocScratchBytes = (size_t)4 << 20;
-static constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-static std::mutex g_noalloc_mu;
-static void *g_noalloc_addr[kMaxDevices];  // device address of g_noalloc_scratch, per device
-static int g_noalloc_sms[kMaxDevices];
+struct NoAllocSlot {
+    void *addr;   // device address of g_noalloc_scratch on that device
+    int num_sms;
+};
+static PerDevice<NoAllocSlot> g_noalloc;
 
-// Address of the scratch array on the current device (set-up on first use there).
+// Address of the scratch array on the current device (set up on the first call there).
 static int noalloc_scratch(void **ptr, int *num_sms)
 {
     int dev = -1;
     EGG_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return fail(EGG_ERR_NO_DEVICE, "device index out of range for the fixed scratch");
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    NoAllocSlot slot{nullptr, 0};
+    int rc = g_noalloc.get(dev, &slot, [](int d, NoAllocSlot *out) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             return fail(EGG_ERR_CUDA, std::string("cudaGetSymbolAddress(fixed scratch): ") + cudaGetErrorString(e));
         int sms = 0;
-        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
         if (e != cudaSuccess || sms <= 0)
             return fail(EGG_ERR_CUDA, std::string("cudaDeviceGetAttribute(SM count): ") + cudaGetErrorString(e));
-        g_noalloc_sms[dev] = sms;
-        g_noalloc_addr[dev] = p;
-    }
-    *ptr = g_noalloc_addr[dev];
-    *num_sms = g_noalloc_sms[dev];
+        *out = NoAllocSlot{p, sms};
+        return (int)EGG_OK;
+    });
+    if (rc == PerDevice<NoAllocSlot>::kBadDevice)
+        return fail(EGG_ERR_NO_DEVICE, "device index " + std::to_string(dev) + " out of range for the fixed scratch");
+    if (rc) return rc;
+    *ptr = slot.addr;
+    *num_sms = slot.num_sms;
     return EGG_OK;
 }
 

@@ -13,6 +13,7 @@
 // sum_i C(e_i, i) (combinatorial number system, e_i the shifted elements in increasing order), and
 // each thread can unrank its own state and rank each of its children without any table.
 #include "egg_internal.cuh"
+#include "egg_perdevice.h"
 
 namespace egg {
 
@@ -170,31 +171,57 @@ int plan_is_closed_form(const DevPlan &p, cudaStream_t st, bool *same)
     return rc;
 }
 
-// ---- the binomial table the closed-form DP kernels read ----------------------------------------
+// ---- the binomial table the closed-form DP kernels and the sieve read ---------------------------
 
-static __device__ uint32_t g_binom32[65 * 65];
-static std::mutex g_binom32_mu;
-static const uint32_t *g_binom32_addr = nullptr;
-
-const uint32_t *binom32_device(cudaStream_t st, int *rc)
+// C(n, k) for n, k <= 64, saturated at 2^32 - 1, row-major with row length 65.  Computed at compile
+// time and placed in the module image, so every device that loads the library holds its own copy
+// from the start: nothing is uploaded and no stream is touched.
+struct Binom32Table {
+    uint32_t v[65 * 65];
+};
+static constexpr Binom32Table make_binom32()
 {
-    std::lock_guard<std::mutex> lk(g_binom32_mu);
+    Binom32Table t{};
+    uint64_t row[65] = {};  // C(nn, k), saturated at 2^32 - 1
+    for (int nn = 0; nn <= 64; ++nn) {
+        for (int k = nn; k >= 1; --k) {
+            const uint64_t v = row[k] + row[k - 1];
+            row[k] = v > 0xFFFFFFFFull ? 0xFFFFFFFFull : v;
+        }
+        row[0] = 1;
+        for (int k = 0; k <= 64; ++k) t.v[nn * 65 + k] = (uint32_t)row[k];
+    }
+    return t;
+}
+static __device__ const Binom32Table g_binom32 = make_binom32();
+static_assert(make_binom32().v[32 * 65 + 16] == 601080390u, "C(32, 16)");
+static_assert(make_binom32().v[40 * 65 + 20] == 0xFFFFFFFFu, "C(40, 20) saturates");
+
+static PerDevice<const uint32_t *> g_binom32_addr;
+
+const uint32_t *binom32_device(int *rc)
+{
     *rc = EGG_OK;
-    if (g_binom32_addr) return g_binom32_addr;
-    std::vector<int64_t> b;
-    host_binom(b);
-    static uint32_t h[65 * 65];
-    for (int i = 0; i < 65 * 65; ++i) h[i] = b[i] > (int64_t)UINT32_MAX ? UINT32_MAX : (uint32_t)b[i];
-    void *addr = nullptr;
-    cudaError_t e = cudaMemcpyToSymbolAsync(g_binom32, h, sizeof(h), 0, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess) e = cudaGetSymbolAddress(&addr, g_binom32);
-    if (e != cudaSuccess || !addr) {
-        *rc = fail(EGG_ERR_CUDA, std::string("binomial table upload: ") + cudaGetErrorString(e));
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        *rc = fail(EGG_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
         return nullptr;
     }
-    g_binom32_addr = (const uint32_t *)addr;
-    return g_binom32_addr;
+    const uint32_t *addr = nullptr;
+    *rc = g_binom32_addr.get(
+        dev, &addr,
+        [](int, const uint32_t **out) {
+            void *p = nullptr;
+            cudaError_t e2 = cudaGetSymbolAddress(&p, g_binom32);
+            if (e2 != cudaSuccess || !p)
+                return fail(EGG_ERR_CUDA, std::string("binomial table address: ") + cudaGetErrorString(e2));
+            *out = (const uint32_t *)p;
+            return (int)EGG_OK;
+        });
+    if (*rc == PerDevice<const uint32_t *>::kBadDevice)
+        *rc = fail(EGG_ERR_NO_DEVICE, "device index " + std::to_string(dev) + " out of range for the binomial table");
+    return *rc ? nullptr : addr;
 }
 
 // Structure check for a plan that came from the host: every transition of level L must name a

@@ -873,7 +873,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.Ax = dAx;
     a.reps = (const int *)(base + off_reps);
     a.binoms = (const double *)(base + off_bin);
-    a.binom32 = binom32_device(st, &rc);
+    a.binom32 = binom32_device(&rc);
     if (!a.binom32) return rc;
     a.inst = (const SieveInst *)(base + off_inst);
     a.lists = (const uint64_t *)(base + off_lst);

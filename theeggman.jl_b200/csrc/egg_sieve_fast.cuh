@@ -39,11 +39,23 @@ namespace egg {
 
 static constexpr unsigned FULL = 0xffffffffu;
 
-// Tables in constant memory, one copy per translation unit (upload_fast_tables before its launches).
-// -1 / (2t) for t = 0..63, rounded on the host (entry 0 unused).
-static __constant__ double c_neg_inv_2t[64];
-// C(x, i) for x, i <= 32 at [x * 33 + i] (C(32, 16) < 2^32).
-static __constant__ uint32_t c_binom[33 * 33];
+// Tables in constant memory, computed at compile time and placed in the module image, so that
+// every device that loads the library holds them from the start (nothing to upload).
+struct FastTables {
+    double neg_inv_2t[64];   // -1 / (2t) for t = 1..63, correctly rounded (entry 0 unused)
+    uint32_t binom[33 * 33]; // C(x, i) for x, i <= 32 at [x * 33 + i] (C(32, 16) < 2^32)
+};
+static constexpr FastTables make_fast_tables()
+{
+    FastTables t{};
+    for (int i = 1; i < 64; ++i) t.neg_inv_2t[i] = -1.0 / (2.0 * i);
+    for (int x = 0; x <= 32; ++x)
+        for (int i = 0; i <= 32; ++i)
+            t.binom[x * 33 + i] = i == 0 ? 1u : (x == 0 ? 0u : t.binom[(x - 1) * 33 + i - 1] + t.binom[(x - 1) * 33 + i]);
+    return t;
+}
+static __constant__ const FastTables c_fast = make_fast_tables();
+static_assert(make_fast_tables().binom[32 * 33 + 16] == 601080390u, "C(32, 16)");
 
 // The k-subset of [0, E) with colex rank R: x_i is the largest x with C(x, i) <= what is left.
 __device__ __forceinline__ uint32_t subset_unrank(int E, int k, uint32_t R)
@@ -51,9 +63,9 @@ __device__ __forceinline__ uint32_t subset_unrank(int E, int k, uint32_t R)
     uint32_t S = 0;
     int x = E - 1;
     for (int i = k; i >= 1; --i) {
-        while (c_binom[x * 33 + i] > R) --x;
+        while (c_fast.binom[x * 33 + i] > R) --x;
         S |= 1u << x;
-        R -= c_binom[x * 33 + i];
+        R -= c_fast.binom[x * 33 + i];
         --x;
     }
     return S;
@@ -281,7 +293,7 @@ __device__ __forceinline__ double series_q(const double *q, int m, int n, int la
         }
         const int t1 = s + 1;
         const double own = (NC > 1 && t1 >= G) ? S[NC - 1] : S[0];
-        fs = __shfl_sync(gm, own, t1 & (G - 1), G) * c_neg_inv_2t[t1];
+        fs = __shfl_sync(gm, own, t1 & (G - 1), G) * c_fast.neg_inv_2t[t1];
     }
     return fs;
 }
@@ -309,7 +321,7 @@ __device__ __forceinline__ cd series_q_c(const cd *q, int m, int n, int lane, un
             }
         }
         const int t1 = s + 1;
-        const double c1 = c_neg_inv_2t[t1];
+        const double c1 = c_fast.neg_inv_2t[t1];
         const double ownr = (NC > 1 && t1 >= G) ? Sr[NC - 1] : Sr[0];
         const double owni = (NC > 1 && t1 >= G) ? Si[NC - 1] : Si[0];
         fr = __shfl_sync(gm, ownr, t1 & (G - 1), G) * c1;
@@ -610,43 +622,6 @@ __device__ __forceinline__ cd term_cplx(const cd *__restrict__ Ax, int lda, int 
     labudde_diag_c<MW, G>(cft, hk, (cd *)ws.q, m, n, lane, gm);
     __syncwarp(gm);
     return series_q_c<G>((const cd *)ws.q, m, n, lane, gm);
-}
-
-static int upload_fast_tables(cudaStream_t st);
-
-// Uploads this translation unit's tables once per device and waits for them; while `st` is being
-// captured into a graph, records the upload on it instead (every time, as the graph may be the only
-// thing that runs).
-static int upload_fast_tables_once(cudaStream_t st)
-{
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    EGG_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
-    if (cs != cudaStreamCaptureStatusNone) return upload_fast_tables(st);
-    int dev = 0;
-    EGG_CUDA_TRY(cudaGetDevice(&dev));
-    static std::atomic<uint64_t> done{0};
-    if (dev >= 0 && dev < 64 && ((done.load() >> dev) & 1u)) return EGG_OK;
-    int rc = upload_fast_tables(st);
-    if (rc) return rc;
-    EGG_CUDA_TRY(cudaStreamSynchronize(st));
-    if (dev >= 0 && dev < 64) done.fetch_or(1ull << dev);
-    return EGG_OK;
-}
-
-static int upload_fast_tables(cudaStream_t st)
-{
-    // -1/(2t), computed with IEEE division on the host.
-    static double host_tab[64];
-    if (host_tab[1] == 0.0)
-        for (int t = 1; t < 64; ++t) host_tab[t] = -1.0 / (2.0 * t);
-    EGG_CUDA_TRY(cudaMemcpyToSymbolAsync(c_neg_inv_2t, host_tab, sizeof(host_tab), 0, cudaMemcpyHostToDevice, st));
-    static uint32_t host_binom[33 * 33];
-    if (host_binom[0] == 0)
-        for (int x = 0; x <= 32; ++x)
-            for (int i = 0; i <= 32; ++i)
-                host_binom[x * 33 + i] = i == 0 ? 1u : (x == 0 ? 0u : host_binom[(x - 1) * 33 + i - 1] + host_binom[(x - 1) * 33 + i]);
-    EGG_CUDA_TRY(cudaMemcpyToSymbolAsync(c_binom, host_binom, sizeof(host_binom), 0, cudaMemcpyHostToDevice, st));
-    return EGG_OK;
 }
 
 }  // namespace egg

@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
             }
         }
     } else if (in.subset && K <= E) {
-        const uint64_t cnt = c_binom[E * 33 + K];
+        const uint64_t cnt = c_fast.binom[E * 33 + K];
         const uint64_t lo = (uint64_t)gslot * cnt / W, hi = ((uint64_t)gslot + 1) * cnt / W;
         const double prefac = ((n - K) & 1) ? -1.0 : 1.0;  // (-1)^(n - k), every binomial factor 1
         uint32_t S = lo < hi ? subset_unrank(E, K, (uint32_t)lo) : 0u;

@@ -19,8 +19,6 @@ namespace egg {
 int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
                       cudaStream_t st)
 {
-    int rc = upload_fast_tables_once(st);
-    if (rc) return rc;
     switch (k) {
         EGG_LEVEL_CASES(true, EGG_LVL_LAUNCH)
     }
@@ -30,8 +28,6 @@ int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, 
 int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st)
 {
     static_assert(kFusedMaxE == 10, "EGG_FUSED_CASES lists the levels 1..kFusedMaxE");
-    int rc = upload_fast_tables_once(st);
-    if (rc) return rc;
     switch (k) {
         EGG_FUSED_CASES(true, EGG_ALL_LAUNCH)
     }

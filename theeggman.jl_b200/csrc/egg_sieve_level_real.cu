@@ -23,8 +23,6 @@ int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, 
                       cudaStream_t st)
 {
     if (k > 16) return level_launch_real_hi(a, strides, B, k, narrow, partial, blocks_x, st);
-    int rc = upload_fast_tables_once(st);
-    if (rc) return rc;
     switch (k) {
         EGG_LEVEL_CASES(false, EGG_LVL_LAUNCH)
     }
@@ -34,8 +32,6 @@ int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, 
 int level_launch_all_real(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st)
 {
     static_assert(kFusedMaxE == 10, "EGG_FUSED_CASES lists the levels 1..kFusedMaxE");
-    int rc = upload_fast_tables_once(st);
-    if (rc) return rc;
     switch (k) {
         EGG_FUSED_CASES(false, EGG_ALL_LAUNCH)
     }

@@ -19,8 +19,6 @@ namespace egg {
 int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
                          cudaStream_t st)
 {
-    int rc = upload_fast_tables_once(st);
-    if (rc) return rc;
     switch (k) {
         EGG_LEVEL_CASES_HI(false, EGG_LVL_LAUNCH)
     }
