@@ -57,6 +57,16 @@ def measured_peaks() -> dict:
         return {}
 
 
+def rel_err(a, b) -> float:
+    """|a - b| / |b| (complex-aware; integers exactly)."""
+    if isinstance(a, int) and isinstance(b, int):
+        return 0.0 if a == b else abs(a - b) / max(abs(b), 1)
+    a, b = complex(a), complex(b)
+    if a == b:
+        return 0.0
+    return abs(a - b) / max(abs(b), 1e-300)
+
+
 # The committed ncu summary (kernel and workload) whose DRAM traffic figure belongs to a workload.
 PROFILE_OF = {"sieve40": "sieve_level_kernel_sieve40.md", "sieve40c": "sieve_level_kernel_sieve40c.md",
               "sieve40g": "sieve_level_kernel_sieve40g.md", "rep14": "sieve_level_kernel_rep14.md",
@@ -85,11 +95,12 @@ class SieveWorkload:
 
     kind = "sieve"
 
-    def __init__(self, egg, W, N: int, cplx: bool, glynn, seed: int, config: str = "2"):
+    def __init__(self, egg, W, N: int, cplx: bool, glynn, seed: int, config: str = "2", prec: str = "fma"):
         from theeggman_b200 import policy as pol
         from theeggman_b200 import roofline as R
 
         self.egg, self.N, self.cplx = egg, N, cplx
+        self.forced_glynn = glynn is not None
         E = N // 2
         self.E = E
         if config == "1":
@@ -104,7 +115,10 @@ class SieveWorkload:
         self.reps = np.ones(E, dtype=np.int64)
         self.flops = R.sieve_flops([1] * E, self.glynn, cplx)
         self.dtype = 1 if cplx else 0
-        self.prec = 1  # EGG_PREC_FMA: the register-resident kernels (the API default for the sieve)
+        # "fma": the register-resident kernels with fused multiply-adds (the API default for the
+        # sieve); "exact": every term in the reference's arithmetic.
+        self.prec_name = prec
+        self.prec = {"exact": 0, "fma": 1}[prec]
         self.hafnians_per_step = 1
         self.dtype_name = "c128" if cplx else "f64"
         label = ("config1: N=20 Float64 U[-1,1]" if config == "1" else
@@ -126,7 +140,27 @@ class SieveWorkload:
             raise RuntimeError(L.egg_last_error().decode())
 
     def step_e2e(self):
-        return self.egg.hafnian(self.A, method="sieve", glynn=self.glynn, check_symmetric=False, prec="fma")
+        # The public call with its defaults (symmetry check included); the variant is left to the
+        # cost model unless the workload forces one, and prec is passed only when not the default.
+        kw = {"glynn": self.glynn} if self.forced_glynn else {}
+        if self.prec_name != "fma":
+            kw["prec"] = self.prec_name
+        return self.egg.hafnian(self.A, method="sieve", **kw)
+
+    def device_result(self):
+        v = self.dout.cpu().numpy()[0]
+        return [complex(v) if self.cplx else float(v)]
+
+    def check(self, O, dev_vals, e2e_val):
+        """The timed result against the oracle: the reference's own plain FP64 summation (all host
+        threads, the reference's default) and the double-double sum of the reference's terms."""
+        plain = O.calc_hafnian(self.Ax, [1] * self.E, self.glynn, nthreads=O.max_threads(), sum_mode=0)
+        dd = O.calc_hafnian(self.Ax, [1] * self.E, self.glynn, nthreads=O.max_threads(), sum_mode=1)
+        got = dev_vals[0]
+        return {"vs_reference_plain_fp64": rel_err(got, plain), "vs_reference_terms_dd": rel_err(got, dd),
+                "e2e_vs_device": rel_err(e2e_val, got), "bar": 1e-10,
+                "reference": "oracle calc_hafnian (src/hafnian.jl:684-738), plain FP64 sum with "
+                             f"nthreads={O.max_threads()}, and the double-double sum of the same terms"}
 
 
     @property
@@ -205,11 +239,42 @@ class DPWorkload:
             raise RuntimeError(L.egg_last_error().decode())
 
     def step_e2e(self):
-        exact = self.code == 4
+        kw = {"exact": True} if self.code == 4 else {}
+        if self.prec_name != "exact":
+            kw["prec"] = self.prec_name
         if self.B == 1:
-            return self.egg.hafnian(self.mats[0], method="dp", check_symmetric=False, prec=self.prec_name, exact=exact)
-        return self.egg.hafnian(self.mats, method="dp", check_symmetric=False, prec=self.prec_name, exact=exact,
-                                backend=self.egg.B200Backend())
+            return self.egg.hafnian(self.mats[0], method="dp", **kw)
+        return self.egg.hafnian(self.mats, method="dp", backend=self.egg.B200Backend(), **kw)
+
+    def device_result(self):
+        raw = self.dout.cpu().numpy()
+        if self.code == 4:  # Int128, little-endian pairs of 64-bit words
+            u = raw.view(np.uint64)
+            vals = []
+            for b in range(self.B):
+                v = int(u[2 * b]) | (int(u[2 * b + 1]) << 64)
+                vals.append(v - (1 << 128) if v >= (1 << 127) else v)
+            return vals
+        if self.code == 1:
+            return list(raw.view(np.complex128)[: self.B])
+        return list(raw[: self.B])
+
+    def check(self, O, dev_vals, e2e_val):
+        """The timed results against the oracle's restatement of the reference DP (plan-free walk of
+        the same states and order above N = 28), in FP64 (Int128 for integer graphs).  The mixed
+        form is compared with the FP64 value."""
+        nb = min(self.B, 4)
+        dt = {0: O.F64, 1: O.C128, 4: O.I64}[self.code]
+        worst = 0.0
+        for b in range(nb):
+            P = O.gather_pairs(self.mats[b], list(range(1, self.N + 1)), self.N)
+            want = O.haf_dp_closed(P, self.N, dt, O.max_threads())
+            worst = max(worst, rel_err(dev_vals[b], want))
+        e2e0 = e2e_val if self.B == 1 else e2e_val[0]
+        return {"max_vs_reference_fp64": worst, "instances_checked": nb, "e2e_vs_device": rel_err(e2e0, dev_vals[0]),
+                "bar": 1e-10 if self.prec_name == "mixed" else 0.0,
+                "reference": "oracle DP (src/dp.jl:344-442) in the reference's order and rounding"
+                             + (", Int128" if self.code == 4 else "")}
 
     @property
     def h2d_bytes(self):
@@ -321,10 +386,31 @@ class MixWorkload:
             raise RuntimeError(L.egg_last_error().decode())
 
     def step_e2e(self):
+        kw = {} if self.prec_name == "exact" else {"prec": self.prec_name}
         if self.seq:
-            return [self.egg.hafnian(self.A[np.ix_(r, r)], method="dp", check_symmetric=False, prec=self.prec_name)
-                    for r in self.idxs]
-        return self.egg.hafnian_submatrices(self.A, self.idxs, check_symmetric=False, prec=self.prec_name)
+            return [self.egg.hafnian(self.A[np.ix_(r, r)], method="dp", **kw) for r in self.idxs]
+        return self.egg.hafnian_submatrices(self.A, self.idxs, **kw)
+
+    def device_result(self):
+        return list(self.dout.cpu().numpy())
+
+    def check(self, O, dev_vals, e2e_val):
+        """Two instances of every degree against the oracle DP (FP64, the reference's order); the
+        mixed form against the oracle too, so its figure is its own error."""
+        worst, n = 0.0, 0
+        seen = {}
+        for b, r in enumerate(self.idxs):
+            K = len(r)
+            if seen.get(K, 0) >= 2:
+                continue
+            seen[K] = seen.get(K, 0) + 1
+            want = O.haf_dp_closed(O.gather_pairs(self.A, [int(i) + 1 for i in r], K), K, O.C128, O.max_threads())
+            worst = max(worst, rel_err(dev_vals[b], want))
+            n += 1
+        e2e_worst = max(rel_err(a, b) for a, b in zip(e2e_val, dev_vals))
+        return {"max_vs_reference_fp64": worst, "instances_checked": n, "e2e_vs_device": e2e_worst,
+                "bar": 1e-10 if self.prec_name == "mixed" else 0.0,
+                "reference": "oracle DP (src/dp.jl:344-442), ComplexF64 in the reference's order"}
 
     @property
     def h2d_bytes(self):
@@ -440,6 +526,25 @@ class RepeatedWorkload:
         return _sieve_device_batch(np.dtype(np.complex128 if self.cplx else np.float64), [a for a, _, _ in self.inst],
                                    [er for _, er, _ in self.inst], [g for _, _, g in self.inst], "fma")
 
+    def device_result(self):
+        raw = self.dout.cpu().numpy()
+        return list(raw.view(np.complex128)[: self.B]) if self.cplx else list(raw[: self.B])
+
+    def check(self, O, dev_vals, e2e_val):
+        """16 instances against the oracle's sieve of the same terms (double-double sum), with the
+        reference's plain-sum figure beside it."""
+        worst_dd, worst_plain = 0.0, 0.0
+        for b in range(0, self.B, max(1, self.B // 16)):
+            Ax, er, g = self.inst[b]
+            dd = O.calc_hafnian(Ax, er, g, nthreads=O.max_threads(), sum_mode=1)
+            plain = O.calc_hafnian(Ax, er, g, nthreads=1, sum_mode=0)
+            worst_dd = max(worst_dd, rel_err(dev_vals[b], dd))
+            worst_plain = max(worst_plain, rel_err(dev_vals[b], plain))
+        e2e_worst = max(rel_err(a, b) for a, b in zip(e2e_val, dev_vals))
+        return {"max_vs_reference_terms_dd": worst_dd, "max_vs_reference_plain_fp64": worst_plain,
+                "instances_checked": 16, "e2e_vs_device": e2e_worst, "bar": 1e-10,
+                "reference": "oracle calc_hafnian (src/hafnian.jl:684-738) per instance"}
+
 
     @property
     def h2d_bytes(self):
@@ -464,8 +569,12 @@ class RepeatedWorkload:
 def make_workload(name: str, egg, W, rank: int):
     if name == "sieve40":
         return SieveWorkload(egg, W, 40, False, None, 2024 + rank)
+    if name == "sieve40x":
+        return SieveWorkload(egg, W, 40, False, None, 2024 + rank, prec="exact")
     if name == "sieve40c":
         return SieveWorkload(egg, W, 40, True, None, 2025 + rank)
+    if name == "sieve40cx":
+        return SieveWorkload(egg, W, 40, True, None, 2025 + rank, prec="exact")
     if name == "sieve40g":
         return SieveWorkload(egg, W, 40, False, True, 2024 + rank)
     if name == "sieve20":
@@ -567,7 +676,7 @@ def run_reference(args):
     from theeggman_b200 import workloads as W
 
     O.build()
-    wl = make_workload(args.workload, egg, W, 0)
+    wl = make_workload(args.workload or "sieve40", egg, W, 0)
     cores = O.max_threads()
     for _ in range(args.warmup):
         wl.cpu_sample(cores)
@@ -588,17 +697,143 @@ def run_reference(args):
     }))
 
 
+# The rest of the metric, timed in the default run after the headline: every configuration of the
+# metric with its own value, e2e, roofline, CPU baseline and error against the oracle.  (name,
+# timed steps at most): the heavy end-to-end forms take fewer steps so that the whole default run
+# stays within a few minutes.
+PER_CONFIG = [("dp20", 20), ("sieve20", 20), ("dp32", 10), ("sieve40", 10), ("sieve40x", 5), ("sieve40c", 5),
+              ("sieve40cx", 3), ("sieve40g", 5), ("dp36", 5), ("dp40", 5), ("dp40mixed", 5), ("dp40int", 5),
+              ("dp20x1024", 10), ("mix4096", 10), ("mix4096mixed", 10), ("mix4096seq", 3), ("rep14", 10),
+              ("rep20c", 3)]
+PER_CONFIG_BUDGET_S = 300.0
+
+
+class Device:
+    """The timing context of one rank: its device, a dedicated stream and the L2 flush buffer."""
+
+    def __init__(self, torch, local):
+        self.torch = torch
+        self.dev = torch.device("cuda", local)
+        torch.cuda.set_device(self.dev)
+        # A dedicated stream: the legacy default stream's handle is NULL, which the C ABI reads as
+        # "use the library's own stream", and events on one stream do not time work on another.
+        self.stream = torch.cuda.Stream(self.dev)
+        self.sp = self.stream.cuda_stream
+        self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=self.dev)
+
+    def bus_id(self):
+        props = self.torch.cuda.get_device_properties(self.dev)
+        bus = getattr(props, "pci_bus_id", None)
+        if bus is None:
+            try:
+                bus = "%02x:%02x" % (props.pci_bus_id, props.pci_device_id)
+            except AttributeError:
+                bus = None
+        return str(bus) if bus is not None and not isinstance(bus, int) else None
+
+
+def measure(wl, D, L, steps, warmup, world, clocks=None):
+    """Time `steps` device steps (inputs resident, L2 flushed between steps outside the events),
+    then `steps` end-to-end public-API calls; max over ranks.  Returns the figures and the last
+    results of both."""
+    import torch
+    import torch.distributed as dist
+
+    for _ in range(warmup):
+        wl.step_device(D.sp)
+    torch.cuda.synchronize(D.dev)
+    if clocks is not None:
+        time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(D.dev)
+    launches0 = L.egg_launch_count()
+    evs = []
+    for _ in range(steps):
+        with torch.cuda.stream(D.stream):
+            D.flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(D.stream)
+        wl.step_device(D.sp)
+        e1.record(D.stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize(D.dev)
+    launches = L.egg_launch_count() - launches0  # the library's own kernel launches, counted by it
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop() if clocks is not None else None
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([ms], dtype=torch.float64, device=D.dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    dev_vals = wl.device_result()
+
+    # End to end through the public API, host arrays in and out.
+    e2e_val = None
+    for _ in range(max(1, min(warmup, 3))):
+        e2e_val = wl.step_e2e()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        e2e_val = wl.step_e2e()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=D.dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    return {"ms": ms_max, "value": world * steps * wl.hafnians_per_step / (ms_max / 1e3),
+            "e2e": world * steps * wl.hafnians_per_step / float(te.item()), "launches": launches, "clocks": clk,
+            "dev_vals": dev_vals, "e2e_val": e2e_val}
+
+
+def cpu_leg(wl, args):
+    """Rank 0 at N = 1 only: the oracle as the CPU baseline (the reference's algorithm on the host's
+    cores) and as the checker of the timed results."""
+    from oracle import oracle as O
+
+    O.build()
+    cores = O.max_threads()
+    rate, sample = wl.cpu_sample(cores)
+    return O, {"value": rate, "unit": "hafnians/s", "cores": cores, "kind": "port", "sample": sample}
+
+
+def form_of(wl) -> str:
+    """The arithmetic form a workload times."""
+    p = getattr(wl, "prec_name", "fma")
+    if wl.kind == "sieve":
+        return {"fma": "prec=fma: register-tile terms with fused multiply-adds, double-double sum",
+                "exact": "prec=exact: every term in the reference's arithmetic, double-double sum"}[p]
+    return {"exact": "prec=exact: the reference's per-state order and rounding",
+            "fma": "prec=fma: fused multiply-adds",
+            "mixed": "prec=mixed: FP32 products, FP64 sums"}[p]
+
+
+def line_for(wl, name, m, steps, warmup, world, peaks, cpu, err):
+    roof = wl.roofline(m["ms"] / steps, peaks)
+    roof["traffic"] = profile_traffic(PROFILE_OF.get(name, ""))
+    return {
+        "workload_key": name, "value": m["value"], "unit": "hafnians/s", "steps": steps, "warmup": warmup,
+        "ms_per_step": m["ms"] / steps, "dtype": wl.dtype_name,
+        "config": {"workload": wl.name, "form": form_of(wl),
+                   **(wl.extra_config() if hasattr(wl, "extra_config") else {})},
+        "e2e": {"value": m["e2e"], "unit": "hafnians/s", "h2d_bytes_per_step": wl.h2d_bytes,
+                "d2h_bytes_per_step": wl.d2h_bytes, "path": "the public API from host memory, default arguments"},
+        "roofline": roof, "cpu_baseline": cpu, "rel_err": err, "gpu_launches": m["launches"],
+    }
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
 
     rank, world, local = dist_env()
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
+    D = Device(torch, local)
     if world > 1:
         from datetime import timedelta
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=D.dev)
     sys.path.insert(0, ROOT)
     egg = load_package()
     from theeggman_b200 import workloads as W
@@ -606,94 +841,54 @@ def run_ours(args):
     L = egg.lib()
     if L.egg_init(local) != 0:
         raise SystemExit(L.egg_last_error().decode())
-    wl = make_workload(args.workload, egg, W, rank)
-    wl.setup_device(torch, dev)
-    torch.cuda.synchronize(dev)
-    # A dedicated stream: the legacy default stream's handle is NULL, which the C ABI reads as
-    # "use the library's own stream", and events on one stream do not time work on another.
-    stream = torch.cuda.Stream(dev)
-    sp = stream.cuda_stream
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-
-    for _ in range(args.warmup):
-        wl.step_device(sp)
-    torch.cuda.synchronize(dev)
-
-    props = torch.cuda.get_device_properties(dev)
-    bus = getattr(props, "pci_bus_id", None)
-    if bus is None:
-        try:
-            bus = "%02x:%02x" % (props.pci_bus_id, props.pci_device_id)
-        except AttributeError:
-            bus = None
-    clocks = ClockSampler(str(bus) if bus is not None and not isinstance(bus, int) else None)
-    time.sleep(0.3)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    launches0 = L.egg_launch_count()
-    evs = []
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        wl.step_device(sp)
-        e1.record(stream)
-        evs.append((e0, e1))
-    torch.cuda.synchronize(dev)
-    launches = L.egg_launch_count() - launches0  # the library's own kernel launches, counted by it
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    ms = sum(a.elapsed_time(b) for a, b in evs)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps * wl.hafnians_per_step / (ms_max / 1e3)
-
-    # End to end through the public API, host arrays in and out.
-    for _ in range(max(1, args.warmup // 2)):
-        wl.step_e2e()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        wl.step_e2e()
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps * wl.hafnians_per_step / float(te.item())
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import oracle as O
-
-        O.build()
-        cores = O.max_threads()
-        rate, sample = wl.cpu_sample(cores)
-        cpu = {"value": rate, "unit": "hafnians/s", "cores": cores, "kind": "port", "sample": sample}
+    headline = args.workload or "sieve40"
+    wl = make_workload(headline, egg, W, rank)
+    wl.setup_device(torch, D.dev)
+    torch.cuda.synchronize(D.dev)
+    clocks = ClockSampler(D.bus_id())
+    m = measure(wl, D, L, args.steps, args.warmup, world, clocks)
 
     peaks = measured_peaks()
-    roof = wl.roofline(ms_max / args.steps, peaks)
-    roof["traffic"] = profile_traffic(PROFILE_OF.get(args.workload, ""))
+    solo = rank == 0 and world == 1 and not args.no_cpu_baseline
+    cpu, err = None, None
+    if solo:
+        O, cpu = cpu_leg(wl, args)
+        err = wl.check(O, m["dev_vals"], m["e2e_val"])
     if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "hafnians/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": wl.dtype_name, "data": "synthetic (seeded SplitMix64)",
-            "config": {"workload": wl.name, "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       **(wl.extra_config() if hasattr(wl, "extra_config") else {})},
-            "e2e": {"value": e2e_value, "unit": "hafnians/s", "h2d_bytes_per_step": wl.h2d_bytes,
-                    "d2h_bytes_per_step": wl.d2h_bytes, "path": "the public API from host memory"},
-            "roofline": roof,
-            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
-        }
-        print(json.dumps(line))
+        line = line_for(wl, headline, m, args.steps, args.warmup, world, peaks, cpu, err)
+        line.pop("workload_key")
+        line = {"metric": METRIC, **{k: line[k] for k in ("value", "unit")}, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": line["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": line["dtype"], "data": "synthetic (seeded SplitMix64)",
+                "config": {**line["config"], "l2": "flushed between steps (256 MiB write outside the timed events)",
+                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                "e2e": line["e2e"], "roofline": line["roofline"], "cpu_baseline": cpu, "rel_err": err,
+                "clocks": m["clocks"], "gpu_launches": m["launches"]}
+    # The other configurations of the metric, in the same process (single GPU, default run only).
+    if args.workload is None and world == 1 and not args.no_per_config:
+        per = []
+        t_start = time.perf_counter()
+        pclocks = ClockSampler(D.bus_id())
+        for name, cap in PER_CONFIG:
+            if time.perf_counter() - t_start > PER_CONFIG_BUDGET_S:
+                per.append({"workload_key": name, "skipped": "per-configuration time budget spent"})
+                continue
+            w2 = make_workload(name, egg, W, rank)
+            w2.setup_device(torch, D.dev)
+            torch.cuda.synchronize(D.dev)
+            st = min(args.steps, cap)
+            m2 = measure(w2, D, L, st, max(args.warmup, 3), world)
+            cpu2, err2 = None, None
+            if solo:
+                O, cpu2 = cpu_leg(w2, args)
+                err2 = w2.check(O, m2["dev_vals"], m2["e2e_val"])
+            per.append(line_for(w2, name, m2, st, max(args.warmup, 3), world, peaks, cpu2, err2))
+            del w2
+            torch.cuda.empty_cache()
+        line["per_config"] = per
+        line["per_config_clocks"] = pclocks.stop()
+    if rank == 0:
+        print(json.dumps(line, default=float))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -705,8 +900,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sieve40")
+    ap.add_argument("--workload", default=None,
+                    help="time one workload (default: the N = 40 sieve headline plus every configuration of the metric)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-per-config", action="store_true", help="time the headline only")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

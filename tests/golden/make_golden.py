@@ -14,6 +14,8 @@ produce vectors.  The fixtures are therefore:
      uses for its gold values (test/runtests.jl:123-133).
   4. Repeated-row cases: hafnian_repeated(A, rpt) gold via the expanded matrix
      (reduction, src/hafnian.jl:1369-1374) at 256 bits.
+  5. N = 24 matrices drawn from the N = 40 sieve workloads' distributions (real U[-1, 1]/sqrt(N),
+     complex parts N(0, 1/(2N))), gold by the memoised recursion at 256 bits.
 
 Numbers are stored as hex floats (complex as [re, im]) so they round-trip exactly.
 Run:  python tests/golden/make_golden.py
@@ -139,6 +141,19 @@ def main():
             cases.append({"N": N, "kind": kind, "seed": seed, "A": enc_matrix(A), "gold": enc_mp(memo_mp(A)),
                           "how": "memoised subset recursion, 256-bit"})
     out["random"] = cases
+
+    # The distributions of the N = 40 sieve workloads, at N = 24 where 256-bit gold is cheap (the
+    # error check BASELINE's sieve configuration asks for, and the N of the reference's own
+    # envelope test, test/runtests.jl:123-133): real U[-1, 1]/sqrt(N), complex parts N(0, 1/(2N)).
+    c2 = []
+    for i in range(4):
+        for kind in ("real", "complex"):
+            N = 24
+            seed = 2400 + 10 * i + (kind == "complex")
+            A = W.dense_real(N, seed, scale=1.0 / np.sqrt(N)) if kind == "real" else W.dense_complex(N, seed, 1.0 / (2 * N))
+            c2.append({"N": N, "kind": kind, "seed": seed, "A": enc_matrix(A), "gold": enc_mp(memo_mp(A)),
+                       "how": "memoised subset recursion, 256-bit"})
+    out["config2_n24"] = c2
 
     rep = []
     for i, rpt in enumerate(([2, 2, 2], [1, 2, 3, 2], [6, 6], [3, 3, 3, 3], [8, 4], [5, 5, 1, 1], [4, 1, 1], [0, 2, 2],
