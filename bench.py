@@ -4,8 +4,9 @@
 
 The default workload is the N = 40 sieve of configuration 2(a): one real symmetric 40 x 40 matrix
 with entries U[-1, 1]/sqrt(40), hafnian(A; method = :sieve), which the reference runs as
-inclusion-exclusion (2^20 terms; its cost model's choice for distinct rows).  A step is one full
-hafnian.  Under torchrun every rank computes its own matrix (seed + rank): the sieve instances are
+inclusion-exclusion (2^20 terms; its cost model's choice for distinct rows), every term in the
+reference's arithmetic (the API default).  A step is one full hafnian.  The default run then times
+every other configuration of the metric in the same process (the `per_config` list).  Under torchrun every rank computes its own matrix (seed + rank): the sieve instances are
 independent, so N GPUs run N replicas with no data-path collective ("scaling": "weak"); the only
 collectives are the timing barrier and the max-over-ranks reduction.
 
@@ -95,7 +96,7 @@ class SieveWorkload:
 
     kind = "sieve"
 
-    def __init__(self, egg, W, N: int, cplx: bool, glynn, seed: int, config: str = "2", prec: str = "fma"):
+    def __init__(self, egg, W, N: int, cplx: bool, glynn, seed: int, config: str = "2", prec: str = "exact"):
         from theeggman_b200 import policy as pol
         from theeggman_b200 import roofline as R
 
@@ -115,8 +116,8 @@ class SieveWorkload:
         self.reps = np.ones(E, dtype=np.int64)
         self.flops = R.sieve_flops([1] * E, self.glynn, cplx)
         self.dtype = 1 if cplx else 0
-        # "fma": the register-resident kernels with fused multiply-adds (the API default for the
-        # sieve); "exact": every term in the reference's arithmetic.
+        # "exact": every term in the reference's arithmetic (the API default); "fma": the register
+        # tiles with fused multiply-adds.
         self.prec_name = prec
         self.prec = {"exact": 0, "fma": 1}[prec]
         self.hafnians_per_step = 1
@@ -143,7 +144,7 @@ class SieveWorkload:
         # The public call with its defaults (symmetry check included); the variant is left to the
         # cost model unless the workload forces one, and prec is passed only when not the default.
         kw = {"glynn": self.glynn} if self.forced_glynn else {}
-        if self.prec_name != "fma":
+        if self.prec_name != "exact":
             kw["prec"] = self.prec_name
         return self.egg.hafnian(self.A, method="sieve", **kw)
 
@@ -463,11 +464,13 @@ class RepeatedWorkload:
 
     kind = "sieve"
 
-    def __init__(self, egg, W, which: str, B: int, seed: int):
+    def __init__(self, egg, W, which: str, B: int, seed: int, prec: str = "exact"):
         from theeggman_b200 import roofline as R
         from theeggman_b200 import policy as pol
 
         self.egg = egg
+        self.prec_name = prec
+        self.prec = {"exact": 0, "fma": 1}[prec]
         if which == "a":
             mats, rpts = W.repeated_real(B, 14, seed)
             self.cplx = False
@@ -514,7 +517,7 @@ class RepeatedWorkload:
     def step_device(self, stream_ptr):
         # The instance tables are host-side and tiny; the matrices stay resident.
         L = self.egg.lib()
-        rc = L.egg_sieve_batch_device(1 if self.cplx else 0, 1, self.B, self.Emax, self.dslab.data_ptr(),
+        rc = L.egg_sieve_batch_device(1 if self.cplx else 0, self.prec, self.B, self.Emax, self.dslab.data_ptr(),
                                       self.E.ctypes.data, self.reps.ctypes.data, self.g.ctypes.data,
                                       self.dout.data_ptr(), stream_ptr)
         if rc:
@@ -524,7 +527,8 @@ class RepeatedWorkload:
         from theeggman_b200.hafnian import _sieve_device_batch
 
         return _sieve_device_batch(np.dtype(np.complex128 if self.cplx else np.float64), [a for a, _, _ in self.inst],
-                                   [er for _, er, _ in self.inst], [g for _, _, g in self.inst], "fma")
+                                   [er for _, er, _ in self.inst], [g for _, _, g in self.inst],
+                                   None if self.prec_name == "exact" else self.prec_name)
 
     def device_result(self):
         raw = self.dout.cpu().numpy()
@@ -567,18 +571,24 @@ class RepeatedWorkload:
 
 
 def make_workload(name: str, egg, W, rank: int):
+    # Sieve workloads run the reference's arithmetic (the API default) unless their name ends in
+    # "f": the fused-multiply-add register tiles.
     if name == "sieve40":
         return SieveWorkload(egg, W, 40, False, None, 2024 + rank)
-    if name == "sieve40x":
-        return SieveWorkload(egg, W, 40, False, None, 2024 + rank, prec="exact")
+    if name == "sieve40f":
+        return SieveWorkload(egg, W, 40, False, None, 2024 + rank, prec="fma")
     if name == "sieve40c":
         return SieveWorkload(egg, W, 40, True, None, 2025 + rank)
-    if name == "sieve40cx":
-        return SieveWorkload(egg, W, 40, True, None, 2025 + rank, prec="exact")
+    if name == "sieve40cf":
+        return SieveWorkload(egg, W, 40, True, None, 2025 + rank, prec="fma")
     if name == "sieve40g":
         return SieveWorkload(egg, W, 40, False, True, 2024 + rank)
+    if name == "sieve40gf":
+        return SieveWorkload(egg, W, 40, False, True, 2024 + rank, prec="fma")
     if name == "sieve20":
         return SieveWorkload(egg, W, 20, False, None, 2020 + rank, config="1")
+    if name == "sieve20f":
+        return SieveWorkload(egg, W, 20, False, None, 2020 + rank, config="1", prec="fma")
     if name == "dp20":
         return DPWorkload(egg, W, 20, 1, "f64", "exact", 2020 + rank)
     if name == "dp32":
@@ -601,8 +611,12 @@ def make_workload(name: str, egg, W, rank: int):
         return MixWorkload(egg, W, 4096, "exact", True, 4 + 100 * rank)
     if name == "rep14":
         return RepeatedWorkload(egg, W, "a", 1024, 5 + 100 * rank)
+    if name == "rep14f":
+        return RepeatedWorkload(egg, W, "a", 1024, 5 + 100 * rank, prec="fma")
     if name == "rep20c":
         return RepeatedWorkload(egg, W, "b", 1024, 6 + 100 * rank)
+    if name == "rep20cf":
+        return RepeatedWorkload(egg, W, "b", 1024, 6 + 100 * rank, prec="fma")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -701,10 +715,10 @@ def run_reference(args):
 # metric with its own value, e2e, roofline, CPU baseline and error against the oracle.  (name,
 # timed steps at most): the heavy end-to-end forms take fewer steps so that the whole default run
 # stays within a few minutes.
-PER_CONFIG = [("dp20", 20), ("sieve20", 20), ("dp32", 10), ("sieve40", 10), ("sieve40x", 5), ("sieve40c", 5),
-              ("sieve40cx", 3), ("sieve40g", 5), ("dp36", 5), ("dp40", 5), ("dp40mixed", 5), ("dp40int", 5),
-              ("dp20x1024", 10), ("mix4096", 10), ("mix4096mixed", 10), ("mix4096seq", 3), ("rep14", 10),
-              ("rep20c", 3)]
+PER_CONFIG = [("dp20", 20), ("sieve20", 20), ("sieve20f", 20), ("dp32", 10), ("sieve40", 10), ("sieve40f", 10),
+              ("sieve40c", 3), ("sieve40cf", 5), ("sieve40gf", 5), ("dp36", 5), ("dp40", 5), ("dp40mixed", 5),
+              ("dp40int", 5), ("dp20x1024", 10), ("mix4096", 10), ("mix4096mixed", 10), ("mix4096seq", 3),
+              ("rep14", 10), ("rep14f", 10), ("rep20cf", 3)]
 PER_CONFIG_BUDGET_S = 300.0
 
 

@@ -5,7 +5,7 @@ in double-double, so the device result is compared with the oracle summing the s
 double-double (sum_mode 1): the bar is 1e-15 relative (in practice they are equal).  Against the
 reference's own plain FP64 summation the difference is bounded by that summation's rounding.
 
-prec="fma" (the default, register-resident kernels): each term differs from the reference's by its
+prec="fma" (the register-resident fused-multiply-add kernels): each term differs from the reference's by its
 own rounding (fused multiply-adds, a Newton reciprocal, another pivot among near-equal candidates),
 and the sieve's alternating sum magnifies that by kappa = sum|terms| / |result|.  The bar is the
 rounding-error bound 4 N eps kappa (+1e-15), with kappa computed from the oracle's terms.
@@ -84,7 +84,7 @@ def test_repeated_rows_mixed_radix(egg, orc, golden):
             got = egg.sieve(Ax, er, glynn=glynn, prec="exact")
             assert rel(got, dd) <= 1e-15, (rpt, glynn)
             assert rel(got, g) < 1e-10, (rpt, glynn)
-            fast = egg.sieve(Ax, er, glynn=glynn)
+            fast = egg.sieve(Ax, er, glynn=glynn, prec="fma")
             assert rel(fast, dd) <= 4 * 2 * len(er) * EPS * kappa(orc, Ax, er, glynn, dd) + 1e-15, (rpt, glynn)
             assert rel(fast, g) < 1e-10, (rpt, glynn)
         assert rel(egg.hafnian_repeated(A, rpt, method="sieve"), g) < 1e-10
@@ -170,7 +170,7 @@ def test_batch_mixes_subset_and_odometer_instances(egg, orc, W, cplx):
         dd = orc.calc_hafnian(Ax, er, g, sum_mode=1)
         tol = 4 * 2 * sum(er) * EPS * kappa(orc, Ax, er, g, dd) + 1e-15
         assert rel(v, dd) <= tol, (er, g, v, dd)
-        assert rel(v, egg.sieve(Ax, er, glynn=g)) <= 1e-15
+        assert rel(v, egg.sieve(Ax, er, glynn=g, prec="fma")) <= 1e-15
 
 
 @pytest.mark.parametrize("cplx", [False, True])
@@ -199,7 +199,7 @@ def test_batch_sharing_multiplicity_patterns(egg, orc, W, cplx):
         dd = orc.calc_hafnian(Ax, er, g, sum_mode=1)
         tol = 4 * 2 * sum(er) * EPS * kappa(orc, Ax, er, g, dd) + 1e-15
         assert rel(v, dd) <= tol, (er, g, v, dd)
-        assert rel(v, egg.sieve(Ax, er, glynn=g)) <= 1e-14
+        assert rel(v, egg.sieve(Ax, er, glynn=g, prec="fma")) <= 1e-14
 
 
 @pytest.mark.parametrize("glynn", [False, True])
@@ -233,7 +233,7 @@ def test_device_entry_point_orders_with_the_caller_stream(egg, W):
         E = N // 2
         A = W.dense_complex(N, 600 + N, 0.5) if cplx else W.dense_real(N, 600 + N, scale=1.0 / np.sqrt(N))
         Ax = A[np.ix_(np.array(distinct_x(E)) - 1, np.array(distinct_x(E)) - 1)]
-        host = egg.sieve(Ax, [1] * E)
+        host = egg.sieve(Ax, [1] * E, prec="fma")
         src = torch.from_numpy(np.ascontiguousarray(Ax.T)).to(dev)  # column-major bytes
         dA = torch.zeros_like(src)
         out = torch.full((2,), float("nan"), dtype=torch.float64, device=dev)

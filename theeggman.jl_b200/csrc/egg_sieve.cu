@@ -620,13 +620,15 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     }
     const int Ews = (int)(Emax > 0 ? Emax : 1);
 
-    // Which kernels run: in FMA mode, each popcount level that some instance has terms in, on the
-    // register tiles (orders n <= 31, one lane per coefficient); the exact kernel takes everything
-    // in exact mode, else whatever exceeds the tiles.
-    const bool fast_ok = prec == EGG_PREC_FMA && nmax <= 31;
+    // Which kernels run: each popcount level that some instance has terms in, on the register tiles
+    // (orders n <= 31, one lane per coefficient) -- with fused multiply-adds, or for real terms of
+    // up to 32 rows in the reference's arithmetic -- and the shared-memory exact kernel for
+    // whatever exceeds the tiles (every complex term in exact mode).
+    const bool exact = prec == EGG_PREC_EXACT;
+    const bool fast_ok = nmax <= 31 && (!exact || !cplx);
     bool all_subset = true;
     for (const SieveInst &si : inst) all_subset = all_subset && si.subset;
-    const int fast_hi = cplx ? 32 : 48;
+    const int fast_hi = cplx ? 32 : (exact ? 32 : 48);
 
     // Term lists for the fast kernels: instances that share a multiplicity pattern (a batch of
     // hafnian_repeated(B, rpt) with one rpt) share one list per level of their terms' digits, so
@@ -747,7 +749,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         const int k = inst[0].E;
         const bool narrow = 2 * k <= 16;
         int cw = 0, bps = 0;
-        int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, &cw, &bps) : level_shape_real(nmax, k, narrow, &cw, &bps);
+        int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, &cw, &bps) : level_shape_real(nmax, k, narrow, exact, &cw, &bps);
         if (rc0) return rc0;
         if (bps < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
         const int64_t terms_all = ((int64_t)1 << k) - 1, per_block = (int64_t)cw * (narrow ? 2 : 1);
@@ -783,9 +785,9 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             if (lvl[(size_t)k] <= 0.0) continue;
             const bool narrow = 2 * k <= 16 && e_odo <= 16;
             int cw = 0, bps = 0;
-            int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, &cw, &bps) : level_shape_real(nmax, k, narrow, &cw, &bps);
+            int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, &cw, &bps) : level_shape_real(nmax, k, narrow, exact, &cw, &bps);
             if (rc0) return rc0;
-            if (bps < 1 || (size_t)cw * (narrow ? 2 : 1) * fast_ws_bytes(nmax, cplx, 2 * k) > 220 * 1024)
+            if (bps < 1 || (size_t)cw * (narrow ? 2 : 1) * level_ws_bytes(nmax, cplx, k, exact) > 220 * 1024)
                 return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
             // Distinct-row levels deal equal shares: one wave.  Odometer runs are only balanced on
             // average and instances differ in size, so those levels get several waves of blocks for
@@ -886,6 +888,11 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.nmax = nmax;
     a.skip_le = skip_le;
     a.terms = terms;
+    if (terms) {
+        // Terms with no surviving edge are zero (src/hafnian.jl:566-567); every other term is
+        // written by the kernel that evaluates it.
+        EGG_CUDA_TRY(cudaMemsetAsync(terms, 0, (size_t)inst[0].steps * (cplx ? 16 : 8), st));
+    }
     PartialSet ps;
     for (int k = 0; k < kMaxPartials; ++k) {
         ps.p[k] = nullptr;
@@ -933,10 +940,10 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             if (side_ok && L.side) ls = c.side[next_side++ % Context::kSideStreams];
             if (fused)
                 rc = cplx ? level_launch_all_cplx(a, L.level, L.narrow, part, L.bx, ls)
-                          : level_launch_all_real(a, L.level, L.narrow, part, L.bx, ls);
+                          : level_launch_all_real(a, L.level, L.narrow, exact, part, L.bx, ls);
             else
                 rc = cplx ? level_launch_cplx(a, dstr, (int)B, L.level, L.narrow, part, L.bx, ls)
-                          : level_launch_real(a, dstr, (int)B, L.level, L.narrow, part, L.bx, ls);
+                          : level_launch_real(a, dstr, (int)B, L.level, L.narrow, exact, part, L.bx, ls);
             if (rc) return rc;
             ps.p[slot] = part;
             ps.w[slot] = L.bx;

@@ -43,22 +43,28 @@ constexpr int kFusedMaxE = 10;
 constexpr int kLevelMaxReal = 24, kLevelMaxCplx = 16;
 constexpr int kMaxPartials = 26;  // the exact kernel and up to 25 level launches
 size_t fast_ws_bytes(int nmax, int cplx, int mhi);  // one warp's scratch for a tile of mhi columns
+// One group's shared workspace of level k's kernel (the real tiles of up to 32 rows hold the
+// reference-arithmetic form's term buffer too when `exact`).
+size_t level_ws_bytes(int nmax, int cplx, int k, bool exact);
 // Launches level k on a grid of blocks_x x B blocks; a.warps_per_inst must be blocks_x times the
 // level's warps per block.  Each block writes one partial (re, im) per instance.  `narrow` puts
 // two terms in each warp for tiles of up to 16 rows (odometer instances then need E <= 16).
-int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
-                      cudaStream_t st);
+// `exact` (real levels 1..16 only) evaluates every term in the reference's arithmetic; with
+// a.terms set those kernels write each term's signed value at its index instead of summing.
+int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, bool exact, dd *partial,
+                      int blocks_x, cudaStream_t st);
 int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
                          cudaStream_t st);
 // One distinct-row instance (B = 1) of k <= kFusedMaxE edges in one launch: every nonzero edge
 // subset, each on the tile of m = 2k columns, the blocks' partials summed inside the launch into
-// a.fused_out.  A separate instantiation of the level kernel, so the level launches are unchanged.
-int level_launch_all_real(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st);
+// a.fused_out (when set).  A separate instantiation of the level kernel, so the level launches are
+// unchanged.
+int level_launch_all_real(const SieveArgs &a, int k, bool narrow, bool exact, dd *partial, int blocks_x, cudaStream_t st);
 int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st);
 int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
                       cudaStream_t st);
 // The level's block size in warps and how many of its blocks one SM holds.
-int level_shape_real(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm);
+int level_shape_real(int nmax, int k, bool narrow, bool exact, int *warps_per_block, int *blocks_per_sm);
 int level_shape_real_hi(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm);
 int level_shape_cplx(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm);
 

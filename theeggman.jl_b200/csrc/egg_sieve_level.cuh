@@ -17,19 +17,21 @@
 // Each block writes one partial (re, im) per instance: its warps' double-double sums added in a
 // fixed order.
 #pragma once
-#include "egg_sieve_fast.cuh"
+#include "egg_sieve_tile.cuh"
 
 namespace egg {
 
 // 128-thread blocks; resident blocks per SM from the tile's register need (65536 / (128 * blocks)
 // registers per thread): a real tile holds m doubles per row, a complex one 2m.
-template <bool CPLX, int K, int G = 32>
+// The reference-arithmetic tiles keep more values live per step (separately rounded products, the
+// buffered term series), so from 24 rows on they take one block fewer.
+template <bool CPLX, int K, int G = 32, bool EXACT = false>
 struct LevelShape {
     static constexpr int MW = 2 * K;
     static constexpr int threads = 128;
     static constexpr int full =
         CPLX ? (MW <= 8 ? 6 : (MW <= 10 ? 5 : (MW <= 16 ? 4 : (MW <= 24 ? 3 : 2))))
-             : (MW <= 8 ? 8 : (MW <= 12 ? 7 : (MW <= 18 ? 6 : (MW <= 26 ? 5 : (MW <= 32 ? 4 : 2)))));
+             : (MW <= 8 ? 8 : (MW <= 12 ? 7 : (MW <= 18 ? 6 : (MW <= (EXACT ? 22 : 26) ? 5 : (MW <= 32 ? 4 : 2)))));
     // Two terms per warp need more registers per thread (the series holds two coefficients per
     // lane); one block fewer still keeps more terms in flight.
     static constexpr int min_blocks = G == 32 ? full : (full > 2 ? full - 1 : 1);
@@ -44,13 +46,42 @@ constexpr int level_group(bool narrow)
     return (narrow && 2 * K <= 16) ? 16 : 32;
 }
 
+// In the reference's arithmetic, real terms of up to 32 rows run on the tile whose columns stay in
+// logical order (egg_sieve_tile.cuh).  With fused multiply-adds every term runs on the relabelled
+// tiles of egg_sieve_fast.cuh, which move no data on a pivot swap and so keep their code compact.
+template <bool CPLX, int K, bool EXACT>
+constexpr bool level_tile() { return EXACT && !CPLX && 2 * K <= 32; }
+
+// One group's shared workspace, in doubles.
+template <bool CPLX, int K, bool EXACT>
+__host__ __device__ inline size_t level_ws_doubles(int nmax)
+{
+    if constexpr (level_tile<CPLX, K, EXACT>()) return tile_ws_doubles(nmax, 2 * K, EXACT);
+    else return fast_ws_doubles(nmax, CPLX, 2 * K);
+}
+
+// Term value of one lane's buffered term (EXACT): the series of its q vector, times its prefactor.
+// Deterministic sum of a group's buffered terms: a fixed shuffle tree of double-double values.
+__device__ __forceinline__ dd group_tree_sum(dd v, unsigned gm, int G)
+{
+    for (int off = G / 2; off > 0; off >>= 1) {
+        const dd o{__shfl_down_sync(gm, v.hi, off, G), __shfl_down_sync(gm, v.lo, off, G)};
+        dd_add(v, o);
+    }
+    return v;
+}
+
 // ALL: the all-levels mode of one small distinct-row instance (level_launch_all_*), a separate
-// instantiation.
-template <bool CPLX, int K, int G, bool ALL = false>
-__global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CPLX, K, G>::min_blocks)
+// instantiation.  EXACT: every term in the reference's arithmetic (real tiles only); the term
+// series are evaluated in batches of G terms, one term per lane, and with a.terms set each term's
+// signed value is written at its index instead of being summed.
+template <bool CPLX, int K, int G, bool ALL = false, bool EXACT = false>
+__global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT>::threads, LevelShape<CPLX, K, G, EXACT>::min_blocks)
     sieve_level_kernel(SieveArgs a, const int64_t *__restrict__ strides, dd *partial)
 {
     constexpr int MW = 2 * K;
+    constexpr bool TILE = level_tile<CPLX, K, EXACT>();
+    static_assert(!EXACT || TILE, "the exact form runs on the real tile");
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
     constexpr int NG = 32 / G;   // groups per warp
     constexpr int GB = cw * NG;  // groups per block
@@ -61,25 +92,70 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
     const int b = blockIdx.y;
     const SieveInst in = a.inst[b];
     const int E = in.E, n = in.n;
-    const FastWs w = fast_carve(smem + (size_t)grp * fast_ws_doubles(a.nmax, CPLX, MW), a.nmax, CPLX, MW);
+    double *wbase = smem + (size_t)grp * level_ws_doubles<CPLX, K, EXACT>(a.nmax);
+    FastWs wf{};
+    const TileWs<MW> wt{wbase};
+    if constexpr (!TILE) wf = fast_carve(wbase, a.nmax, CPLX, MW);
+    int *const eidx = TILE ? wt.eidx() : wf.eidx;
+    double *const kval = TILE ? wt.kval() : wf.kval;
     const int gslot = blockIdx.x * GB + grp;
     const uint64_t W = (uint64_t)a.warps_per_inst * NG;  // groups per instance
     dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
-    // One term: the surviving edges are compacted into w.eidx / w.kval (mE of them, mE = K except
-    // in the all-levels mode) by the caller.
-    auto eval_term = [&](double prefac, int mE) {
-        if constexpr (!CPLX) {
-            const double val = term_real<MW, (MW > 32 ? 2 : 1), G>((const double *)a.Ax + in.ax_off, in.lda, E,
-                                                                   ALL ? mE : K, n, w, gl, gm);
-            if (gl == 0) dd_add(acc_re, prefac * val);
-        } else {
-            const cd val = term_cplx<MW, G>((const cd *)a.Ax + in.ax_off, in.lda, E, ALL ? mE : K, n, w, gl, gm);
+    // EXACT: the group's buffered terms (slot s: q vector at qbuf + s * (nmax + 1), prefactor,
+    // index and size at pre[s], jx[s], mx[s]).
+    int nbuf = 0;
+    auto flush = [&]() {
+        if constexpr (EXACT) {
+            __syncwarp(gm);
+            double v = 0.0;
+            if (gl < nbuf) {
+                double f[32];
+                const double val = series_exact(wt.qbuf() + (size_t)gl * (a.nmax + 1), f, wt.mx()[gl], n);
+                v = __dmul_rn(wt.pre()[gl], val);
+                if (a.terms) a.terms[wt.jx()[gl]] = v;
+            }
+            if (!a.terms) {
+                const dd t = group_tree_sum(dd{v, 0.0}, gm, G);
+                if (gl == 0) dd_add(acc_re, t);
+            }
+            nbuf = 0;
+            __syncwarp(gm);
+        }
+    };
+    // One term: the surviving edges are compacted into eidx / kval (mE of them, mE = K except in
+    // the all-levels mode) by the caller; jidx is the term's index (used with a.terms).
+    auto eval_term = [&](double prefac, int mE, int64_t jidx) {
+        if constexpr (CPLX) {
+            const cd val = term_cplx<MW, G>((const cd *)a.Ax + in.ax_off, in.lda, E, ALL ? mE : K, n, wf, gl, gm);
             if (gl == 0) {
                 dd_add(acc_re, prefac * val.re);
                 dd_add(acc_im, prefac * val.im);
             }
+        } else if constexpr (TILE) {
+            const int mm = 2 * (ALL ? mE : K);
+            term_real_tile<MW, G, EXACT>((const double *)a.Ax + in.ax_off, in.lda, E, ALL ? mE : K, n, wt, gl, gm);
+            {
+                // Buffer q_1..q_min(m,n) in slot nbuf; the lane of that slot keeps the rest.
+                double *dst = wt.qbuf() + (size_t)nbuf * (a.nmax + 1);
+                const int jm = mm < n ? mm : n;
+                for (int j = 1 + gl; j <= jm; j += G) dst[j] = wt.q()[j];
+                if (gl == 0) {
+                    wt.pre()[nbuf] = prefac;
+                    wt.mx()[nbuf] = mm;
+                    wt.jx()[nbuf] = jidx;
+                }
+                if (++nbuf == G) flush();
+                __syncwarp(gm);
+            }
+        } else {
+            const double val = term_real<MW, (MW > 32 ? 2 : 1), G>((const double *)a.Ax + in.ax_off, in.lda, E,
+                                                                   ALL ? mE : K, n, wf, gl, gm);
+            if (gl == 0) dd_add(acc_re, prefac * val);
         }
     };
+    // The index of the term whose edge subset is S (edge i at bit E-1-i of the index, as the
+    // odometer's edge E-1 is least significant).
+    auto subset_index = [&](uint32_t S) -> int64_t { return E ? (int64_t)(__brev(S) >> (32 - E)) : 0; };
     // The group's lanes of a warp vote, as bits 0..G-1.
     auto group_ballot = [&](bool p) -> unsigned {
         const unsigned v = __ballot_sync(gm, p);
@@ -87,157 +163,164 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
     };
     // Each round every group first finds its next term, then the warp evaluates them together (the
     // groups of a warp stay converged through the term), until no group of the warp has one left.
-    if constexpr (ALL) {
-        // Every nonzero edge subset of the one instance (E <= K): subset r + 1 for r = gslot,
-        // gslot + W, ...; a term of k edges has m = 2k <= MW rows.
-        const uint64_t cnt = ((uint64_t)1 << E) - 1;
-        for (uint64_t r = gslot;; r += W) {
-            const bool has = r < cnt;
-            if (!__any_sync(FULL, has)) break;
-            if (has) {
-                const uint32_t S = (uint32_t)r + 1u;
-                const int k = __popc(S);
-                const double prefac = ((n - k) & 1) ? -1.0 : 1.0;
-                for (int e = gl; e < E; e += G)
-                    if ((S >> e) & 1u) {
-                        const int pos = __popc(S & ((1u << e) - 1u));
-                        w.eidx[pos] = e;
-                        w.kval[pos] = 1.0;
-                    }
-                __syncwarp(gm);
-                eval_term(prefac, k);
-                __syncwarp(gm);
-            }
-        }
-    } else if (in.subset && K <= E) {
+    // Every way of dealing terms feeds the one evaluation below, so that it is compiled once.
+    //
+    //   * ALL: every nonzero edge subset of the one instance (E <= K): subset r + 1 for
+    //     r = gslot, gslot + W, ...; a term of k edges has m = 2k <= MW rows.
+    //   * subsets: all multiplicities 1 under inclusion-exclusion, so the level's terms are the
+    //     K-subsets of the edges; the group takes an equal share of them (one colex unrank, then
+    //     successors).
+    //   * lists: the level's terms listed by digits (a multiplicity pattern shared by instances of
+    //     the batch); the group takes an equal share of the list.  Lane i of the group takes digit i
+    //     (E <= 16 here), and the term is set up as on the odometer.
+    //   * odometer: the mixed-radix odometer (src/hafnian.jl:542-580): lane i of the group holds
+    //     digit i (edge E-1 least significant; E <= G here), digit 0 clipped to its lower half under
+    //     Glynn.  Runs of kRunTerms consecutive indices are dealt round robin: a term's size is set
+    //     by its digits, and a long contiguous range fixes the high digits, so contiguous ranges
+    //     would hand some groups most of a level and others none of it.
+    enum { kAll, kSubset, kList, kOdometer, kNone };
+    const int mode = ALL ? kAll : (K > E ? kNone : (in.subset ? kSubset : (in.pattern >= 0 ? kList : kOdometer)));
+    const int *reps = a.reps + in.reps_off;
+    const int mr1 = a.maxrep + 1;
+    const bool unit = a.maxrep <= 1;  // all multiplicities <= 1: every binomial factor is 1
+    constexpr int64_t kRunTerms = 16;
+    // ALL: rk is the next subset; subsets and lists: the group's share is [lo, hi), rk the next;
+    // odometer: the current run is [lo, hi), rk the next index.
+    int64_t rk = 0, lo = 0, hi = 0;
+    uint32_t S = 0;
+    int64_t lb = 0;
+    int r = 0, base = 1, digit = 0;  // odometer and lists: this lane's multiplicity, radix and digit
+    if (mode == kAll) {
+        rk = gslot;
+    } else if (mode == kSubset) {
         const uint64_t cnt = c_fast.binom[E * 33 + K];
-        const uint64_t lo = (uint64_t)gslot * cnt / W, hi = ((uint64_t)gslot + 1) * cnt / W;
-        const double prefac = ((n - K) & 1) ? -1.0 : 1.0;  // (-1)^(n - k), every binomial factor 1
-        uint32_t S = lo < hi ? subset_unrank(E, K, (uint32_t)lo) : 0u;
-        for (uint64_t rk = lo;; ++rk) {
-            const bool has = rk < hi;
-            if (!__any_sync(FULL, has)) break;
-            if (has) {
-                if (rk > lo) S = subset_next(S);
-                for (int e = gl; e < E; e += G)
-                    if ((S >> e) & 1u) {
-                        const int pos = __popc(S & ((1u << e) - 1u));
-                        w.eidx[pos] = e;
-                        w.kval[pos] = 1.0;
-                    }
-                __syncwarp(gm);
-                eval_term(prefac, K);
-                __syncwarp(gm);
-            }
-        }
-    } else if (in.pattern >= 0 && K <= E) {
-        // The level's terms listed by digits (a multiplicity pattern shared by instances of the
-        // batch): every group takes an equal share of the list, as for subsets.  Lane i of the group
-        // takes digit i (E <= 16 here), and the term is set up as on the odometer below.
+        lo = (int64_t)((uint64_t)gslot * cnt / W);
+        hi = (int64_t)(((uint64_t)gslot + 1) * cnt / W);
+        rk = lo;
+        S = lo < hi ? subset_unrank(E, K, (uint32_t)lo) : 0u;
+    } else if (mode == kList) {
         const int64_t lrow = (int64_t)in.pattern * a.list_stride + K;
-        const int64_t lb = a.list_off[lrow];
+        lb = a.list_off[lrow];
         const uint64_t cnt = (uint64_t)(a.list_off[lrow + 1] - lb);
-        const uint64_t lo = (uint64_t)gslot * cnt / W, hi = ((uint64_t)gslot + 1) * cnt / W;
-        const int *reps = a.reps + in.reps_off;
-        const int mr1 = a.maxrep + 1;
-        const bool unit = a.maxrep <= 1;
-        const int r = gl < E ? reps[gl] : 0;
-        for (uint64_t rk = lo;; ++rk) {
-            const bool has = rk < hi;
-            if (!__any_sync(FULL, has)) break;
-            if (has) {
-                const uint64_t word = a.lists[lb + (int64_t)rk];
-                const int digit = gl < E ? (int)((word >> (4 * gl)) & 15u) : 0;
-                const int kk = gl < E ? (in.glynn ? 2 * digit - r : digit) : 0;
-                const bool nz = gl < E && kk != 0;
-                const unsigned mask = group_ballot(nz);
-                const int esum = __reduce_add_sync(gm, gl < E ? digit : 0);
-                double bp = 1.0;
-                if (!unit) {
-                    bp = gl < E ? a.binoms[r + digit * mr1] : 1.0;
-                    for (int off = G / 2; off > 0; off >>= 1) bp *= __shfl_xor_sync(gm, bp, off, G);
-                }
-                double prefac = ((n - esum) & 1) ? -bp : bp;
-                const int k0 = __shfl_sync(gm, kk, 0, G);
-                if (in.glynn && k0 == 0) prefac *= 0.5;  // the mirror's fixed point (:570-573)
-                if (nz) {
-                    const int pos = __popc(mask & ((1u << gl) - 1u));
-                    w.eidx[pos] = gl;
-                    w.kval[pos] = (double)kk;
-                }
-                __syncwarp(gm);
-                eval_term(prefac, K);
-                __syncwarp(gm);
-            }
-        }
-    } else if (K <= E) {
-        // Mixed-radix odometer (src/hafnian.jl:542-580): lane i of the group holds digit i (edge
-        // E-1 least significant; E <= G here), digit 0 clipped to its lower half under Glynn.  Runs
-        // of kRunTerms consecutive indices are dealt round robin: a term's size is set by its
-        // digits, and a long contiguous range fixes the high digits, so contiguous ranges would hand
-        // some groups most of a level and others none of it.
-        const int *reps = a.reps + in.reps_off;
-        const int mr1 = a.maxrep + 1;
-        const bool unit = a.maxrep <= 1;  // all multiplicities <= 1: every binomial factor is 1
-        int r = 0, base = 1, digit = 0;
+        lo = (int64_t)((uint64_t)gslot * cnt / W);
+        hi = (int64_t)(((uint64_t)gslot + 1) * cnt / W);
+        rk = lo;
+        r = gl < E ? reps[gl] : 0;
+    } else if (mode == kOdometer) {
         if (gl < E) {
             r = reps[gl];
             base = (in.glynn && gl == 0) ? (r + 2) / 2 : r + 1;
         }
-        constexpr int64_t kRunTerms = 16;
-        int64_t j0 = (int64_t)gslot * kRunTerms;
-        int64_t j = j0, j1 = j0 < in.steps ? (j0 + kRunTerms < in.steps ? j0 + kRunTerms : in.steps) : j0;
-        if (gl < E && j0 < in.steps) digit = (int)((j0 / strides[in.reps_off + gl]) % base);
-        for (;;) {
-            bool has = false;
-            double prefac = 0.0;
-            while (j < j1) {
+        lo = (int64_t)gslot * kRunTerms;
+        rk = lo;
+        hi = lo < in.steps ? (lo + kRunTerms < in.steps ? lo + kRunTerms : in.steps) : lo;
+        if (gl < E && lo < in.steps) digit = (int)((lo / strides[in.reps_off + gl]) % base);
+    }
+    // Sets this group's next term up (eidx/kval, prefactor, surviving edges, index) for a digit
+    // vector held one digit per lane: the Glynn substitution, the binomial product and the sign.
+    auto setup_digits = [&](int dg, double &prefac, int64_t &jidx, bool want_index) -> void {
+        const int kk = gl < E ? (in.glynn ? 2 * dg - r : dg) : 0;
+        const bool nz = gl < E && kk != 0;
+        const unsigned mask = group_ballot(nz);
+        const int esum = __reduce_add_sync(gm, gl < E ? dg : 0);
+        double bp = 1.0;
+        if (!unit) {
+            bp = gl < E ? a.binoms[r + dg * mr1] : 1.0;
+            for (int off = G / 2; off > 0; off >>= 1) bp *= __shfl_xor_sync(gm, bp, off, G);
+        }
+        prefac = ((n - esum) & 1) ? -bp : bp;
+        const int k0 = __shfl_sync(gm, kk, 0, G);
+        if (in.glynn && k0 == 0) prefac *= 0.5;  // the mirror's fixed point (:570-573)
+        if (nz) {
+            const int pos = __popc(mask & ((1u << gl) - 1u));
+            eidx[pos] = gl;
+            kval[pos] = (double)kk;
+        }
+        if (EXACT && want_index && a.terms) {
+            // The term's index: its digits in the mixed-radix place values.
+            int64_t part = gl < E ? (int64_t)dg * strides[in.reps_off + gl] : 0;
+            for (int off = G / 2; off > 0; off >>= 1) part += __shfl_xor_sync(gm, part, off, G);
+            jidx = part;
+        }
+    };
+    // Edges of subset S into eidx/kval (every multiplicity 1).
+    auto setup_subset = [&](uint32_t Sv) -> void {
+        for (int e = gl; e < E; e += G)
+            if ((Sv >> e) & 1u) {
+                const int pos = __popc(Sv & ((1u << e) - 1u));
+                eidx[pos] = e;
+                kval[pos] = 1.0;
+            }
+    };
+    for (;;) {
+        bool has = false;
+        double prefac = 0.0;
+        int mE = K;
+        int64_t jidx = 0;
+        if (mode == kAll) {
+            const int64_t cnt = ((int64_t)1 << E) - 1;
+            if (rk < cnt) {
+                const uint32_t Sv = (uint32_t)rk + 1u;
+                mE = __popc(Sv);
+                prefac = ((n - mE) & 1) ? -1.0 : 1.0;
+                setup_subset(Sv);
+                jidx = subset_index(Sv);
+                rk += W;
+                has = true;
+            }
+        } else if (mode == kSubset) {
+            if (rk < hi) {
+                if (rk > lo) S = subset_next(S);
+                prefac = ((n - K) & 1) ? -1.0 : 1.0;  // (-1)^(n - k), every binomial factor 1
+                setup_subset(S);
+                jidx = subset_index(S);
+                ++rk;
+                has = true;
+            }
+        } else if (mode == kList) {
+            const bool more = rk < hi;
+            if (more) {
+                const uint64_t word = a.lists[lb + rk];
+                const int dg = gl < E ? (int)((word >> (4 * gl)) & 15u) : 0;
+                setup_digits(dg, prefac, jidx, true);
+                ++rk;
+                has = true;
+            }
+        } else if (mode == kOdometer) {
+            while (rk < hi) {
                 const int kk = gl < E ? (in.glynn ? 2 * digit - r : digit) : 0;
-                const bool nz = gl < E && kk != 0;
-                const unsigned mask = group_ballot(nz);
-                const bool hit = __popc(mask) == K;
+                const bool hit = __popc(group_ballot(gl < E && kk != 0)) == K;
                 if (hit) {
-                    const int esum = __reduce_add_sync(gm, gl < E ? digit : 0);
-                    double bp = 1.0;
-                    if (!unit) {
-                        bp = gl < E ? a.binoms[r + digit * mr1] : 1.0;
-                        for (int off = G / 2; off > 0; off >>= 1) bp *= __shfl_xor_sync(gm, bp, off, G);
-                    }
-                    prefac = ((n - esum) & 1) ? -bp : bp;
-                    const int k0 = __shfl_sync(gm, kk, 0, G);
-                    if (in.glynn && k0 == 0) prefac *= 0.5;  // the mirror's fixed point (:570-573)
-                    if (nz) {
-                        const int pos = __popc(mask & ((1u << gl) - 1u));
-                        w.eidx[pos] = gl;
-                        w.kval[pos] = (double)kk;
-                    }
+                    setup_digits(digit, prefac, jidx, false);
+                    jidx = rk;
                     has = true;
                 }
-                // Move to index j + 1: the next odometer value, or the start of the group's next run.
-                ++j;
-                if (j < j1) {
+                // Move to index rk + 1: the next odometer value, or the start of the group's next run.
+                ++rk;
+                if (rk < hi) {
                     const unsigned notmax = group_ballot(gl < E && digit != base - 1);
                     const int h = 31 - __clz(notmax);
                     if (gl == h) ++digit;
                     else if (gl > h && gl < E) digit = 0;
                 } else {
-                    j0 += (int64_t)W * kRunTerms;
-                    if (j0 < in.steps) {
-                        j = j0;
-                        j1 = j0 + kRunTerms < in.steps ? j0 + kRunTerms : in.steps;
-                        if (gl < E) digit = (int)((j0 / strides[in.reps_off + gl]) % base);
+                    lo += (int64_t)W * kRunTerms;
+                    if (lo < in.steps) {
+                        rk = lo;
+                        hi = lo + kRunTerms < in.steps ? lo + kRunTerms : in.steps;
+                        if (gl < E) digit = (int)((lo / strides[in.reps_off + gl]) % base);
                     }
                 }
                 if (hit) break;
             }
-            if (!__any_sync(FULL, has)) break;
-            if (has) {
-                __syncwarp(gm);
-                eval_term(prefac, K);
-                __syncwarp(gm);
-            }
+        }
+        if (!__any_sync(FULL, has)) break;
+        if (has) {
+            __syncwarp(gm);
+            eval_term(prefac, mE, jidx);
+            __syncwarp(gm);
         }
     }
+    flush();
     // The block's groups summed in a fixed order: one partial per block.
     __shared__ dd red[2 * GB];
     if (gl == 0) {
@@ -296,19 +379,24 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G>::threads, LevelShape<CP
                     if (CPLX) dd_add(fi, red[2 * w + 1]);
                 }
                 const double hr = __dadd_rn(fr.hi, fr.lo);
-                if (CPLX) ((cd *)a.fused_out)[0] = cd{hr, __dadd_rn(fi.hi, fi.lo)};
-                else ((double *)a.fused_out)[0] = hr;
+                if (!a.fused_out) {
+                    // term output: nothing to sum
+                } else if (CPLX) {
+                    ((cd *)a.fused_out)[0] = cd{hr, __dadd_rn(fi.hi, fi.lo)};
+                } else {
+                    ((double *)a.fused_out)[0] = hr;
+                }
             }
         }
     }
 }
 
-template <bool CPLX, int K, int G>
+template <bool CPLX, int K, int G, bool EXACT = false>
 static int level_launch_k(const SieveArgs &a, const int64_t *strides, int B, dd *partial, int blocks_x, cudaStream_t st)
 {
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
-    const size_t smem = (size_t)cw * (32 / G) * fast_ws_doubles(a.nmax, CPLX, 2 * K) * sizeof(double);
-    auto k = sieve_level_kernel<CPLX, K, G>;
+    const size_t smem = (size_t)cw * (32 / G) * level_ws_doubles<CPLX, K, EXACT>(a.nmax) * sizeof(double);
+    auto k = sieve_level_kernel<CPLX, K, G, false, EXACT>;
     int rc = smem_limit_at_least((const void *)k, smem);
     if (rc) return rc;
     k<<<dim3((unsigned)blocks_x, (unsigned)B), cw * 32, smem, st>>>(a, strides, partial);
@@ -317,12 +405,12 @@ static int level_launch_k(const SieveArgs &a, const int64_t *strides, int B, dd 
     return EGG_OK;
 }
 
-template <bool CPLX, int K, int G>
+template <bool CPLX, int K, int G, bool EXACT = false>
 static int level_launch_all_k(const SieveArgs &a, dd *partial, int blocks_x, cudaStream_t st)
 {
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
-    const size_t smem = (size_t)cw * (32 / G) * fast_ws_doubles(a.nmax, CPLX, 2 * K) * sizeof(double);
-    auto k = sieve_level_kernel<CPLX, K, G, true>;
+    const size_t smem = (size_t)cw * (32 / G) * level_ws_doubles<CPLX, K, EXACT>(a.nmax) * sizeof(double);
+    auto k = sieve_level_kernel<CPLX, K, G, true, EXACT>;
     int rc = smem_limit_at_least((const void *)k, smem);
     if (rc) return rc;
     k<<<dim3((unsigned)blocks_x, 1u), cw * 32, smem, st>>>(a, nullptr, partial);
@@ -331,12 +419,12 @@ static int level_launch_all_k(const SieveArgs &a, dd *partial, int blocks_x, cud
     return EGG_OK;
 }
 
-template <bool CPLX, int K, int G>
+template <bool CPLX, int K, int G, bool EXACT = false>
 static int level_shape_k(int nmax, int *warps_per_block, int *blocks_per_sm)
 {
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
-    const size_t smem = (size_t)cw * (32 / G) * fast_ws_doubles(nmax, CPLX, 2 * K) * sizeof(double);
-    auto k = sieve_level_kernel<CPLX, K, G>;
+    const size_t smem = (size_t)cw * (32 / G) * level_ws_doubles<CPLX, K, EXACT>(nmax) * sizeof(double);
+    auto k = sieve_level_kernel<CPLX, K, G, false, EXACT>;
     int nb = 0;
     int rc = smem_limit_at_least((const void *)k, smem);
     if (!rc) rc = egg::blocks_per_sm((const void *)k, cw * 32, smem, &nb);
@@ -355,8 +443,8 @@ static int level_shape_k(int nmax, int *warps_per_block, int *blocks_per_sm)
 // Case K of a switch over the all-levels launches (groups as for the level launch).
 #define EGG_ALL_LAUNCH(CPLX, K)                                                                      \
     case K:                                                                                          \
-        return narrow ? level_launch_all_k<CPLX, K, level_group<K>(true)>(a, partial, blocks_x, st)  \
-                      : level_launch_all_k<CPLX, K, 32>(a, partial, blocks_x, st);
+        return narrow ? level_launch_all_k<CPLX, K, level_group<K>(true), EXACT>(a, partial, blocks_x, st)  \
+                      : level_launch_all_k<CPLX, K, 32, EXACT>(a, partial, blocks_x, st);
 #define EGG_FUSED_CASES(CPLX, X)                                                                    \
     X(CPLX, 1) X(CPLX, 2) X(CPLX, 3) X(CPLX, 4) X(CPLX, 5) X(CPLX, 6) X(CPLX, 7) X(CPLX, 8) X(CPLX, 9) \
     X(CPLX, 10)

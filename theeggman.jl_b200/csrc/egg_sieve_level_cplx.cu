@@ -28,6 +28,7 @@ int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, 
 int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st)
 {
     static_assert(kFusedMaxE == 10, "EGG_FUSED_CASES lists the levels 1..kFusedMaxE");
+    constexpr bool EXACT = false;  // complex terms run with fused multiply-adds only
     switch (k) {
         EGG_FUSED_CASES(true, EGG_ALL_LAUNCH)
     }

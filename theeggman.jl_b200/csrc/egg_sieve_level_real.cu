@@ -1,68 +1,50 @@
-// egg_sieve_level_real.cu -- popcount-level sieve kernels for Float64 terms, m = 2 .. 32 (levels 17-24 are
-// in egg_sieve_level_real_hi.cu).
-#include <mutex>
-
-#include "egg_sieve_level.cuh"
+// egg_sieve_level_real.cu -- popcount-level sieve kernels for Float64 terms, m = 2 .. 32, with fused
+// multiply-adds, and the dispatch over every real level (levels 17-24 are in
+// egg_sieve_level_real_hi.cu, the reference-arithmetic form in egg_sieve_level_real_x.cu).
+#include "egg_sieve_level_real.cuh"
 
 namespace egg {
 
 size_t fast_ws_bytes(int nmax, int cplx, int mhi) { return fast_ws_doubles(nmax, cplx, mhi) * sizeof(double); }
 
-// Level K with groups of 16 lanes when `narrow` and the tile allows it, else whole warps.
-#define EGG_LVL_LAUNCH(CPLX, K)                                                                     \
-    case K:                                                                                          \
-        return narrow ? level_launch_k<CPLX, K, level_group<K>(true)>(a, strides, B, partial, blocks_x, st) \
-                      : level_launch_k<CPLX, K, 32>(a, strides, B, partial, blocks_x, st);
-#define EGG_LVL_SHAPE(CPLX, K)                                                                       \
-    case K:                                                                                          \
-        rc = narrow ? level_shape_k<CPLX, K, level_group<K>(true)>(nmax, warps_per_block, blocks_per_sm) \
-                    : level_shape_k<CPLX, K, 32>(nmax, warps_per_block, blocks_per_sm);              \
-        break;
-
-int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
-                      cudaStream_t st)
+size_t level_ws_bytes(int nmax, int cplx, int k, bool exact)
 {
-    if (k > 16) return level_launch_real_hi(a, strides, B, k, narrow, partial, blocks_x, st);
-    switch (k) {
-        EGG_LEVEL_CASES(false, EGG_LVL_LAUNCH)
-    }
-    return fail(EGG_ERR_ARGUMENT, "no such sieve level");
+    if (exact && !cplx && k <= 16) return tile_ws_doubles(nmax, 2 * k, true) * sizeof(double);
+    return fast_ws_doubles(nmax, cplx, 2 * k) * sizeof(double);
 }
 
-int level_launch_all_real(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st)
-{
-    static_assert(kFusedMaxE == 10, "EGG_FUSED_CASES lists the levels 1..kFusedMaxE");
-    switch (k) {
-        EGG_FUSED_CASES(false, EGG_ALL_LAUNCH)
-    }
-    return fail(EGG_ERR_ARGUMENT, "no all-levels sieve launch for this edge count");
-}
+template int level_launch_real_lo<false>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
+template int level_launch_all_real_lo<false>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
+template int level_shape_real_lo<false>(int, int, bool, int *, int *);
+extern template int level_launch_real_lo<true>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
+extern template int level_launch_all_real_lo<true>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
+extern template int level_shape_real_lo<true>(int, int, bool, int *, int *);
 
-int level_shape_real(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm)
+int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, bool exact, dd *partial,
+                      int blocks_x, cudaStream_t st)
 {
-    static std::mutex mu;  // the entry point that allocates nothing reaches this without the library's lock
-    std::lock_guard<std::mutex> lk(mu);
-    static int cache[kLevelMaxReal + 1][2][2];
-    int *slot = (k >= 1 && k <= kLevelMaxReal) ? cache[k][narrow ? 1 : 0] : nullptr;
-    if (slot && slot[1] > 0) {
-        *warps_per_block = slot[0];
-        *blocks_per_sm = slot[1];
-        return EGG_OK;
-    }
-    int rc = fail(EGG_ERR_ARGUMENT, "no such sieve level");
     if (k > 16) {
-        rc = level_shape_real_hi(nmax, k, narrow, warps_per_block, blocks_per_sm);
-    } else {
-        switch (k) {
-            EGG_LEVEL_CASES(false, EGG_LVL_SHAPE)
-        }
+        if (exact) return fail(EGG_ERR_ARGUMENT, "the reference-arithmetic tiles hold up to 32 rows");
+        return level_launch_real_hi(a, strides, B, k, narrow, partial, blocks_x, st);
     }
-    if (rc) return rc;
-    if (slot) {
-        slot[0] = *warps_per_block;
-        slot[1] = *blocks_per_sm;
+    return exact ? level_launch_real_lo<true>(a, strides, B, k, narrow, partial, blocks_x, st)
+                 : level_launch_real_lo<false>(a, strides, B, k, narrow, partial, blocks_x, st);
+}
+
+int level_launch_all_real(const SieveArgs &a, int k, bool narrow, bool exact, dd *partial, int blocks_x, cudaStream_t st)
+{
+    return exact ? level_launch_all_real_lo<true>(a, k, narrow, partial, blocks_x, st)
+                 : level_launch_all_real_lo<false>(a, k, narrow, partial, blocks_x, st);
+}
+
+int level_shape_real(int nmax, int k, bool narrow, bool exact, int *warps_per_block, int *blocks_per_sm)
+{
+    if (k > 16) {
+        if (exact) return fail(EGG_ERR_ARGUMENT, "the reference-arithmetic tiles hold up to 32 rows");
+        return level_shape_real_hi(nmax, k, narrow, warps_per_block, blocks_per_sm);
     }
-    return EGG_OK;
+    return exact ? level_shape_real_lo<true>(nmax, k, narrow, warps_per_block, blocks_per_sm)
+                 : level_shape_real_lo<false>(nmax, k, narrow, warps_per_block, blocks_per_sm);
 }
 
 }  // namespace egg

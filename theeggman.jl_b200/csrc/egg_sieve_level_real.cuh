@@ -1,0 +1,68 @@
+// egg_sieve_level_real.cuh -- dispatch over the real popcount levels 1..16 (m = 2 .. 32), the tiles
+// whose columns stay in logical order, for one arithmetic form.  Instantiated once per form
+// (egg_sieve_level_real.cu: fused multiply-adds, egg_sieve_level_real_x.cu: the reference's
+// arithmetic) so that the two compile in parallel.
+#pragma once
+#include <mutex>
+
+#include "egg_sieve_level.cuh"
+
+namespace egg {
+
+// Level K with groups of 16 lanes when `narrow` and the tile allows it, else whole warps.
+#define EGG_LVLR_LAUNCH(CPLX, K)                                                                              \
+    case K:                                                                                                    \
+        return narrow ? level_launch_k<CPLX, K, level_group<K>(true), EXACT>(a, strides, B, partial, blocks_x, st) \
+                      : level_launch_k<CPLX, K, 32, EXACT>(a, strides, B, partial, blocks_x, st);
+#define EGG_LVLR_SHAPE(CPLX, K)                                                                                  \
+    case K:                                                                                                      \
+        rc = narrow ? level_shape_k<CPLX, K, level_group<K>(true), EXACT>(nmax, warps_per_block, blocks_per_sm)   \
+                    : level_shape_k<CPLX, K, 32, EXACT>(nmax, warps_per_block, blocks_per_sm);                   \
+        break;
+
+template <bool EXACT>
+int level_launch_real_lo(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
+                         cudaStream_t st)
+{
+    switch (k) {
+        EGG_LEVEL_CASES(false, EGG_LVLR_LAUNCH)
+    }
+    return fail(EGG_ERR_ARGUMENT, "no such sieve level");
+}
+
+template <bool EXACT>
+int level_launch_all_real_lo(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st)
+{
+    static_assert(kFusedMaxE == 10, "EGG_FUSED_CASES lists the levels 1..kFusedMaxE");
+    switch (k) {
+        EGG_FUSED_CASES(false, EGG_ALL_LAUNCH)
+    }
+    return fail(EGG_ERR_ARGUMENT, "no all-levels sieve launch for this edge count");
+}
+
+template <bool EXACT>
+int level_shape_real_lo(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm)
+{
+    static std::mutex mu;  // the entry point that allocates nothing reaches this without the library's lock
+    std::lock_guard<std::mutex> lk(mu);
+    // Occupancy figures, the same on every device of one model.
+    static int cache[16 + 1][2][2];
+    int *slot = (k >= 1 && k <= 16) ? cache[k][narrow ? 1 : 0] : nullptr;
+    if (slot && slot[1] > 0) {
+        *warps_per_block = slot[0];
+        *blocks_per_sm = slot[1];
+        return EGG_OK;
+    }
+    int rc = fail(EGG_ERR_ARGUMENT, "no such sieve level");
+    switch (k) {
+        EGG_LEVEL_CASES(false, EGG_LVLR_SHAPE)
+    }
+    if (rc) return rc;
+    if (slot) {
+        slot[0] = *warps_per_block;
+        slot[1] = *blocks_per_sm;
+    }
+    return EGG_OK;
+}
+
+}  // namespace egg

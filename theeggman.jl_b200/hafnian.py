@@ -10,7 +10,8 @@ Differences from the reference, all additive:
   * `prec` picks the rounding: "exact" = the reference CPU's, term by term, for both the DP and
     the sieve; "fma" = fused multiply-adds (the reference GPU kernel's DP rounding, and the
     register-resident sieve kernels); "mixed" = FP32 multiplies with FP64 accumulation in the
-    DP.  The default (None) runs the DP exactly and the sieve on the fast kernels;
+    DP.  The default (None) is "exact" for both: every sieve term in the reference's arithmetic
+    (bit-identical to _glynn_term!), summed in double-double;
   * `exact=True` runs integer matrices in Int64/Int128 instead of promoting them to Float64.
 """
 from __future__ import annotations
@@ -266,11 +267,12 @@ def _dp_prec(prec) -> str:
 
 
 def _sieve_prec(prec) -> int:
-    """Sieve kernel: reference term arithmetic for prec='exact' (and 'reference', which also sums
-    in the reference's order), the register-resident FMA kernels otherwise (the default)."""
+    """Sieve kernel: the reference's term arithmetic for prec None (the default), 'exact' and
+    'reference' (which also sums in the reference's order); the fused-multiply-add register tiles for
+    'fma' and 'mixed' (the sieve has no mixed form)."""
     if prec not in (None, "exact", "fma", "mixed", "reference"):
         raise ArgumentError("prec must be one of None, 'exact', 'fma', 'mixed', 'reference'")
-    return nat.PREC["exact"] if prec in ("exact", "reference") else nat.PREC["fma"]
+    return nat.PREC["fma"] if prec in ("fma", "mixed") else nat.PREC["exact"]
 
 
 # The last equal-size batch shape's stacking buffers, reused (under _lock) so that a batch does not
@@ -697,9 +699,9 @@ def reduction(A, rpt) -> np.ndarray:
 def sieve(Ax, edge_reps, *, glynn: bool = False, prec: str | None = None, nthreads: int | None = None):
     """The device sieve on a pre-permuted matrix: _calc_hafnian(Ax, edge_reps; nthreads, glynn)
     (src/hafnian.jl:684), the seam the reference has no device hook for.  prec='exact' evaluates
-    every term in the reference's rounding and sums them in double-double; prec='reference' also
-    sums them in the reference's order for `nthreads` threads, so the result is the reference's to
-    the last bit; the default uses the fast kernels."""
+    every term in the reference's rounding and sums them in double-double (the default);
+    prec='reference' also sums them in the reference's order for `nthreads` threads, so the result
+    is the reference's to the last bit; prec='fma' uses the fused-multiply-add register tiles."""
     Ax = np.asarray(Ax)
     T = _haf_dtype(Ax)
     return _sieve_one(T, Ax, list(edge_reps), glynn, prec, nthreads or _default_nthreads())
