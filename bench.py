@@ -496,39 +496,46 @@ class RepeatedWorkload:
                      + ", mixed-radix sieve, variant by the cost model")
 
     def setup_device(self, torch, dev):
-        B = self.B
-        Emax = max(len(er) for _, er, _ in self.inst)
-        lda = max(2 * Emax, 1)
+        # The raw inputs stay resident: each instance's d x d matrix and its multiplicities.  The
+        # device forms every instance's matching, variant and permuted matrix in each step.
         CT = np.complex128 if self.cplx else np.float64
-        slab = np.zeros((B, lda, lda), dtype=CT)
-        for b, (Ax, er, g) in enumerate(self.inst):
-            m = 2 * len(er)
-            slab[b, :m, :m] = Ax.T
-        self.Emax = Emax
-        self.dslab = torch.from_numpy(slab).to(dev)
-        self.E = np.array([len(er) for _, er, _ in self.inst], dtype=np.int64)
-        self.reps = np.zeros((B, max(Emax, 1)), dtype=np.int64)
-        for b, (_, er, _) in enumerate(self.inst):
-            self.reps[b, : len(er)] = er
-        self.g = np.array([1 if g else 0 for _, _, g in self.inst], dtype=np.int32)
-        self.dout = torch.zeros(2 * B, dtype=torch.float64, device=dev)
-        self.dE = self.E
+        self.stack = np.ascontiguousarray(np.stack([np.asarray(A, dtype=CT).T for A in self.mats]))
+        self.R = np.ascontiguousarray(self.rpts, dtype=np.int64)
+        self.d = self.stack.shape[1]
+        self.dstack = torch.from_numpy(self.stack).to(dev)
+        self.drpts = torch.from_numpy(self.R).to(dev)
+        self.dout = torch.zeros(2 * self.B, dtype=torch.float64, device=dev)
 
     def step_device(self, stream_ptr):
-        # The instance tables are host-side and tiny; the matrices stay resident.
         L = self.egg.lib()
-        rc = L.egg_sieve_batch_device(1 if self.cplx else 0, self.prec, self.B, self.Emax, self.dslab.data_ptr(),
-                                      self.E.ctypes.data, self.reps.ctypes.data, self.g.ctypes.data,
-                                      self.dout.data_ptr(), stream_ptr)
+        rc = L.egg_sieve_repeated_batch_device(1 if self.cplx else 0, self.prec, self.B, self.d, self.dstack.data_ptr(),
+                                               self.d * self.d, self.drpts.data_ptr(), -1, self.dout.data_ptr(),
+                                               stream_ptr)
         if rc:
             raise RuntimeError(L.egg_last_error().decode())
 
     def step_e2e(self):
-        from theeggman_b200.hafnian import _sieve_device_batch
+        kw = {} if self.prec_name == "exact" else {"prec": self.prec_name}
+        return self.egg.hafnian_repeated_batch(self.mats, self.rpts, **kw)
 
-        return _sieve_device_batch(np.dtype(np.complex128 if self.cplx else np.float64), [a for a, _, _ in self.inst],
-                                   [er for _, er, _ in self.inst], [g for _, _, g in self.inst],
-                                   None if self.prec_name == "exact" else self.prec_name)
+    @property
+    def h2d_bytes(self):
+        return int(self.stack.nbytes + self.R.nbytes)
+
+    @property
+    def d2h_bytes(self):
+        return self.B * (16 if self.cplx else 8)
+
+    roofline = SieveWorkload.roofline
+
+    def cpu_sample(self, nthreads):
+        from oracle import oracle as O
+
+        nb = min(self.B, 64)
+        t = time.perf_counter()
+        for Ax, er, g in self.inst[:nb]:
+            O.calc_hafnian(Ax, er, g, nthreads=nthreads)
+        return nb / (time.perf_counter() - t), f"{nb} instances, each with the reference's sieve threading"
 
     def device_result(self):
         raw = self.dout.cpu().numpy()
@@ -548,26 +555,6 @@ class RepeatedWorkload:
         return {"max_vs_reference_terms_dd": worst_dd, "max_vs_reference_plain_fp64": worst_plain,
                 "instances_checked": 16, "e2e_vs_device": e2e_worst, "bar": 1e-10,
                 "reference": "oracle calc_hafnian (src/hafnian.jl:684-738) per instance"}
-
-
-    @property
-    def h2d_bytes(self):
-        return int(self.dslab.numel() * self.dslab.element_size()) if hasattr(self, "dslab") else 0
-
-    @property
-    def d2h_bytes(self):
-        return self.B * (16 if self.cplx else 8)
-
-    roofline = SieveWorkload.roofline
-
-    def cpu_sample(self, nthreads):
-        from oracle import oracle as O
-
-        nb = min(self.B, 64)
-        t = time.perf_counter()
-        for Ax, er, g in self.inst[:nb]:
-            O.calc_hafnian(Ax, er, g, nthreads=nthreads)
-        return nb / (time.perf_counter() - t), f"{nb} instances, each with the reference's sieve threading"
 
 
 def make_workload(name: str, egg, W, rank: int):

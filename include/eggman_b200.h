@@ -186,6 +186,25 @@ int egg_sieve_batch(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax
 int egg_sieve_batch_device(int dtype, int prec, int64_t B, int64_t Emax, const void *Ax, const int64_t *E,
                            const int64_t *edge_reps, const int32_t *glynn, void *out, void *stream);
 
+/* B instances of hafnian_repeated(A_b, rpt_b; method = :sieve), each with its own matrix and
+ * multiplicities, prepared on the device.  A_b is the d x d column-major matrix at mats + b *
+ * mat_stride elements (mat_stride 0: one matrix shared by every instance), rpt_b the d entries at
+ * rpts + b * d.  Per instance the device forms matched_reps(rpt_b) (src/hafnian.jl:142-188), the
+ * sieve variant the reference's cost model picks (:855-884, :974-976; glynn = 0 or 1 forces one,
+ * -1 takes the cost model's) and the permuted matrix A_b[x, x] (:786-792), then the batch runs as
+ * egg_sieve_batch does; out receives B values.  A zero total gives 1 and an odd one 0.  Instances
+ * that match into more than 32 edges, or whose total exceeds 126, are refused with
+ * EGG_ERR_TOO_LARGE.  Host pointers.  No counterpart in the reference, whose
+ * hafnian_repeated(A, rpts) takes one matrix and runs its batch as a CPU loop (:1317-1359). */
+int egg_sieve_repeated_batch(int dtype, int prec, int64_t B, int64_t d, const void *mats, int64_t mat_stride,
+                             const int64_t *rpts, int glynn, void *out);
+
+/* Same, with mats, rpts and out in device memory, enqueued on `stream`.  The per-instance edge
+ * counts, multiplicities and variants come back to the host, where the sieve's launches are
+ * planned, so the call waits for the preparation kernel. */
+int egg_sieve_repeated_batch_device(int dtype, int prec, int64_t B, int64_t d, const void *mats, int64_t mat_stride,
+                                    const int64_t *rpts, int glynn, void *out, void *stream);
+
 /* One sieve summed exactly as the reference sums it: every term in the reference's arithmetic
  * (as EGG_PREC_EXACT), then plain FP64 `+=` over `nchunks` equal chunks of the term range, each
  * in term order, and the chunk sums left to right, times 2^-(n-1) under Glynn
@@ -221,8 +240,11 @@ int egg_dp_mix_device(int dtype, int prec, const void *A, int64_t n, int64_t B, 
  * timing the candidates on the first batch that had more than one instance of that degree:
  * batched = 1 runs groups of `group` instances instance-fastest (one thread per state and
  * instance); batched = 0 runs `group` single-instance evaluations side by side.  Degrees up to 22
- * always run as one whole-instance launch per batch and are not tuned.  EGG_ERR_NO_PLAN if K has
- * not been tuned yet.  No counterpart in the reference. */
+ * always run as one whole-instance launch per batch and are not tuned.  Choices are kept in a JSON
+ * file per GPU model and SM count ($EGG_TUNE_CACHE, else $XDG_CACHE_HOME/eggman_b200/mix_tuning.json
+ * or ~/.cache/eggman_b200/mix_tuning.json; an empty $EGG_TUNE_CACHE turns the file off), which a
+ * process reads before its first batch, so a degree tuned once is not timed again.
+ * EGG_ERR_NO_PLAN if K has not been tuned yet.  No counterpart in the reference. */
 int egg_dp_mix_tuning(int K, int dtype, int prec, int *batched, int64_t *group);
 
 /* Pin the evaluation of degree K (> 22) for this dtype and mode instead of timing candidates:

@@ -139,3 +139,39 @@ def test_mix_graph_replay(egg, nat, W):
     for b, r in enumerate(rows2):
         exp = egg.hafnian(_sub(A, r), method="dp", check_symmetric=False) if len(r) else 1
         assert other[b] == exp, b
+
+
+def test_tuner_choice_persists_across_processes(tmp_path):
+    """The tuner writes its per-degree choice to the tuning file, and a later process on the same
+    GPU model starts from it without timing again (egg_dp_mix_tuning answers before any batch)."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = f"""
+import ctypes, json, sys
+sys.path.insert(0, {root!r}); sys.path.insert(0, {os.path.join(root, 'tests')!r})
+from conftest import load_package
+egg = load_package()
+from theeggman_b200 import workloads as W, _native as nat
+L = nat.lib()
+if sys.argv[1] == "tune":
+    A, idxs = W.gbs_mix(8, 64, [24], 4)
+    egg.hafnian_submatrices(A, idxs)
+b, g = ctypes.c_int(), ctypes.c_int64()
+rc = L.egg_dp_mix_tuning(24, 1, 0, ctypes.byref(b), ctypes.byref(g))
+print(json.dumps([rc, b.value, g.value]))
+"""
+    path = tmp_path / "tuning" / "mix_tuning.json"
+    env = dict(os.environ, EGG_TUNE_CACHE=str(path))
+    runs = []
+    for mode in ("tune", "read"):
+        r = subprocess.run([sys.executable, "-c", script, mode], env=env, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        runs.append(json.loads(r.stdout.strip().splitlines()[-1]))
+        if mode == "tune":
+            text = path.read_text()
+            assert '"K": 24' in text and '"dtype": 1' in text, text
+    assert runs[0][0] == 0 and runs[1] == runs[0], runs

@@ -22,3 +22,14 @@ def test_per_device_values_are_set_up_per_device(tmp_path):
                     os.path.join(ROOT, "tests", "perdevice_check.cpp"), "-o", str(exe)], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_tuner_file_round_trip(tmp_path):
+    """The mixed-degree tuner's choices survive the process: the file format
+    (csrc/egg_tunecache.h) written, merged per (device, SMs, degree, type, mode) and read back."""
+    exe = tmp_path / "tunecache_check"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "theeggman.jl_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "tunecache_check.cpp"), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr

@@ -286,16 +286,18 @@ def test_repeated_batch_equal_patterns(egg, W, monkeypatch):
 
     seen = []
 
-    def fake_sieve(T, Axs, reps_list, glynns, prec=None):
-        seen.extend(tuple(r) for r in reps_list)
-        return np.array([float(np.sum(np.abs(a))) * 1000 + sum(r) + 0.5 * bool(g)
-                         for a, r, g in zip(Axs, reps_list, glynns)], dtype=T)
+    def fake_repeated(T, mats, stride, rpts, glynn, prec):
+        # The device path of the sieve patterns: one shared matrix (stride 0), the raw patterns.
+        assert stride == 0 and np.asarray(mats).ndim == 2
+        seen.extend(tuple(r) for r in rpts)
+        return np.array([float(np.sum(np.abs(mats))) * 1000 + 7 * sum(i * x for i, x in enumerate(r))
+                         for r in rpts], dtype=T)
 
     def fake_dp(T, P, K, prec, max_batch, exact_int):
         seen.extend(range(np.asarray(P).shape[0]))
         return np.array([float(np.sum(np.abs(p))) for p in np.asarray(P)], dtype=T)
 
-    monkeypatch.setattr(H, "_sieve_device_batch", fake_sieve)
+    monkeypatch.setattr(H, "_repeated_device", fake_repeated)
     monkeypatch.setattr(H, "_dp_device", fake_dp)
     A = W.dense_real(8, 17)
     pats = [[2, 2, 2, 2, 0, 0, 0, 0], [1, 1, 1, 1, 1, 1, 1, 1], [3, 1, 2, 0, 2, 0, 0, 0], [4, 4, 0, 0, 0, 0, 0, 0]]

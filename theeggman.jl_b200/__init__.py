@@ -18,6 +18,7 @@ from .hafnian import (  # noqa: F401
     gpu_cache_bytes,
     hafnian,
     hafnian_repeated,
+    hafnian_repeated_batch,
     hafnian_submatrices,
     reduction,
     sieve,

@@ -422,6 +422,7 @@ int egg_plan_release(int K, int idx_bytes)
     auto it = ctx().plans.find({K, idx_bytes});
     if (it == ctx().plans.end()) return fail(EGG_ERR_NO_PLAN, "no resident plan for degree " + std::to_string(K));
     cudaStreamSynchronize(ctx().stream);
+    mix_graphs_clear();  // recorded mixed-degree batches may read this plan's arrays
     release_plan_memory(it->second);
     ctx().plans.erase(it);
     return EGG_OK;

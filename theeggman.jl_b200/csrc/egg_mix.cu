@@ -16,6 +16,7 @@
 #include <tuple>
 
 #include "egg_internal.cuh"
+#include "egg_tunecache.h"
 
 namespace egg {
 
@@ -108,9 +109,54 @@ struct BinExec {
     int64_t group;
 };
 
-// Chosen per (degree, dtype, precision) by timing on first use; kept for the process.
+// Chosen per (degree, dtype, precision) by timing on first use, kept for the process and in the
+// tuning file (egg_tunecache.h), from which the next process on the same GPU model starts.
 static std::map<std::tuple<int, int, int>, BinExec> g_tuned;
 static std::mutex g_tuned_mu;
+static bool g_tuned_loaded = false;
+
+// This device's identity in the tuning file: its model name and SM count.
+static TuneRecord tune_identity()
+{
+    TuneRecord r;
+    int dev = 0;
+    cudaDeviceProp prop{};
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+        r.device = prop.name;
+        r.sms = prop.multiProcessorCount;
+    }
+    return r;
+}
+
+// Reads the tuning file's records of this device into g_tuned, once (callers hold g_tuned_mu).
+// Choices pinned or tuned in this process before the first read take precedence.
+static void tuned_load_once()
+{
+    if (g_tuned_loaded) return;
+    g_tuned_loaded = true;
+    const std::string path = tune_cache_path();
+    if (path.empty()) return;
+    std::vector<TuneRecord> rs;
+    if (!tune_read_file(path, rs)) return;
+    const TuneRecord me = tune_identity();
+    for (const TuneRecord &r : rs)
+        if (r.device == me.device && r.sms == me.sms && r.group >= 1 && r.K >= 2 && r.K <= 64)
+            g_tuned.emplace(std::make_tuple((int)r.K, (int)r.dtype, (int)r.prec), BinExec{r.batched != 0, r.group});
+}
+
+// Adds one tuned choice to the tuning file (a failure to write only costs a re-tune later).
+static void tuned_save(int K, int dtype, int prec, const BinExec &ex)
+{
+    const std::string path = tune_cache_path();
+    if (path.empty()) return;
+    TuneRecord r = tune_identity();
+    r.K = K;
+    r.dtype = dtype;
+    r.prec = prec;
+    r.batched = ex.batched ? 1 : 0;
+    r.group = ex.group;
+    tune_merge_file(path, r);
+}
 
 static int launch_gather(int dtype, const void *dA, int64_t n, const int64_t *doff, const int32_t *drows,
                          const int32_t *dorder, const MixBins &bins, int64_t total, void *dP, cudaStream_t st)
@@ -333,6 +379,7 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
             bool found = false;
             {
                 std::lock_guard<std::mutex> lk(g_tuned_mu);
+                tuned_load_once();
                 auto it = g_tuned.find(key);
                 if (it != g_tuned.end()) {
                     ex = it->second;
@@ -349,6 +396,7 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
                 if (rc) return rc;
                 std::lock_guard<std::mutex> lk(g_tuned_mu);
                 g_tuned[key] = ex;
+                tuned_save(bn.K, dtype, prec, ex);
             } else if (!found) {
                 ex = dp_grouped_ok(bn.K, dtype, prec) && plans[k]->closed_form() ? BinExec{false, 4} : BinExec{true, bn.count};
             }
@@ -373,6 +421,14 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
         key.shape.insert(key.shape.end(), {(int64_t)bins.b[k].K, bins.b[k].count, exs[k].batched ? 1 : 0, exs[k].group});
     }
     for (const DevBuf &b : c.scratch) key.ptrs.push_back(b.ptr);
+    // Every device array a recorded kernel may read: the plans' transition arrays (explicit plans)
+    // and their cluster lists, which exist only once built.  A graph keyed on them is never
+    // replayed against a plan that was released and rebuilt elsewhere.
+    for (const DevPlan *pl : plans) {
+        key.ptrs.push_back(pl->trans);
+        key.ptrs.push_back(pl->cluster_lists[0]);
+        key.ptrs.push_back(pl->cluster_lists[1]);
+    }
     GraphEntry *ge = cap == cudaStreamCaptureStatusNone ? &graph_entry(key) : nullptr;
     if (ge && ge->exec) {
         EGG_CUDA_TRY(cudaGraphLaunch(ge->exec, st));
@@ -453,6 +509,7 @@ int mix_set_tuning(int K, int dtype, int prec, int batched, int64_t group)
 int mix_tuned(int K, int dtype, int prec, int *batched, int64_t *group)
 {
     std::lock_guard<std::mutex> lk(g_tuned_mu);
+    tuned_load_once();
     auto it = g_tuned.find(std::make_tuple(K, dtype, prec));
     if (it == g_tuned.end()) return fail(EGG_ERR_NO_PLAN, "degree " + std::to_string(K) + " has not been tuned");
     *batched = it->second.batched ? 1 : 0;

@@ -621,11 +621,11 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     const int Ews = (int)(Emax > 0 ? Emax : 1);
 
     // Which kernels run: each popcount level that some instance has terms in, on the register tiles
-    // (orders n <= 31, one lane per coefficient) -- with fused multiply-adds, or for real terms of
-    // up to 32 rows in the reference's arithmetic -- and the shared-memory exact kernel for
-    // whatever exceeds the tiles (every complex term in exact mode).
+    // (orders n <= 31, one lane per coefficient) -- with fused multiply-adds, or for terms of up to
+    // 32 rows in the reference's arithmetic -- and the shared-memory exact kernel for whatever
+    // exceeds the tiles.
     const bool exact = prec == EGG_PREC_EXACT;
-    const bool fast_ok = nmax <= 31 && (!exact || !cplx);
+    const bool fast_ok = nmax <= 31;
     bool all_subset = true;
     for (const SieveInst &si : inst) all_subset = all_subset && si.subset;
     const int fast_hi = cplx ? 32 : (exact ? 32 : 48);
@@ -749,7 +749,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         const int k = inst[0].E;
         const bool narrow = 2 * k <= 16;
         int cw = 0, bps = 0;
-        int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, &cw, &bps) : level_shape_real(nmax, k, narrow, exact, &cw, &bps);
+        int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, exact, &cw, &bps) : level_shape_real(nmax, k, narrow, exact, &cw, &bps);
         if (rc0) return rc0;
         if (bps < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
         const int64_t terms_all = ((int64_t)1 << k) - 1, per_block = (int64_t)cw * (narrow ? 2 : 1);
@@ -785,7 +785,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             if (lvl[(size_t)k] <= 0.0) continue;
             const bool narrow = 2 * k <= 16 && e_odo <= 16;
             int cw = 0, bps = 0;
-            int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, &cw, &bps) : level_shape_real(nmax, k, narrow, exact, &cw, &bps);
+            int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, exact, &cw, &bps) : level_shape_real(nmax, k, narrow, exact, &cw, &bps);
             if (rc0) return rc0;
             if (bps < 1 || (size_t)cw * (narrow ? 2 : 1) * level_ws_bytes(nmax, cplx, k, exact) > 220 * 1024)
                 return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
@@ -939,10 +939,10 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             cudaStream_t ls = st;
             if (side_ok && L.side) ls = c.side[next_side++ % Context::kSideStreams];
             if (fused)
-                rc = cplx ? level_launch_all_cplx(a, L.level, L.narrow, part, L.bx, ls)
+                rc = cplx ? level_launch_all_cplx(a, L.level, L.narrow, exact, part, L.bx, ls)
                           : level_launch_all_real(a, L.level, L.narrow, exact, part, L.bx, ls);
             else
-                rc = cplx ? level_launch_cplx(a, dstr, (int)B, L.level, L.narrow, part, L.bx, ls)
+                rc = cplx ? level_launch_cplx(a, dstr, (int)B, L.level, L.narrow, exact, part, L.bx, ls)
                           : level_launch_real(a, dstr, (int)B, L.level, L.narrow, exact, part, L.bx, ls);
             if (rc) return rc;
             ps.p[slot] = part;

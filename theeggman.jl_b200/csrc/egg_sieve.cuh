@@ -49,7 +49,7 @@ size_t level_ws_bytes(int nmax, int cplx, int k, bool exact);
 // Launches level k on a grid of blocks_x x B blocks; a.warps_per_inst must be blocks_x times the
 // level's warps per block.  Each block writes one partial (re, im) per instance.  `narrow` puts
 // two terms in each warp for tiles of up to 16 rows (odometer instances then need E <= 16).
-// `exact` (real levels 1..16 only) evaluates every term in the reference's arithmetic; with
+// `exact` (levels 1..16 only) evaluates every term in the reference's arithmetic; with
 // a.terms set those kernels write each term's signed value at its index instead of summing.
 int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, bool exact, dd *partial,
                       int blocks_x, cudaStream_t st);
@@ -60,12 +60,12 @@ int level_launch_real_hi(const SieveArgs &a, const int64_t *strides, int B, int 
 // a.fused_out (when set).  A separate instantiation of the level kernel, so the level launches are
 // unchanged.
 int level_launch_all_real(const SieveArgs &a, int k, bool narrow, bool exact, dd *partial, int blocks_x, cudaStream_t st);
-int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st);
-int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
-                      cudaStream_t st);
+int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, bool exact, dd *partial, int blocks_x, cudaStream_t st);
+int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, bool exact, dd *partial,
+                      int blocks_x, cudaStream_t st);
 // The level's block size in warps and how many of its blocks one SM holds.
 int level_shape_real(int nmax, int k, bool narrow, bool exact, int *warps_per_block, int *blocks_per_sm);
 int level_shape_real_hi(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm);
-int level_shape_cplx(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm);
+int level_shape_cplx(int nmax, int k, bool narrow, bool exact, int *warps_per_block, int *blocks_per_sm);
 
 }  // namespace egg

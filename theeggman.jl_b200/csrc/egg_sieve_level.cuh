@@ -46,17 +46,18 @@ constexpr int level_group(bool narrow)
     return (narrow && 2 * K <= 16) ? 16 : 32;
 }
 
-// In the reference's arithmetic, real terms of up to 32 rows run on the tile whose columns stay in
-// logical order (egg_sieve_tile.cuh).  With fused multiply-adds every term runs on the relabelled
-// tiles of egg_sieve_fast.cuh, which move no data on a pivot swap and so keep their code compact.
+// In the reference's arithmetic, terms of up to 32 rows (real or complex) run on the tiles whose
+// columns stay in logical order (egg_sieve_tile.cuh).  With fused multiply-adds every term runs on
+// the relabelled tiles of egg_sieve_fast.cuh, which move no data on a pivot swap and so keep their
+// code compact.
 template <bool CPLX, int K, bool EXACT>
-constexpr bool level_tile() { return EXACT && !CPLX && 2 * K <= 32; }
+constexpr bool level_tile() { return EXACT && 2 * K <= 32; }
 
 // One group's shared workspace, in doubles.
 template <bool CPLX, int K, bool EXACT>
 __host__ __device__ inline size_t level_ws_doubles(int nmax)
 {
-    if constexpr (level_tile<CPLX, K, EXACT>()) return tile_ws_doubles(nmax, 2 * K, EXACT);
+    if constexpr (level_tile<CPLX, K, EXACT>()) return CPLX ? ctile_ws_doubles(nmax, 2 * K) : tile_ws_doubles(nmax, 2 * K, EXACT);
     else return fast_ws_doubles(nmax, CPLX, 2 * K);
 }
 
@@ -72,7 +73,7 @@ __device__ __forceinline__ dd group_tree_sum(dd v, unsigned gm, int G)
 }
 
 // ALL: the all-levels mode of one small distinct-row instance (level_launch_all_*), a separate
-// instantiation.  EXACT: every term in the reference's arithmetic (real tiles only); the term
+// instantiation.  EXACT: every term in the reference's arithmetic (logical-order tiles); the term
 // series are evaluated in batches of G terms, one term per lane, and with a.terms set each term's
 // signed value is written at its index instead of being summed.
 template <bool CPLX, int K, int G, bool ALL = false, bool EXACT = false>
@@ -81,7 +82,7 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT>::threads, LevelS
 {
     constexpr int MW = 2 * K;
     constexpr bool TILE = level_tile<CPLX, K, EXACT>();
-    static_assert(!EXACT || TILE, "the exact form runs on the real tile");
+    static_assert(!EXACT || TILE, "the exact form runs on the logical-order tiles");
     constexpr int cw = LevelShape<CPLX, K>::threads / 32;
     constexpr int NG = 32 / G;   // groups per warp
     constexpr int GB = cw * NG;  // groups per block
@@ -95,9 +96,10 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT>::threads, LevelS
     double *wbase = smem + (size_t)grp * level_ws_doubles<CPLX, K, EXACT>(a.nmax);
     FastWs wf{};
     const TileWs<MW> wt{wbase};
+    const CTileWs<MW> wc{wbase};
     if constexpr (!TILE) wf = fast_carve(wbase, a.nmax, CPLX, MW);
-    int *const eidx = TILE ? wt.eidx() : wf.eidx;
-    double *const kval = TILE ? wt.kval() : wf.kval;
+    int *const eidx = TILE ? (CPLX ? wc.eidx() : wt.eidx()) : wf.eidx;
+    double *const kval = TILE ? (CPLX ? wc.kval() : wt.kval()) : wf.kval;
     const int gslot = blockIdx.x * GB + grp;
     const uint64_t W = (uint64_t)a.warps_per_inst * NG;  // groups per instance
     dd acc_re{0.0, 0.0}, acc_im{0.0, 0.0};
@@ -105,7 +107,7 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT>::threads, LevelS
     // index and size at pre[s], jx[s], mx[s]).
     int nbuf = 0;
     auto flush = [&]() {
-        if constexpr (EXACT) {
+        if constexpr (EXACT && !CPLX) {
             __syncwarp(gm);
             double v = 0.0;
             if (gl < nbuf) {
@@ -120,12 +122,49 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT>::threads, LevelS
             }
             nbuf = 0;
             __syncwarp(gm);
+        } else if constexpr (EXACT) {
+            __syncwarp(gm);
+            double vr = 0.0, vi = 0.0;
+            if (gl < nbuf) {
+                cd f[32];
+                const cd val = series_cplx_exact(wc.qbuf() + (size_t)gl * (a.nmax + 1), f, wc.mx()[gl], n);
+                const double pf = wc.pre()[gl];
+                vr = __dmul_rn(pf, val.re);
+                vi = __dmul_rn(pf, val.im);
+                if (a.terms) {
+                    a.terms[2 * wc.jx()[gl]] = vr;
+                    a.terms[2 * wc.jx()[gl] + 1] = vi;
+                }
+            }
+            if (!a.terms) {
+                const dd tr = group_tree_sum(dd{vr, 0.0}, gm, G);
+                const dd ti = group_tree_sum(dd{vi, 0.0}, gm, G);
+                if (gl == 0) {
+                    dd_add(acc_re, tr);
+                    dd_add(acc_im, ti);
+                }
+            }
+            nbuf = 0;
+            __syncwarp(gm);
         }
     };
     // One term: the surviving edges are compacted into eidx / kval (mE of them, mE = K except in
     // the all-levels mode) by the caller; jidx is the term's index (used with a.terms).
     auto eval_term = [&](double prefac, int mE, int64_t jidx) {
-        if constexpr (CPLX) {
+        if constexpr (CPLX && TILE) {
+            const int mm = 2 * (ALL ? mE : K);
+            term_cplx_tile<MW, G>((const cd *)a.Ax + in.ax_off, in.lda, E, ALL ? mE : K, n, wc, gl, gm);
+            cd *dst = wc.qbuf() + (size_t)nbuf * (a.nmax + 1);
+            const int jm = mm < n ? mm : n;
+            for (int j = 1 + gl; j <= jm; j += G) dst[j] = wc.q()[j];
+            if (gl == 0) {
+                wc.pre()[nbuf] = prefac;
+                wc.mx()[nbuf] = mm;
+                wc.jx()[nbuf] = jidx;
+            }
+            if (++nbuf == G) flush();
+            __syncwarp(gm);
+        } else if constexpr (CPLX) {
             const cd val = term_cplx<MW, G>((const cd *)a.Ax + in.ax_off, in.lda, E, ALL ? mE : K, n, wf, gl, gm);
             if (gl == 0) {
                 dd_add(acc_re, prefac * val.re);

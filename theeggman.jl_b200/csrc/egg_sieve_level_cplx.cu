@@ -1,61 +1,34 @@
-// egg_sieve_level_cplx.cu -- popcount-level sieve kernels for ComplexF64 terms, m = 2 .. 32.
-#include <mutex>
-
-#include "egg_sieve_level.cuh"
+// egg_sieve_level_cplx.cu -- popcount-level sieve kernels for ComplexF64 terms, m = 2 .. 32, with
+// fused multiply-adds, and the dispatch over the complex levels (the reference-arithmetic form is
+// in egg_sieve_level_cplx_x.cu).
+#include "egg_sieve_level_cplx.cuh"
 
 namespace egg {
 
-// Level K with groups of 16 lanes when `narrow` and the tile allows it, else whole warps.
-#define EGG_LVL_LAUNCH(CPLX, K)                                                                     \
-    case K:                                                                                          \
-        return narrow ? level_launch_k<CPLX, K, level_group<K>(true)>(a, strides, B, partial, blocks_x, st) \
-                      : level_launch_k<CPLX, K, 32>(a, strides, B, partial, blocks_x, st);
-#define EGG_LVL_SHAPE(CPLX, K)                                                                       \
-    case K:                                                                                          \
-        rc = narrow ? level_shape_k<CPLX, K, level_group<K>(true)>(nmax, warps_per_block, blocks_per_sm) \
-                    : level_shape_k<CPLX, K, 32>(nmax, warps_per_block, blocks_per_sm);              \
-        break;
+template int level_launch_cplx_lo<false>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
+template int level_launch_all_cplx_lo<false>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
+template int level_shape_cplx_lo<false>(int, int, bool, int *, int *);
+extern template int level_launch_cplx_lo<true>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
+extern template int level_launch_all_cplx_lo<true>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
+extern template int level_shape_cplx_lo<true>(int, int, bool, int *, int *);
 
-int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, dd *partial, int blocks_x,
-                      cudaStream_t st)
+int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, bool exact, dd *partial,
+                      int blocks_x, cudaStream_t st)
 {
-    switch (k) {
-        EGG_LEVEL_CASES(true, EGG_LVL_LAUNCH)
-    }
-    return fail(EGG_ERR_ARGUMENT, "no such sieve level");
+    return exact ? level_launch_cplx_lo<true>(a, strides, B, k, narrow, partial, blocks_x, st)
+                 : level_launch_cplx_lo<false>(a, strides, B, k, narrow, partial, blocks_x, st);
 }
 
-int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, dd *partial, int blocks_x, cudaStream_t st)
+int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, bool exact, dd *partial, int blocks_x, cudaStream_t st)
 {
-    static_assert(kFusedMaxE == 10, "EGG_FUSED_CASES lists the levels 1..kFusedMaxE");
-    constexpr bool EXACT = false;  // complex terms run with fused multiply-adds only
-    switch (k) {
-        EGG_FUSED_CASES(true, EGG_ALL_LAUNCH)
-    }
-    return fail(EGG_ERR_ARGUMENT, "no all-levels sieve launch for this edge count");
+    return exact ? level_launch_all_cplx_lo<true>(a, k, narrow, partial, blocks_x, st)
+                 : level_launch_all_cplx_lo<false>(a, k, narrow, partial, blocks_x, st);
 }
 
-int level_shape_cplx(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm)
+int level_shape_cplx(int nmax, int k, bool narrow, bool exact, int *warps_per_block, int *blocks_per_sm)
 {
-    static std::mutex mu;  // the entry point that allocates nothing reaches this without the library's lock
-    std::lock_guard<std::mutex> lk(mu);
-    static int cache[kLevelMaxCplx + 1][2][2];
-    int *slot = (k >= 1 && k <= kLevelMaxCplx) ? cache[k][narrow ? 1 : 0] : nullptr;
-    if (slot && slot[1] > 0) {
-        *warps_per_block = slot[0];
-        *blocks_per_sm = slot[1];
-        return EGG_OK;
-    }
-    int rc = fail(EGG_ERR_ARGUMENT, "no such sieve level");
-    switch (k) {
-        EGG_LEVEL_CASES(true, EGG_LVL_SHAPE)
-    }
-    if (rc) return rc;
-    if (slot) {
-        slot[0] = *warps_per_block;
-        slot[1] = *blocks_per_sm;
-    }
-    return EGG_OK;
+    return exact ? level_shape_cplx_lo<true>(nmax, k, narrow, warps_per_block, blocks_per_sm)
+                 : level_shape_cplx_lo<false>(nmax, k, narrow, warps_per_block, blocks_per_sm);
 }
 
 }  // namespace egg

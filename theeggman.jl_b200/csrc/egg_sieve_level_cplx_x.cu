@@ -1,0 +1,11 @@
+// egg_sieve_level_cplx_x.cu -- popcount-level sieve kernels for ComplexF64 terms, m = 2 .. 32, in
+// the reference's arithmetic (each term bit-identical to _glynn_term!, src/hafnian.jl:528-602).
+#include "egg_sieve_level_cplx.cuh"
+
+namespace egg {
+
+template int level_launch_cplx_lo<true>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
+template int level_launch_all_cplx_lo<true>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
+template int level_shape_cplx_lo<true>(int, int, bool, int *, int *);
+
+}  // namespace egg

@@ -9,7 +9,7 @@ size_t fast_ws_bytes(int nmax, int cplx, int mhi) { return fast_ws_doubles(nmax,
 
 size_t level_ws_bytes(int nmax, int cplx, int k, bool exact)
 {
-    if (exact && !cplx && k <= 16) return tile_ws_doubles(nmax, 2 * k, true) * sizeof(double);
+    if (exact && k <= 16) return (cplx ? ctile_ws_doubles(nmax, 2 * k) : tile_ws_doubles(nmax, 2 * k, true)) * sizeof(double);
     return fast_ws_doubles(nmax, cplx, 2 * k) * sizeof(double);
 }
 

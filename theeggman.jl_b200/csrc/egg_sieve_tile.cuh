@@ -337,4 +337,281 @@ __device__ __forceinline__ double series_exact(const double *q, double *f, int m
     return f[n];
 }
 
+// ---- complex terms in the reference's arithmetic (_hessenberg_split!, src/hafnian.jl:271-335) ----
+//
+// The same tile with the real and imaginary parts of each row in two register arrays.  Pivot on the
+// squared modulus (:277-286), multipliers ((ar xr + ai xi) / d, (ai xr - ar xi) / d) with
+// d = xr^2 + xi^2 (:296-304), the row update Mr -= ur ar - ui ai, Mi -= ur ai + ui ar (:307-314) and
+// the column update Mr += mr Mr_i - mi Mi_i, Mi += mr Mi_i + mi Mr_i (:317-324), every product and
+// sum rounded separately; La Budde and the series use Julia's complex product
+// (ar br - ai bi, ar bi + ai br).
+
+// Layout in doubles from the group's base (complex arrays hold re, im pairs).
+__host__ __device__ constexpr int ctile_off_cft() { return 256; }
+__host__ __device__ constexpr int ctile_off_hk(int mw) { return 256 + 2 * cft_row_cplx(mw + 1); }
+__host__ __device__ constexpr int ctile_off_sub(int mw) { return ctile_off_hk(mw) + 2 * (mw + 2); }
+__host__ __device__ constexpr int ctile_off_q(int mw) { return ctile_off_sub(mw) + 2 * (mw + 2); }
+__host__ __device__ constexpr int ctile_off_kval(int mw) { return ctile_off_q(mw) + 64; }
+__host__ __device__ constexpr int ctile_off_eidx(int mw) { return ctile_off_kval(mw) + 32; }
+__host__ __device__ constexpr int ctile_off_pre(int mw) { return ctile_off_eidx(mw) + 16; }
+__host__ __device__ constexpr int ctile_off_jx(int mw) { return ctile_off_pre(mw) + 32; }
+__host__ __device__ constexpr int ctile_off_mx(int mw) { return ctile_off_jx(mw) + 32; }
+__host__ __device__ constexpr int ctile_off_qbuf(int mw) { return ctile_off_mx(mw) + 16; }
+
+__host__ __device__ inline size_t ctile_ws_doubles(int nmax, int mhi)
+{
+    return ((size_t)ctile_off_qbuf(mhi) + 64 * (size_t)(nmax + 1) + 1) & ~(size_t)1;
+}
+
+template <int MW>
+struct CTileWs {
+    double *base;
+    __device__ double *prr() const { return base; }
+    __device__ double *pri() const { return base + 64; }
+    __device__ double *wvr() const { return base + 128; }
+    __device__ double *wvi() const { return base + 192; }
+    __device__ cd *cft() const { return (cd *)(base + ctile_off_cft()); }
+    __device__ cd *hk() const { return (cd *)(base + ctile_off_hk(MW)); }
+    __device__ cd *sub() const { return (cd *)(base + ctile_off_sub(MW)); }
+    __device__ cd *q() const { return (cd *)(base + ctile_off_q(MW)); }
+    __device__ double *kval() const { return base + ctile_off_kval(MW); }
+    __device__ int *eidx() const { return (int *)(base + ctile_off_eidx(MW)); }
+    __device__ double *pre() const { return base + ctile_off_pre(MW); }
+    __device__ long long *jx() const { return (long long *)(base + ctile_off_jx(MW)); }
+    __device__ int *mx() const { return (int *)(base + ctile_off_mx(MW)); }
+    __device__ cd *qbuf() const { return (cd *)(base + ctile_off_qbuf(MW)); }
+};
+
+template <int K, int LO, int HI, int MW>
+__device__ __forceinline__ void swap_cols2(double (&A)[MW], double (&Bv)[MW], int p)
+{
+    if constexpr (HI - LO == 1) {
+        const double t = A[K];
+        A[K] = A[LO];
+        A[LO] = t;
+        const double u = Bv[K];
+        Bv[K] = Bv[LO];
+        Bv[LO] = u;
+    } else {
+        constexpr int MID = (LO + HI) / 2;
+        if (p < MID) swap_cols2<K, LO, MID, MW>(A, Bv, p);
+        else swap_cols2<K, MID, HI, MW>(A, Bv, p);
+    }
+}
+
+template <int MW, int G>
+struct CTileCtx {
+    double (&Rr)[MW];
+    double (&Ri)[MW];
+    int &lab;
+    const CTileWs<MW> &ws;
+    int m, lane;
+    unsigned gm;
+};
+
+// Step K of the split reduction (pivot row K, pivot column K - 1; 0-based).
+template <int K, int MW, int G>
+__device__ __forceinline__ void step_cplx(CTileCtx<MW, G> &c)
+{
+    double (&Rr)[MW] = c.Rr;
+    double (&Ri)[MW] = c.Ri;
+    int &lab = c.lab;
+    const int m = c.m;
+    const bool cand = lab >= K && lab < m;
+    // -- pivot: the first row of largest squared modulus (:277-286); NaN as in the real form
+    const double a = __dadd_rn(__dmul_rn(Rr[K - 1], Rr[K - 1]), __dmul_rn(Ri[K - 1], Ri[K - 1]));
+    int plab, pl;
+    if (__any_sync(c.gm, lab == K && a != a)) {
+        plab = K;
+        pl = -1;
+    } else {
+        const unsigned long long key = cand ? abs_key(a) : 0ull;
+        const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+        const unsigned mhi = __reduce_max_sync(c.gm, hi);
+        const unsigned mlo = __reduce_max_sync(c.gm, hi == mhi ? lo : 0u);
+        const bool win = key != 0ull && hi == mhi && lo == mlo;
+        const unsigned wb = __ballot_sync(c.gm, win);
+        if (__popc(wb) == 1) {
+            pl = __ffs((int)wb) - 1;
+            if (G < 32) pl &= G - 1;
+            plab = __shfl_sync(c.gm, lab, pl, G);
+        } else {
+            plab = (int)__reduce_min_sync(c.gm, win ? (unsigned)lab : 0x7fffffffu);
+            if (plab == 0x7fffffff) plab = K;
+            pl = -1;
+        }
+    }
+    if (pl < 0) {
+        pl = __ffs((int)__ballot_sync(c.gm, lab == plab)) - 1;
+        if (G < 32) pl &= G - 1;
+    }
+    const double xr = __shfl_sync(c.gm, Rr[K - 1], pl, G), xi = __shfl_sync(c.gm, Ri[K - 1], pl, G);
+    // -- swap rows (relabel) and columns (move)
+    if (lab == K) lab = plab;
+    else if (lab == plab) lab = K;
+    if (plab != K) swap_cols2<K, K + 1, MW, MW>(Rr, Ri, plab);
+    const double d = __dadd_rn(__dmul_rn(xr, xr), __dmul_rn(xi, xi));
+    if (d == 0.0) return;  // (:293)
+    // -- multipliers (:296-304)
+    double mr = 0.0, mi = 0.0;
+    if (lab > K && lab < m) {
+        const double ar = Rr[K - 1], ai = Ri[K - 1];
+        mr = __ddiv_rn(__dadd_rn(__dmul_rn(ar, xr), __dmul_rn(ai, xi)), d);
+        mi = __ddiv_rn(__dsub_rn(__dmul_rn(ai, xr), __dmul_rn(ar, xi)), d);
+    }
+    constexpr int J0 = K & ~1;
+    double *prr = c.ws.prr(), *pri = c.ws.pri(), *wvr = c.ws.wvr(), *wvi = c.ws.wvi();
+    if (c.lane == pl) {
+#pragma unroll
+        for (int j = J0; j < MW; j += 2) {
+            *reinterpret_cast<double2 *>(prr + j) = make_double2(Rr[j], Rr[j + 1]);
+            *reinterpret_cast<double2 *>(pri + j) = make_double2(Ri[j], Ri[j + 1]);
+        }
+    }
+    wvr[lab] = mr;
+    wvi[lab] = mi;
+    __syncwarp(c.gm);
+    // -- row update (:307-314)
+#pragma unroll
+    for (int j = J0; j < MW; j += 2) {
+        const double2 ar2 = *reinterpret_cast<const double2 *>(prr + j);
+        const double2 ai2 = *reinterpret_cast<const double2 *>(pri + j);
+        if (j >= K) {
+            Rr[j] = __dsub_rn(Rr[j], __dsub_rn(__dmul_rn(mr, ar2.x), __dmul_rn(mi, ai2.x)));
+            Ri[j] = __dsub_rn(Ri[j], __dadd_rn(__dmul_rn(mr, ai2.x), __dmul_rn(mi, ar2.x)));
+        }
+        Rr[j + 1] = __dsub_rn(Rr[j + 1], __dsub_rn(__dmul_rn(mr, ar2.y), __dmul_rn(mi, ai2.y)));
+        Ri[j + 1] = __dsub_rn(Ri[j + 1], __dadd_rn(__dmul_rn(mr, ai2.y), __dmul_rn(mi, ar2.y)));
+    }
+    // -- column update (:317-324), i ascending
+    constexpr int I0 = (K + 1) & ~1;
+    double accr = Rr[K], acci = Ri[K];
+#pragma unroll
+    for (int i = I0; i < MW; i += 2) {
+        const double2 w_r = *reinterpret_cast<const double2 *>(wvr + i);
+        const double2 w_i = *reinterpret_cast<const double2 *>(wvi + i);
+        if (i > K) {
+            accr = __dadd_rn(accr, __dsub_rn(__dmul_rn(w_r.x, Rr[i]), __dmul_rn(w_i.x, Ri[i])));
+            acci = __dadd_rn(acci, __dadd_rn(__dmul_rn(w_r.x, Ri[i]), __dmul_rn(w_i.x, Rr[i])));
+        }
+        accr = __dadd_rn(accr, __dsub_rn(__dmul_rn(w_r.y, Rr[i + 1]), __dmul_rn(w_i.y, Ri[i + 1])));
+        acci = __dadd_rn(acci, __dadd_rn(__dmul_rn(w_r.y, Ri[i + 1]), __dmul_rn(w_i.y, Rr[i + 1])));
+    }
+    Rr[K] = accr;
+    Ri[K] = acci;
+    __syncwarp(c.gm);
+}
+
+template <int K, int MW, int G>
+__device__ __forceinline__ void steps_cplx(CTileCtx<MW, G> &c)
+{
+    if constexpr (K <= MW - 2) {
+        if (K > c.m - 2) return;
+        step_cplx<K, MW, G>(c);
+        steps_cplx<K + 1, MW, G>(c);
+    }
+}
+
+__device__ __forceinline__ cd c_sub_rn(cd a, cd b) { return cd{__dsub_rn(a.re, b.re), __dsub_rn(a.im, b.im)}; }
+
+// La Budde by diagonals, complex, in the reference's order and rounding (see labudde_diag_exact).
+template <int MW, int G>
+__device__ __forceinline__ void labudde_diag_cplx_exact(const cd *__restrict__ cft, const cd *__restrict__ hk, cd *q, int m,
+                                                        int n, int lane, unsigned gm)
+{
+    cd D[MW + 1];
+    D[0] = cd{lane == 0 ? 1.0 : 0.0, 0.0};
+#pragma unroll
+    for (int r = 1; r <= MW; ++r) D[r] = cd{0.0, 0.0};
+#pragma unroll
+    for (int k = 1; k <= MW; ++k) {
+        if (k > m) break;
+        cd up{__shfl_up_sync(gm, D[k - 1].re, 1, G), __shfl_up_sync(gm, D[k - 1].im, 1, G)};
+        if (lane == 0) up = cd{0.0, 0.0};
+        const cd *row = cft + cft_row_cplx(k);
+        cd v = c_sub_rn(up, x_cmul(hk[k], D[k - 1]));
+#pragma unroll
+        for (int i = k - 1; i >= 1; --i) v = c_sub_rn(v, x_cmul(row[i - 1], D[i - 1]));
+        D[k] = v;
+        if (k == m && lane < m && lane >= m - n) q[m - lane] = D[k];
+    }
+}
+
+// One complex term (m = 2 mE <= MW <= 32) in the reference's arithmetic: leaves q_1..q_min(m,n).
+template <int MW, int G>
+__device__ __forceinline__ void term_cplx_tile(const cd *__restrict__ Ax, int lda, int E, int mE, int n,
+                                               const CTileWs<MW> &ws, int lane, unsigned gm)
+{
+    static_assert(MW <= 32, "one row per lane");
+    static_assert(G == 32 || MW <= 16, "a group of 16 lanes holds up to 16 rows");
+    const int m = 2 * mE;
+    double Rr[MW], Ri[MW];
+    int lab = lane;
+    {
+        const int *eidx = ws.eidx();
+        const double *kval = ws.kval();
+        const bool live = lane < m;
+        const int ra = live ? (lane < mE ? eidx[lane] : eidx[lane - mE] + E) : 0;
+#pragma unroll
+        for (int j = 0; j < MW; ++j) {
+            double vr = 0.0, vi = 0.0;
+            if (live && j < m) {
+                const int b = j < mE ? j : j - mE;
+                const int col = eidx[b] + (j < mE ? E : 0);
+                const double2 z = __ldg(reinterpret_cast<const double2 *>(Ax + (size_t)col * lda + ra));
+                vr = __dmul_rn(kval[b], z.x);  // M = A_S X D (:582-593)
+                vi = __dmul_rn(kval[b], z.y);
+            }
+            Rr[j] = vr;
+            Ri[j] = vi;
+        }
+    }
+    CTileCtx<MW, G> c{Rr, Ri, lab, ws, m, lane, gm};
+    steps_cplx<1, MW, G>(c);
+    if (lab < m) {
+#pragma unroll
+        for (int j = 0; j < MW; ++j) {
+            const cd v{Rr[j], Ri[j]};
+            if (j == lab - 1) ws.sub()[lab] = v;
+            if (j == lab) ws.hk()[j + 1] = v;
+            if (j > lab && j < m) ws.cft()[cft_row_cplx(j + 1) + lab] = v;
+        }
+    }
+    __syncwarp(gm);
+    {
+        const int k = lane + 1;
+        if (k <= m) {
+            cd *row = ws.cft() + cft_row_cplx(k);
+            cd beta{1.0, 0.0};
+            for (int i = k - 1; i >= 1; --i) {
+                beta = x_cmul(beta, ws.sub()[i]);
+                row[i - 1] = x_cmul(row[i - 1], beta);
+            }
+        }
+    }
+    __syncwarp(gm);
+    labudde_diag_cplx_exact<MW, G>(ws.cft(), ws.hk(), ws.q(), m, n, lane, gm);
+    __syncwarp(gm);
+}
+
+// _inv_sqrt_det_coeff! for a complex term, in the reference's order and rounding, on one lane.
+__device__ __forceinline__ cd series_cplx_exact(const cd *q, cd *f, int m, int n)
+{
+    f[0] = cd{1.0, 0.0};
+    for (int t = 1; t <= n; ++t) {
+        cd s{0.0, 0.0};
+        const int jm = t < m ? t : m;
+        for (int j = 1; j <= jm; ++j) {
+            const double wt = (double)(2 * t - j);
+            const cd wq{__dmul_rn(wt, q[j].re), __dmul_rn(wt, q[j].im)};
+            const cd pr = x_cmul(wq, f[t - j]);
+            s.re = __dadd_rn(s.re, pr.re);
+            s.im = __dadd_rn(s.im, pr.im);
+        }
+        const double d2 = (double)(2 * t);
+        f[t] = cd{__ddiv_rn(-s.re, d2), __ddiv_rn(-s.im, d2)};
+    }
+    return f[n];
+}
+
 }  // namespace egg

@@ -617,9 +617,10 @@ def _hafnian_repeated_batch(A, rpts, *, nthreads, glynn, method, check_symmetric
             dp_idx.append(b)
         else:
             sv_idx.append(b)
-            sv_ax.append(_permuted(T, A, x))
-            sv_reps.append(er)
-            sv_g.append(sg if glynn is None else glynn)
+            if prec == "reference":  # the other forms permute on the device
+                sv_ax.append(_permuted(T, A, x))
+                sv_reps.append(er)
+                sv_g.append(sg if glynn is None else glynn)
     if dp_idx:
         idxs = np.stack([_expanded_indices(rpts[b], total) for b in dp_idx])
         vals = _dp_device(T, _gather_pairs_batch(T, A, idxs, total), total, _dp_prec(prec), max_batch, exact_int)
@@ -628,10 +629,77 @@ def _hafnian_repeated_batch(A, rpts, *, nthreads, glynn, method, check_symmetric
     if sv_idx:
         if exact_int:
             raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
-        vals = _sieve_device_batch(T, sv_ax, sv_reps, sv_g, prec)
+        if prec == "reference":
+            vals = _sieve_device_batch(T, sv_ax, sv_reps, sv_g, prec)
+        else:
+            # One call on the shared matrix: the device forms each pattern's matching, variant and
+            # permuted matrix itself.
+            vals = _repeated_device(T, np.asarray(A), 0, [rpts[b] for b in sv_idx], glynn, prec)
         for k, b in enumerate(sv_idx):
             out[b] = vals[k]
     return out if exact_int else np.array(out, dtype=T)
+
+
+def _repeated_device(T: np.dtype, mats: np.ndarray, stride: int, rpts, glynn, prec) -> np.ndarray:
+    """egg_sieve_repeated_batch over B patterns: mats is one d x d matrix (stride 0) or a B x d x d
+    stack (stride d * d); the device forms each instance's matching, variant and permuted matrix."""
+    cplx = np.dtype(T).kind == "c"
+    CT = np.complex128 if cplx else np.float64
+    R = np.ascontiguousarray(rpts, dtype=np.int64)
+    B, d = R.shape
+    # Column-major per matrix: store each transposed (the matrices are symmetric, but be exact).
+    M = np.ascontiguousarray(np.swapaxes(np.asarray(mats, dtype=CT), -1, -2))
+    out = np.zeros(B, CT)
+    g = -1 if glynn is None else (1 if glynn else 0)
+    with _lock:
+        nat.check(nat.lib().egg_sieve_repeated_batch(nat.EGG_C128 if cplx else nat.EGG_F64, _sieve_prec(prec), B, d,
+                                                     nat.ptr(M), stride, nat.ptr(R), g, nat.ptr(out)))
+    return out.astype(T, copy=False)
+
+
+def hafnian_repeated_batch(As, rpts, *, glynn: bool | None = None, check_symmetric: bool = True,
+                           prec: str | None = None) -> np.ndarray:
+    """hafnian_repeated(As[b], rpts[b]; method=:sieve) for every b, in one device call.
+
+    Each instance has its own d x d matrix and multiplicity vector (the reference's
+    hafnian_repeated(A, rpts) shares one matrix and runs its batch as a CPU loop,
+    src/hafnian.jl:1317-1359).  The device forms every instance's matched_reps, the sieve variant
+    of the reference's cost model (unless `glynn` forces one) and its permuted matrix, then runs
+    the batched sieve.  A zero total gives 1 and an odd total 0.  prec as for the sieve."""
+    S = np.asarray(As)
+    if S.ndim != 3 or S.shape[1] != S.shape[2]:
+        raise DimensionMismatch(f"expected B square matrices of one size, got an array of shape {S.shape}")
+    B, d = S.shape[0], S.shape[1]
+    R = np.asarray(rpts)
+    if R.shape != (B, d):
+        raise DimensionMismatch(f"{B} matrices of size {d} need {B} multiplicity vectors of length {d}, got {R.shape}")
+    if B == 0:
+        return np.zeros(0)
+    R = np.ascontiguousarray(R, dtype=np.int64)
+    if (R < 0).any():
+        b = int(np.nonzero((R < 0).any(axis=1))[0][0])
+        raise ArgumentError(f"rpt {b + 1} contains a negative entry")
+    T = _haf_dtype_of(S.dtype)
+    if check_symmetric and d >= 2:
+        # One comparison for the whole stack; only matrices that differ from their transpose get
+        # the reference's tolerance test (and its error message).
+        with np.errstate(invalid="ignore"):
+            diff = (S != S.transpose(0, 2, 1)).reshape(B, -1).any(axis=1)
+        for b in np.nonzero(diff)[0]:
+            _check_symmetric(S[b])
+    if prec == "reference":
+        vals = []
+        for A, rp in zip(S, R.tolist()):
+            x, er, _, sg = _pattern_choice(tuple(rp), sum(rp))
+            tot = sum(rp)
+            if tot == 0:
+                vals.append(T.type(1))
+            elif tot % 2:
+                vals.append(T.type(0))
+            else:
+                vals.append(_sieve_reference(T, _permuted(T, A, list(x)), list(er), sg if glynn is None else glynn, 1))
+        return np.array(vals, dtype=T)
+    return _repeated_device(T, S, d * d, R, glynn, prec)
 
 
 def _mix_layout(rows_list) -> tuple[np.ndarray, np.ndarray]:
