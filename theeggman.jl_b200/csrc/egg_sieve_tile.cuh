@@ -81,6 +81,35 @@ struct TileWs {
     __device__ double *qbuf() const { return base + tile_off_qbuf(MW); }
 };
 
+// The correctly rounded quotient a / b given y = RN(1/b), the same for every lane of a step
+// (Markstein's division, "Computation of elementary functions on the IBM RISC System/6000 processor",
+// IBM J. Res. Dev. 34(1), 1990; Muller et al., Handbook of Floating-Point Arithmetic, 2nd ed., 2018,
+// sec. 5.3): q0 = RN(a y) is within 1.5 ulp of a/b; one correction q1 = q0 + (a - b q0) y (the
+// remainder exact in one fused multiply-add) brings it within 1 ulp; by Markstein's theorem a
+// second correction from a reciprocal within half an ulp then yields RN(a/b).  Valid while nothing
+// overflows or underflows: |b| and |a| within [2^-1000, 2^1000] and the quotient at least 2^-1000
+// (here |a| <= |b|, the pivot being the largest entry); outside that, and for zero, Inf or NaN, the
+// quotient comes from the correctly rounded division itself.  The parity tests hold every term of
+// the N = 40 sieves to the reference's bits (the reference-order sum must equal the oracle's), so a
+// quotient one ulp off anywhere would fail them.
+__device__ __forceinline__ bool div_scale_ok(double v)
+{
+    const double av = fabs(v);
+    return av >= 0x1p-1000 && av <= 0x1p+1000;
+}
+__device__ __forceinline__ double div_rn_shared(double a, double b, double y, bool b_ok)
+{
+    if (b_ok && div_scale_ok(a)) {
+        const double q0 = __dmul_rn(a, y);
+        const double r0 = __fma_rn(-b, q0, a);
+        const double q1 = __fma_rn(r0, y, q0);
+        const double r1 = __fma_rn(-b, q1, a);
+        const double q2 = __fma_rn(r1, y, q1);
+        if (fabs(q2) >= 0x1p-1000) return q2;
+    }
+    return __ddiv_rn(a, b);
+}
+
 // 64-bit order key of |v| for the exact pivot search: non-negative doubles order as their bit
 // patterns; +1 so that a candidate equal to zero still beats a non-candidate (key 0).  NaN never
 // wins (key 0).
@@ -170,7 +199,10 @@ __device__ __forceinline__ void step_real(TileCtx<MW, G, EXACT> &c)
     // -- the multipliers of the rows below the pivot (:234-237)
     double mult = 0.0;
     if constexpr (EXACT) {
-        if (lab > K && lab < m) mult = __ddiv_rn(R[K - 1], x);
+        // One correctly rounded reciprocal per step, shared by the lanes' quotients.
+        const bool x_ok = div_scale_ok(x);
+        const double y = x_ok ? __drcp_rn(x) : 0.0;
+        if (lab > K && lab < m) mult = div_rn_shared(R[K - 1], x, y, x_ok);
     } else {
         const double rx = recip(x);
         if (lab > K && lab < m) mult = R[K - 1] * rx;
@@ -454,10 +486,14 @@ __device__ __forceinline__ void step_cplx(CTileCtx<MW, G> &c)
     if (d == 0.0) return;  // (:293)
     // -- multipliers (:296-304)
     double mr = 0.0, mi = 0.0;
-    if (lab > K && lab < m) {
-        const double ar = Rr[K - 1], ai = Ri[K - 1];
-        mr = __ddiv_rn(__dadd_rn(__dmul_rn(ar, xr), __dmul_rn(ai, xi)), d);
-        mi = __ddiv_rn(__dsub_rn(__dmul_rn(ai, xr), __dmul_rn(ar, xi)), d);
+    {
+        const bool d_ok = div_scale_ok(d);
+        const double y = d_ok ? __drcp_rn(d) : 0.0;
+        if (lab > K && lab < m) {
+            const double ar = Rr[K - 1], ai = Ri[K - 1];
+            mr = div_rn_shared(__dadd_rn(__dmul_rn(ar, xr), __dmul_rn(ai, xi)), d, y, d_ok);
+            mi = div_rn_shared(__dsub_rn(__dmul_rn(ai, xr), __dmul_rn(ar, xi)), d, y, d_ok);
+        }
     }
     constexpr int J0 = K & ~1;
     double *prr = c.ws.prr(), *pri = c.ws.pri(), *wvr = c.ws.wvr(), *wvi = c.ws.wvi();
