@@ -69,9 +69,10 @@ def rel_err(a, b) -> float:
 
 
 # The committed ncu summary (kernel and workload) whose DRAM traffic figure belongs to a workload.
-PROFILE_OF = {"sieve40": "sieve_level_kernel_sieve40.md", "sieve40c": "sieve_level_kernel_sieve40c.md",
-              "sieve40g": "sieve_level_kernel_sieve40g.md", "rep14": "sieve_level_kernel_rep14.md",
-              "dp40": "dpc_fixed_kernel_dp40.md", "dp20": "dpc_cluster_kernel_dp20.md"}
+PROFILE_OF = {"sieve40": "sieve_level_kernel_exact_sieve40.md", "sieve40f": "sieve_level_kernel_sieve40.md",
+              "sieve40cf": "sieve_level_kernel_sieve40c.md", "sieve40gf": "sieve_level_kernel_sieve40g.md",
+              "rep14f": "sieve_level_kernel_rep14.md", "dp40": "dpc_fixed_kernel_dp40.md",
+              "dp20": "dpc_cluster_kernel_dp20.md"}
 
 
 def profile_traffic(name: str):
@@ -715,7 +716,7 @@ def run_reference(args):
 PER_CONFIG = [("dp20", 20), ("sieve20", 20), ("sieve20f", 20), ("dp32", 10), ("sieve40", 10), ("sieve40f", 10),
               ("sieve40c", 3), ("sieve40cf", 5), ("sieve40gf", 5), ("dp36", 5), ("dp40", 5), ("dp40mixed", 5),
               ("dp40int", 5), ("dp20x1024", 10), ("mix4096", 10), ("mix4096fma", 10), ("mix4096mixed", 10), ("mix4096seq", 3),
-              ("rep14", 10), ("rep14f", 10), ("rep20cf", 3)]
+              ("rep14", 10), ("rep14f", 10), ("rep20c", 3), ("rep20cf", 3)]
 PER_CONFIG_BUDGET_S = 300.0
 
 
