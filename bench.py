@@ -179,10 +179,16 @@ class SieveWorkload:
         sm_max = float(peaks.get("sm_max_mhz", 1965.0))
         peak = R.fp64_nominal_tflops(sm_max)
         achieved = self.flops / (ms / 1e3) / 1e12
-        return {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+        roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": f"nominal FP64: 148 SMs x 64 FMA/clk x 2 x {sm_max:.0f} MHz (no FP64 figure in "
                                "MEASURED_PEAKS.json)",
                 "work": f"{self.flops:.4e} algorithmic flops per hafnian"}
+        if getattr(self, "prec_name", "fma") == "exact":
+            # The reference rounds every product and every sum, so each algorithmic FMA issues as a
+            # multiply and an add: the form's own ceiling is half the nominal rate.
+            roof["separate_rounding_peak"] = peak / 2
+            roof["frac_of_separate_rounding_peak"] = achieved / (peak / 2)
+        return roof
 
     def cpu_sample(self, nthreads):
         from oracle import oracle as O

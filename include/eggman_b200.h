@@ -67,6 +67,15 @@ const char *egg_last_error(void);
  * the reference. */
 int64_t egg_launch_count(void);
 
+/* A diagnostic of the reference-arithmetic sieve's division: for i < n (n <= 2^26, host arrays)
+ * writes to q_shared[i] the quotient a[i]/b[i] as the sieve's reference-arithmetic tiles form it
+ * (one correctly rounded reciprocal of the divisor, then Markstein's corrections; the full division
+ * where operands or quotient leave [2^-1000, 2^1000]) and to q_rn[i] the device's correctly rounded
+ * quotient.  The two must agree bit for bit, as the reference's `/` does (src/hafnian.jl:235).
+ * Runs synchronously on the calling thread's current device, allocating 32n bytes there for the
+ * call.  No counterpart in the reference. */
+int egg_selfcheck_division(const double *a, const double *b, int64_t n, double *q_shared, double *q_rn);
+
 /* Bind the library to one CUDA device (idempotent; the first call of any other entry point does
  * this with device 0).  Fails with EGG_ERR_NO_DEVICE if there is none.  The library's streams,
  * plans and work buffers belong to that device: binding another device in the same process fails
