@@ -349,10 +349,10 @@ class MixWorkload:
 
     kind = "dp"
 
-    def __init__(self, egg, W, B: int, prec: str, seq: bool, seed: int):
+    def __init__(self, egg, W, B: int, prec: str, seq: bool, seed: int, engine: int = 1):
         from theeggman_b200.hafnian import _mix_layout
 
-        self.egg, self.B, self.prec_name, self.seq = egg, B, prec, seq
+        self.egg, self.B, self.prec_name, self.seq, self.engine = egg, B, prec, seq, engine
         self.prec = {"exact": 0, "fma": 1, "mixed": 2}[prec]
         self.A, self.idxs = W.gbs_mix(B, 64, range(8, 33, 2), seed)
         self.offsets, self.flat = _mix_layout(self.idxs)
@@ -363,7 +363,9 @@ class MixWorkload:
         self.bins = [(K, int(degs[K])) for K in range(2, 65, 2) if degs[K]]
         self.name = (f"config4: {B} hafnians of A[r, r], A = U diag(tanh r) U^T 64x64 complex (U Haar), |r| even "
                      f"uniform in 8..32, distinct rows; prec={prec}; "
-                     + ("one single-instance DP call per hafnian" if seq else "one egg_dp_mix call per step"))
+                     + ("one single-instance DP call per hafnian" if seq else
+                        "one egg_dp_mix call per step, " + ("one cooperative launch" if engine == 1 else
+                                                            "per-level launches replayed as a CUDA graph")))
 
     def setup_device(self, torch, dev):
         from theeggman_b200.hafnian import _dp_plan, _gather_pairs_batch
@@ -388,6 +390,7 @@ class MixWorkload:
                 if rc:
                     raise RuntimeError(L.egg_last_error().decode())
             return
+        L.egg_dp_mix_set_engine(self.engine)
         rc = L.egg_dp_mix_device(1, self.prec, self.dA.data_ptr(), 64, self.B, self.offsets.ctypes.data,
                                  self.drows.data_ptr(), self.dout.data_ptr(), stream_ptr)
         if rc:
@@ -397,6 +400,7 @@ class MixWorkload:
         kw = {} if self.prec_name == "exact" else {"prec": self.prec_name}
         if self.seq:
             return [self.egg.hafnian(self.A[np.ix_(r, r)], method="dp", **kw) for r in self.idxs]
+        self.egg.lib().egg_dp_mix_set_engine(self.engine)
         return self.egg.hafnian_submatrices(self.A, self.idxs, **kw)
 
     def device_result(self):
@@ -447,6 +451,8 @@ class MixWorkload:
 
         if self.seq:
             return {}
+        if self.engine == 1:
+            return {"engine": "one cooperative launch per call: gather, every degree's levels in lockstep, scatter"}
         L = self.egg.lib()
         tiles = {}
         for K, _ in self.bins:
@@ -611,6 +617,8 @@ def make_workload(name: str, egg, W, rank: int):
         return MixWorkload(egg, W, 4096, "fma", False, 4 + 100 * rank)
     if name == "mix4096mixed":
         return MixWorkload(egg, W, 4096, "mixed", False, 4 + 100 * rank)
+    if name == "mix4096levels":
+        return MixWorkload(egg, W, 4096, "exact", False, 4 + 100 * rank, engine=0)
     if name == "mix4096seq":
         return MixWorkload(egg, W, 4096, "exact", True, 4 + 100 * rank)
     if name == "rep14":
@@ -721,7 +729,7 @@ def run_reference(args):
 # stays within a few minutes.
 PER_CONFIG = [("dp20", 20), ("sieve20", 20), ("sieve20f", 20), ("dp32", 10), ("sieve40", 10), ("sieve40f", 10),
               ("sieve40c", 3), ("sieve40cf", 5), ("sieve40gf", 5), ("dp36", 5), ("dp40", 5), ("dp40mixed", 5),
-              ("dp40int", 5), ("dp20x1024", 10), ("mix4096", 10), ("mix4096fma", 10), ("mix4096mixed", 10), ("mix4096seq", 3),
+              ("dp40int", 5), ("dp20x1024", 10), ("mix4096", 10), ("mix4096levels", 10), ("mix4096fma", 10), ("mix4096mixed", 10), ("mix4096seq", 3),
               ("rep14", 10), ("rep14f", 10), ("rep20c", 3), ("rep20cf", 3)]
 PER_CONFIG_BUDGET_S = 300.0
 

@@ -245,6 +245,26 @@ int egg_dp_mix(int dtype, int prec, const void *A, int64_t n, int64_t B, const i
 int egg_dp_mix_device(int dtype, int prec, const void *A, int64_t n, int64_t B, const int64_t *offsets, const int32_t *rows,
                       void *out, void *stream);
 
+/* The engine of the two calls above.  1 (the default): a mix whose degrees are all at most 32
+ * (Float64, ComplexF64 or Int64 parents, closed-form plans) runs as ONE cooperative kernel launch
+ * -- the gather, every degree's levels in lockstep, the scatter -- with grid-wide barriers between
+ * phases; other mixes, and calls made while the stream is being captured, use engine 0.  0: a
+ * gather launch, one launch per level of each group of each degree, and a scatter launch,
+ * recorded as one CUDA graph on a shape's second call and replayed after that.  Both engines give
+ * identical results.  Each barrier wait of engine 1 is bounded (2 s); a launch that gave up makes
+ * egg_dp_mix return EGG_ERR_TIMEOUT, and for egg_dp_mix_device the next call of either returns
+ * it.  EGG_ERR_ARGUMENT for another value.  No counterpart in the reference. */
+int egg_dp_mix_set_engine(int engine);
+int egg_dp_mix_engine(void);
+
+/* A diagnostic of engine 1's grid barrier: every block of a cooperative grid on the library's device
+ * passes three barriers that each expect `extra` (0..1024) more blocks than the grid has.  With
+ * extra = 0 this is the normal barrier and returns EGG_OK; with extra > 0 the first wait runs out
+ * after wait_ns (1 ms .. 2 s) and the call returns EGG_ERR_TIMEOUT, having ended every block.
+ * *passes (may be null) receives the barriers passed, summed over blocks.  No counterpart in the
+ * reference. */
+int egg_selfcheck_barrier(int extra, int64_t wait_ns, int64_t *passes);
+
 /* How the mixed-degree batch evaluates degree K in this dtype and precision mode, as chosen by
  * timing the candidates on the first batch that had more than one instance of that degree:
  * batched = 1 runs groups of `group` instances instance-fastest (one thread per state and

@@ -14,6 +14,16 @@ def nat(egg):
     return _native
 
 
+@pytest.fixture
+def level_engine(nat):
+    """Runs a test on the per-level engine (launch per level, graph replay), then restores the default."""
+    L = nat.lib()
+    prev = L.egg_dp_mix_engine()
+    nat.check(L.egg_dp_mix_set_engine(0))
+    yield
+    nat.check(L.egg_dp_mix_set_engine(prev))
+
+
 def _sub(A, r):
     r = np.asarray(r, dtype=np.int64)
     return A[np.ix_(r, r)]
@@ -93,7 +103,7 @@ def test_mix_refusals(egg, W):
 
 
 @pytest.mark.parametrize("prec", ["exact", "fma", "mixed"])
-def test_mix_evaluations_agree(egg, nat, W, prec):
+def test_mix_evaluations_agree(egg, nat, W, prec, level_engine):
     # Degrees past the whole-instance kernel, pinned to each evaluation in turn: batched groups of
     # several sizes and grouped single instances must give the same bits.
     import ctypes
@@ -118,7 +128,7 @@ def test_mix_evaluations_agree(egg, nat, W, prec):
             assert results[0][b] == egg.hafnian(_sub(A, r), method="dp", check_symmetric=False)
 
 
-def test_mix_graph_replay(egg, nat, W):
+def test_mix_graph_replay(egg, nat, W, level_engine):
     # The second call of a shape records a graph and later calls replay it: results must not
     # change, including when the row sets change but the degree counts do not.
     A = W.gbs_parent(48, 51)
@@ -157,6 +167,7 @@ from conftest import load_package
 egg = load_package()
 from theeggman_b200 import workloads as W, _native as nat
 L = nat.lib()
+assert L.egg_dp_mix_set_engine(0) == 0  # the per-level engine is the one that tunes
 if sys.argv[1] == "tune":
     A, idxs = W.gbs_mix(8, 64, [24], 4)
     egg.hafnian_submatrices(A, idxs)
@@ -175,3 +186,112 @@ print(json.dumps([rc, b.value, g.value]))
             text = path.read_text()
             assert '"K": 24' in text and '"dtype": 1' in text, text
     assert runs[0][0] == 0 and runs[1] == runs[0], runs
+
+
+def _engine_results(egg, nat, engine, fn):
+    L = nat.lib()
+    prev = L.egg_dp_mix_engine()
+    nat.check(L.egg_dp_mix_set_engine(engine))
+    try:
+        n0 = L.egg_launch_count()
+        out = fn()
+        return out, L.egg_launch_count() - n0
+    finally:
+        nat.check(L.egg_dp_mix_set_engine(prev))
+
+
+@pytest.mark.parametrize("dtype,prec", [("f64", "exact"), ("f64", "fma"), ("f64", "mixed"), ("c128", "exact"),
+                                        ("c128", "fma"), ("c128", "mixed"), ("int", "exact")])
+def test_persistent_engine_equals_level_engine(egg, nat, W, dtype, prec):
+    """One cooperative launch per call (egg_mix_persist.cu) gives the per-level engine's bits, for
+    every element type and precision mode, on a mix of every degree 0..32 with odd sizes, empty row
+    sets and repeated rows."""
+    n = 48
+    if dtype == "int":
+        A = W.er_graph(n, 0.5, 61)
+    elif dtype == "c128":
+        A = W.gbs_parent(n, 62)
+    else:
+        A = W.dense_real(n, 63)
+    rng = np.random.default_rng(64)
+    sizes = list(range(0, 33)) * 3
+    rows = [rng.choice(n, size=k, replace=False) for k in sizes]
+    rows += [[0, 0, 1, 1], [5, 5, 5, 5, 7, 9]]
+    kw = dict(check_symmetric=False)
+    if dtype == "int":
+        kw["exact"] = True
+    else:
+        kw["prec"] = prec
+    lev, nl = _engine_results(egg, nat, 0, lambda: egg.hafnian_submatrices(A, rows, **kw))
+    per, npers = _engine_results(egg, nat, 1, lambda: egg.hafnian_submatrices(A, rows, **kw))
+    assert np.array_equal(per, lev)
+    assert npers == 1 and nl > 1, (npers, nl)
+    if dtype != "int" and prec == "exact":
+        for b in range(0, len(rows), 9):
+            r = rows[b]
+            exp = egg.hafnian(_sub(A, r), method="dp", check_symmetric=False) if len(r) else 1
+            assert per[b] == exp, b
+
+
+def test_persistent_engine_waves(egg, nat, W):
+    """A mix whose level buffers exceed the persistent launch's budget runs in waves of instances
+    (600 instances of degree 32 in Float64: two waves): same bits as the per-level engine."""
+    A = W.dense_real(40, 71)
+    rng = np.random.default_rng(72)
+    rows = [rng.choice(40, size=32, replace=False) for _ in range(600)]
+    rows += [rng.choice(40, size=k, replace=False) for k in (30, 28, 8, 2, 0, 31)]
+    lev, _ = _engine_results(egg, nat, 0, lambda: egg.hafnian_submatrices(A, rows, check_symmetric=False))
+    per, npers = _engine_results(egg, nat, 1, lambda: egg.hafnian_submatrices(A, rows, check_symmetric=False))
+    assert npers == 1
+    assert np.array_equal(per, lev)
+    # Only odd and empty row sets: no degree bin, the launch only scatters.
+    rows = [[1], [], [2, 3, 4], []]
+    per, npers = _engine_results(egg, nat, 1, lambda: egg.hafnian_submatrices(A, rows, check_symmetric=False))
+    assert npers == 1 and list(per) == [0.0, 1.0, 0.0, 1.0]
+
+
+def test_persistent_engine_device_entry(egg, nat, W):
+    """egg_dp_mix_device on the persistent engine equals the host entry; the engine switch refuses
+    other values."""
+    import torch
+
+    A = W.gbs_parent(40, 81)
+    rng = np.random.default_rng(82)
+    rows = [rng.choice(40, size=k, replace=False) for k in (24, 26, 8, 0, 3, 28)]
+    host = egg.hafnian_submatrices(A, rows, check_symmetric=False)
+    offs = np.zeros(len(rows) + 1, dtype=np.int64)
+    offs[1:] = np.cumsum([len(r) for r in rows])
+    flat = np.concatenate([np.asarray(r, dtype=np.int32) for r in rows])
+    dev = torch.device("cuda", 0)
+    dA = torch.from_numpy(np.asfortranarray(A).ravel(order="F").view(np.float64).copy()).to(dev)
+    drows = torch.from_numpy(flat).to(dev)
+    dout = torch.empty(2 * len(rows), dtype=torch.float64, device=dev)
+    L = nat.lib()
+    st = torch.cuda.Stream(dev)  # a stream of the caller's (the legacy default stream would be handle 0)
+    st.wait_stream(torch.cuda.current_stream(dev))
+    nat.check(L.egg_dp_mix_device(nat.EGG_C128, 0, dA.data_ptr(), 40, len(rows), nat.ptr(offs), drows.data_ptr(),
+                                  dout.data_ptr(), st.cuda_stream))
+    st.synchronize()
+    got = dout.cpu().numpy().view(np.complex128)
+    assert np.array_equal(got, host)
+    with pytest.raises(egg.ArgumentError):
+        nat.check(L.egg_dp_mix_set_engine(2))
+
+
+def test_barrier_bounded_wait(egg, nat):
+    """The persistent launch's grid barrier: with every block present it passes; made to expect one
+    block more than the grid has, each wait runs out after its limit, the launch still ends, the
+    call reports EGG_ERR_TIMEOUT, and the device stays usable."""
+    import ctypes
+
+    L = nat.lib()
+    passes = ctypes.c_int64(0)
+    nat.check(L.egg_selfcheck_barrier(0, 200_000_000, ctypes.byref(passes)))
+    assert passes.value > 0 and passes.value % 3 == 0
+    rc = L.egg_selfcheck_barrier(1, 20_000_000, ctypes.byref(passes))
+    assert rc == nat.EGG_ERR_TIMEOUT, rc
+    assert b"ran out" in L.egg_last_error()
+    with pytest.raises(egg.ArgumentError):
+        nat.check(L.egg_selfcheck_barrier(0, 10, None))
+    A = np.array([[0.0, 2.0], [2.0, 0.0]])
+    assert egg.hafnian_submatrices(A, [[0, 1]], check_symmetric=False)[0] == 2.0

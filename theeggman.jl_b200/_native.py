@@ -46,6 +46,7 @@ EXPORTS = (
     "egg_sieve_device", "egg_sieve_batch", "egg_sieve_batch_device", "egg_sieve_device_noalloc", "egg_launch_count",
     "egg_dp_mix", "egg_dp_mix_device", "egg_dp_mix_tuning", "egg_dp_mix_set_tuning", "egg_sieve_reference_sum",
     "egg_sieve_repeated_batch", "egg_sieve_repeated_batch_device", "egg_selfcheck_division",
+    "egg_dp_mix_set_engine", "egg_dp_mix_engine", "egg_selfcheck_barrier",
 )
 
 
@@ -113,6 +114,8 @@ def lib() -> ctypes.CDLL:
     L.egg_sieve_repeated_batch.argtypes = [i32, i32, i64, i64, vp, i64, vp, i32, vp]
     L.egg_sieve_repeated_batch_device.argtypes = [i32, i32, i64, i64, vp, i64, vp, i32, vp, vp]
     L.egg_selfcheck_division.argtypes = [vp, vp, i64, vp, vp]
+    L.egg_dp_mix_set_engine.argtypes = [i32]
+    L.egg_selfcheck_barrier.argtypes = [i32, i64, vp]
     return L
 
 

@@ -11,6 +11,7 @@
 #include <tuple>
 
 #include "egg_internal.cuh"
+#include "egg_mix.cuh"
 
 namespace egg {
 
@@ -649,11 +650,13 @@ int egg_dp_mix(int dtype, int prec, const void *A, int64_t n, int64_t B, const i
     char *base = (char *)c.scratch[7].ptr;
     if (abytes) EGG_CUDA_TRY(cudaMemcpyAsync(base, A, abytes, cudaMemcpyHostToDevice, c.stream));
     if (nrows) EGG_CUDA_TRY(cudaMemcpyAsync(base + offr, rows, (size_t)nrows * 4, cudaMemcpyHostToDevice, c.stream));
+    rc = mix_persistent_take_timeout();  // an earlier asynchronous mix that gave up at a barrier
+    if (rc) return rc;
     rc = mix_run(dtype, prec, base, n, B, offsets, (const int32_t *)(base + offr), base + offo, c.stream);
     if (rc) return rc;
     EGG_CUDA_TRY(cudaMemcpyAsync(out, base + offo, (size_t)B * oes, cudaMemcpyDeviceToHost, c.stream));
     EGG_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    return EGG_OK;
+    return mix_persistent_take_timeout();
 }
 
 int egg_dp_mix_device(int dtype, int prec, const void *A, int64_t n, int64_t B, const int64_t *offsets, const int32_t *rows,
@@ -665,7 +668,23 @@ int egg_dp_mix_device(int dtype, int prec, const void *A, int64_t n, int64_t B, 
     if (!offsets || !out || (n > 0 && !A) || (offsets[B] > 0 && !rows)) return fail(EGG_ERR_ARGUMENT, "null argument");
     if (offsets[0] != 0) return fail(EGG_ERR_ARGUMENT, "offsets[0] must be 0");
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+    const int rc = mix_persistent_take_timeout();  // an earlier asynchronous mix that gave up at a barrier
+    if (rc) return rc;
     return mix_run(dtype, prec, A, n, B, offsets, rows, out, st);
+}
+
+int egg_dp_mix_set_engine(int engine)
+{
+    std::lock_guard<std::recursive_mutex> lk(ctx().mu);
+    return mix_set_engine(engine);
+}
+
+int egg_dp_mix_engine(void) { return mix_engine(); }
+
+int egg_selfcheck_barrier(int extra, int64_t wait_ns, int64_t *passes)
+{
+    EGG_GUARD();
+    return barrier_selfcheck(extra, wait_ns, passes);
 }
 
 int egg_dp_mix_set_tuning(int K, int dtype, int prec, int batched, int64_t group)

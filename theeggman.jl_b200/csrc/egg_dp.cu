@@ -143,25 +143,6 @@ __global__ void __launch_bounds__(512) dp_small_kernel(const I *__restrict__ tra
 // suf now and its C(e - 1, j) joins pre one step later.  The arithmetic per state is that of the
 // plan kernels, in the same order, so results are identical.
 
-// Loads that bypass L1, for a level written earlier in the same kernel by other SMs (their L1
-// copies of the buffer, from two levels back, would be stale).
-template <class T> __device__ __forceinline__ T ld_l2(const T *p) { return __ldcg(p); }
-template <> __device__ __forceinline__ cd ld_l2<cd>(const cd *p)
-{
-    const double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
-    return cd{v.x, v.y};
-}
-template <> __device__ __forceinline__ cf ld_l2<cf>(const cf *p)
-{
-    const float2 v = __ldcg(reinterpret_cast<const float2 *>(p));
-    return cf{v.x, v.y};
-}
-template <> __device__ __forceinline__ __int128 ld_l2<__int128>(const __int128 *p)
-{
-    const longlong2 v = __ldcg(reinterpret_cast<const longlong2 *>(p));
-    return (__int128)(unsigned long long)v.x | ((__int128)v.y << 64);
-}
-
 // One step of the walk: load the child value and pair value for element ej, then advance
 // pre/suf/ej to the next element (if this is not the last step).  L2ONLY reads the child level
 // through L2 only.
@@ -255,23 +236,6 @@ __device__ __forceinline__ AT walk_state(M m, const uint2 *TP, int ld, int c, in
             if (x + u <= c) acc = madd(Op{}, acc, pv[u], hv[u]);
     }
     return acc;
-}
-
-// Level c = 2: state s = {e1 < e2} (colex rank C(e2, 2) + e1) has the single transition to the
-// empty set, whose value is 1.
-template <class Op, class PT, class HT, class AT>
-__device__ __forceinline__ HT first_level_value(int64_t s, int K, const PT *P, int64_t B, int64_t b)
-{
-    const int m0 = (K - 2) / 2;
-    int e2 = (int)((1.0 + sqrt(1.0 + 8.0 * (double)s)) * 0.5);
-    while ((int64_t)e2 * (e2 - 1) / 2 > s) --e2;
-    while ((int64_t)(e2 + 1) * e2 / 2 <= s) ++e2;
-    const int e1 = (int)(s - (int64_t)e2 * (e2 - 1) / 2);
-    const int ib = e1 + m0 + 1;
-    const int q = (ib - 1) * K - (ib * (ib + 1)) / 2 + m0 + e2;
-    HT out;
-    store(out, madd(Op{}, zero_of<AT>(), P[(int64_t)q * B + b], one_of<HT>()));
-    return out;
 }
 
 template <class Op, class PT, class HT, class AT>
@@ -1187,8 +1151,6 @@ __global__ void __launch_bounds__(256) dpc_first_grouped_kernel(const PT *__rest
         Hi[s] = first_level_value<Op, PT, HT, AT>(s, K, Pi, 1, 0);
 }
 
-__device__ __forceinline__ void store(double &d, float a) { d = (double)a; }
-__device__ __forceinline__ void store(cd &d, cf a) { d = cd{(double)a.re, (double)a.im}; }
 
 template <class HT, class OT>
 __global__ void copy_strided_kernel(const HT *__restrict__ in, int64_t ld, OT *__restrict__ out, int64_t G)

@@ -52,6 +52,49 @@ __device__ __forceinline__ void store(cd &d, cd a) { d = a; }
 __device__ __forceinline__ void store(cf &d, cf a) { d = a; }
 __device__ __forceinline__ void store(cf &d, cd a) { d = cf{__double2float_rn(a.re), __double2float_rn(a.im)}; }
 __device__ __forceinline__ void store(__int128 &d, __int128 a) { d = a; }
+// Widening stores of the mixed form's results (FP32 storage, FP64 output).
+__device__ __forceinline__ void store(double &d, float a) { d = (double)a; }
+__device__ __forceinline__ void store(cd &d, cf a) { d = cd{(double)a.re, (double)a.im}; }
+
+// Loads that bypass L1, for a level written earlier in the same kernel by other SMs (their L1
+// copies of the buffer, from two levels back, would be stale).
+template <class T> __device__ __forceinline__ T ld_l2(const T *p) { return __ldcg(p); }
+template <> __device__ __forceinline__ int64_t ld_l2<int64_t>(const int64_t *p)
+{
+    return (int64_t)__ldcg(reinterpret_cast<const long long *>(p));
+}
+template <> __device__ __forceinline__ cd ld_l2<cd>(const cd *p)
+{
+    const double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
+    return cd{v.x, v.y};
+}
+template <> __device__ __forceinline__ cf ld_l2<cf>(const cf *p)
+{
+    const float2 v = __ldcg(reinterpret_cast<const float2 *>(p));
+    return cf{v.x, v.y};
+}
+template <> __device__ __forceinline__ __int128 ld_l2<__int128>(const __int128 *p)
+{
+    const longlong2 v = __ldcg(reinterpret_cast<const longlong2 *>(p));
+    return (__int128)(unsigned long long)v.x | ((__int128)v.y << 64);
+}
+
+// Level c = 2: state s = {e1 < e2} (colex rank C(e2, 2) + e1) has the single transition to the
+// empty set, whose value is 1.
+template <class Op, class PT, class HT, class AT>
+__device__ __forceinline__ HT first_level_value(int64_t s, int K, const PT *P, int64_t B, int64_t b)
+{
+    const int m0 = (K - 2) / 2;
+    int e2 = (int)((1.0 + sqrt(1.0 + 8.0 * (double)s)) * 0.5);
+    while ((int64_t)e2 * (e2 - 1) / 2 > s) --e2;
+    while ((int64_t)(e2 + 1) * e2 / 2 <= s) ++e2;
+    const int e1 = (int)(s - (int64_t)e2 * (e2 - 1) / 2);
+    const int ib = e1 + m0 + 1;
+    const int q = (ib - 1) * K - (ib * (ib + 1)) / 2 + m0 + e2;
+    HT out;
+    store(out, madd(Op{}, zero_of<AT>(), P[(int64_t)q * B + b], one_of<HT>()));
+    return out;
+}
 
 // Transitions whose loads a thread issues together before accumulating them in order.
 static constexpr int kBatch = 8;

@@ -12,7 +12,9 @@
 
 namespace egg {
 
-template <int C, class Op, class M, class PT, class HT, class AT>
+// L2ONLY reads the child level through L2 only: a kernel that wrote that level itself, on other
+// SMs, must not read it through an SM's L1, which may still hold the buffer's previous contents.
+template <int C, class Op, class M, class PT, class HT, class AT, bool L2ONLY = false>
 __device__ __forceinline__ AT walk_fixed(M m, const uint2 *__restrict__ TP, int K, int m0, const PT *__restrict__ Ps,
                                          const HT *__restrict__ Hprev)
 {
@@ -45,7 +47,7 @@ __device__ __forceinline__ AT walk_fixed(M m, const uint2 *__restrict__ TP, int 
         for (int u = 0; u < kBatch; ++u) {
             const int x = x0 + u;
             if (x <= C) {
-                hv[u] = Hprev[pre + suf];
+                hv[u] = L2ONLY ? ld_l2(Hprev + pre + suf) : Hprev[pre + suf];
                 pv[u] = Prow[ej];
                 pre += padd;
                 if (x < C) {

@@ -162,9 +162,9 @@ struct Context {
     static constexpr size_t kPinnedBytes = 128 * 1024;
     int num_sms = 0;
     std::map<std::pair<int, int>, DevPlan> plans;
-    DevBuf scratch[10];  // H, P, out, sieve matrix, sieve out, misc, mixed-degree batch + its staging,
-                         // the reference-order sieve's terms, the repeated batches' preparation:
-                         // grown on demand, never shrunk
+    DevBuf scratch[11];  // H, P, out, sieve matrix, sieve out, misc, mixed-degree batch + its staging,
+                         // the reference-order sieve's terms, the repeated batches' preparation, the
+                         // persistent mix launch's step tables: grown on demand, never shrunk
     std::recursive_mutex mu;
 };
 

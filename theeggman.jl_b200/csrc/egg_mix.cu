@@ -11,76 +11,25 @@
 //   3. each bin runs the subset DP of its degree on its resident closed-form plan (dp_run);
 //   4. one scatter kernel writes the results back in the caller's order (odd sizes give 0,
 //      empty row sets give 1).
+// Those are the per-level engine's launches.  By default, mixes of degrees up to 32 run steps 2-4 as
+// one cooperative launch instead (egg_mix_persist.cu); both give the same results, bit for bit.
 // Every result is the value hafnian(A[r, r]; method = :dp) gives for the same precision mode.
 #include <map>
 #include <tuple>
 
 #include "egg_internal.cuh"
+#include "egg_mix.cuh"
 #include "egg_tunecache.h"
 
 namespace egg {
 
-static constexpr int kMaxBins = 32;  // even degrees 2..64
-
-struct MixBin {
-    int K, npairs;
-    int64_t count;  // instances in the bin
-    int64_t first;  // position of the bin's first instance in the sorted order
-    int64_t poff;   // element offset of the bin's P
-    int64_t ebase;  // gather elements before this bin
-    int64_t lay;    // P layout: consecutive groups of `lay` instances, instance-fastest within a group
-};
-
-struct MixBins {
-    int nb;
-    MixBin b[kMaxBins];
-};
-
-template <class T> __device__ __forceinline__ T mix_one();
-template <> __device__ __forceinline__ double mix_one<double>() { return 1.0; }
-template <> __device__ __forceinline__ cd mix_one<cd>() { return cd{1.0, 0.0}; }
-template <> __device__ __forceinline__ __int128 mix_one<__int128>() { return 1; }
-
-template <class T> __device__ __forceinline__ T nan_of();
-template <> __device__ __forceinline__ double nan_of<double>() { return __longlong_as_double(0x7ff8000000000000LL); }
-template <> __device__ __forceinline__ cd nan_of<cd>() { return cd{nan_of<double>(), nan_of<double>()}; }
-template <> __device__ __forceinline__ int64_t nan_of<int64_t>() { return 0; }
-
-// The bin's pairs, A[r[qi], r[qj]] for q = _pair_index(qi+1, qj+1, K) - 1, in groups of `lay`
-// instances: group g at poff + g * npairs * lay, pair q of its instance i at q * glen + i.  (lay = 1
-// is instance-major; lay >= count is the instance-fastest matrix of _gather_pairs_batch.)
-// Row indices outside [0, n) are not read: the pair gets NaN (0 for integers).
 template <class T>
 __global__ void mix_gather_kernel(const T *__restrict__ A, int64_t n, const int64_t *__restrict__ offsets,
                                   const int32_t *__restrict__ rows, const int32_t *__restrict__ order, MixBins bins,
                                   int64_t total, T *__restrict__ P)
 {
-    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x) {
-        int k = 0;
-        while (k + 1 < bins.nb && bins.b[k + 1].ebase <= g) ++k;
-        const MixBin &bn = bins.b[k];
-        const int64_t e = g - bn.ebase;
-        // e enumerates (group, pair, instance in group); groups hold `lay` instances (the last fewer).
-        const int64_t per = (int64_t)bn.npairs * bn.lay;
-        const int64_t grp = e / per, g0 = grp * bn.lay;
-        const int64_t glen = bn.count - g0 < bn.lay ? bn.count - g0 : bn.lay;
-        const int64_t w = e - grp * per;
-        const int64_t q = w / glen, i = g0 + (w - q * glen);
-        int qi = 0, rem = (int)q, len = bn.K - 1;
-        while (rem >= len) {
-            rem -= len;
-            --len;
-            ++qi;
-        }
-        const int qj = qi + 1 + rem;
-        const int32_t *r = rows + offsets[order[bn.first + i]];
-        const int64_t a = r[qi], c = r[qj];
-        if (a < 0 || a >= n || c < 0 || c >= n) {
-            P[bn.poff + e] = nan_of<T>();
-        } else {
-            P[bn.poff + e] = A[a + c * n];
-        }
-    }
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x)
+        mix_gather_elem<T, T>(g, A, n, offsets, rows, order, bins, P);
 }
 
 // out[order[k]] = sorted[k] for the DP instances; the trailing `nzero` entries of the order get 0
@@ -365,10 +314,17 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
     char *dP = base + off_p, *dsorted = base + off_r, *tmpP = base + off_t, *tmpO = base + off_to;
     EGG_CUDA_TRY(cudaMemcpyAsync(doff, offsets, (size_t)(B + 1) * 8, cudaMemcpyHostToDevice, st));
     EGG_CUDA_TRY(cudaMemcpyAsync(dorder, order.data(), (size_t)B * 4, cudaMemcpyHostToDevice, st));
-    // 3. How each bin runs: one launch for degrees the whole-instance kernel covers, else the tuned
-    // choice (timed on first use, unless the stream is being captured).
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     EGG_CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+    // The whole mix in one cooperative launch where that engine takes it (a stream being captured
+    // records the per-level launches instead).
+    if (mix_engine() == kMixPersistent && cap == cudaStreamCaptureStatusNone && mix_persistent_ok(bins, plans, dtype, prec)) {
+        rc = mix_persistent_run(dtype, prec, dA, n, B, bins, plans, doff, drows, dorder, total, ndp, nzero, dsorted, dout, st);
+        if (rc != kDpNotHere) return rc;
+        rc = EGG_OK;
+    }
+    // 3. How each bin runs: one launch for degrees the whole-instance kernel covers, else the tuned
+    // choice (timed on first use, unless the stream is being captured).
     std::vector<BinExec> exs(bins.nb);
     size_t hmax = 0, p32max = 0;
     for (int k = 0; k < bins.nb; ++k) {
