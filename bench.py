@@ -349,7 +349,7 @@ class MixWorkload:
 
     kind = "dp"
 
-    def __init__(self, egg, W, B: int, prec: str, seq: bool, seed: int, engine: int = 1):
+    def __init__(self, egg, W, B: int, prec: str, seq: bool, seed: int, engine: int = 0):
         from theeggman_b200.hafnian import _mix_layout
 
         self.egg, self.B, self.prec_name, self.seq, self.engine = egg, B, prec, seq, engine
@@ -617,8 +617,8 @@ def make_workload(name: str, egg, W, rank: int):
         return MixWorkload(egg, W, 4096, "fma", False, 4 + 100 * rank)
     if name == "mix4096mixed":
         return MixWorkload(egg, W, 4096, "mixed", False, 4 + 100 * rank)
-    if name == "mix4096levels":
-        return MixWorkload(egg, W, 4096, "exact", False, 4 + 100 * rank, engine=0)
+    if name == "mix4096one":
+        return MixWorkload(egg, W, 4096, "exact", False, 4 + 100 * rank, engine=1)
     if name == "mix4096seq":
         return MixWorkload(egg, W, 4096, "exact", True, 4 + 100 * rank)
     if name == "rep14":
@@ -729,7 +729,7 @@ def run_reference(args):
 # stays within a few minutes.
 PER_CONFIG = [("dp20", 20), ("sieve20", 20), ("sieve20f", 20), ("dp32", 10), ("sieve40", 10), ("sieve40f", 10),
               ("sieve40c", 3), ("sieve40cf", 5), ("sieve40gf", 5), ("dp36", 5), ("dp40", 5), ("dp40mixed", 5),
-              ("dp40int", 5), ("dp20x1024", 10), ("mix4096", 10), ("mix4096levels", 10), ("mix4096fma", 10), ("mix4096mixed", 10), ("mix4096seq", 3),
+              ("dp40int", 5), ("dp20x1024", 10), ("mix4096", 10), ("mix4096one", 10), ("mix4096fma", 10), ("mix4096mixed", 10), ("mix4096seq", 3),
               ("rep14", 10), ("rep14f", 10), ("rep20c", 3), ("rep20cf", 3)]
 PER_CONFIG_BUDGET_S = 300.0
 

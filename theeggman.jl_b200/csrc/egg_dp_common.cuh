@@ -79,6 +79,31 @@ template <> __device__ __forceinline__ __int128 ld_l2<__int128>(const __int128 *
     return (__int128)(unsigned long long)v.x | ((__int128)v.y << 64);
 }
 
+// Weak loads cached in L1 (ld.global.ca), never the read-only path: for a level that other blocks
+// of the same launch wrote before a grid-wide barrier.  The barrier's fences order those writes
+// before these loads, as for any ordinary load after a cooperative grid synchronisation; the
+// read-only path (ld.global.nc), which a const __restrict__ pointer may get, has no such guarantee.
+template <class T> __device__ __forceinline__ T ld_ca(const T *p) { return __ldca(p); }
+template <> __device__ __forceinline__ int64_t ld_ca<int64_t>(const int64_t *p)
+{
+    return (int64_t)__ldca(reinterpret_cast<const long long *>(p));
+}
+template <> __device__ __forceinline__ cd ld_ca<cd>(const cd *p)
+{
+    const double2 v = __ldca(reinterpret_cast<const double2 *>(p));
+    return cd{v.x, v.y};
+}
+template <> __device__ __forceinline__ cf ld_ca<cf>(const cf *p)
+{
+    const float2 v = __ldca(reinterpret_cast<const float2 *>(p));
+    return cf{v.x, v.y};
+}
+template <> __device__ __forceinline__ __int128 ld_ca<__int128>(const __int128 *p)
+{
+    const longlong2 v = __ldca(reinterpret_cast<const longlong2 *>(p));
+    return (__int128)(unsigned long long)v.x | ((__int128)v.y << 64);
+}
+
 // Level c = 2: state s = {e1 < e2} (colex rank C(e2, 2) + e1) has the single transition to the
 // empty set, whose value is 1.
 template <class Op, class PT, class HT, class AT>

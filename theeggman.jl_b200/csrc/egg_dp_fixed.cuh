@@ -12,9 +12,11 @@
 
 namespace egg {
 
-// L2ONLY reads the child level through L2 only: a kernel that wrote that level itself, on other
-// SMs, must not read it through an SM's L1, which may still hold the buffer's previous contents.
-template <int C, class Op, class M, class PT, class HT, class AT, bool L2ONLY = false>
+// How the child level is read: kLoadPlain (the level kernels: the level was written by an earlier
+// launch), kLoadL2 (through L2 only) or kLoadCA (weak loads cached in L1, for a level that other
+// blocks of the same launch wrote before a grid-wide barrier; see ld_ca).
+constexpr int kLoadPlain = 0, kLoadL2 = 1, kLoadCA = 2;
+template <int C, class Op, class M, class PT, class HT, class AT, int LOAD = kLoadPlain>
 __device__ __forceinline__ AT walk_fixed(M m, const uint2 *__restrict__ TP, int K, int m0, const PT *__restrict__ Ps,
                                          const HT *__restrict__ Hprev)
 {
@@ -47,7 +49,9 @@ __device__ __forceinline__ AT walk_fixed(M m, const uint2 *__restrict__ TP, int 
         for (int u = 0; u < kBatch; ++u) {
             const int x = x0 + u;
             if (x <= C) {
-                hv[u] = L2ONLY ? ld_l2(Hprev + pre + suf) : Hprev[pre + suf];
+                if constexpr (LOAD == kLoadL2) hv[u] = ld_l2(Hprev + pre + suf);
+                else if constexpr (LOAD == kLoadCA) hv[u] = ld_ca(Hprev + pre + suf);
+                else hv[u] = Hprev[pre + suf];
                 pv[u] = Prow[ej];
                 pre += padd;
                 if (x < C) {

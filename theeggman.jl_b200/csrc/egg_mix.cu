@@ -11,8 +11,9 @@
 //   3. each bin runs the subset DP of its degree on its resident closed-form plan (dp_run);
 //   4. one scatter kernel writes the results back in the caller's order (odd sizes give 0,
 //      empty row sets give 1).
-// Those are the per-level engine's launches.  By default, mixes of degrees up to 32 run steps 2-4 as
-// one cooperative launch instead (egg_mix_persist.cu); both give the same results, bit for bit.
+// Those are the per-level engine's launches, the default.  On request (egg_dp_mix_set_engine),
+// mixes of degrees up to 32 run steps 2-4 as one cooperative launch instead (egg_mix_persist.cu);
+// both give the same results, bit for bit.
 // Every result is the value hafnian(A[r, r]; method = :dp) gives for the same precision mode.
 #include <map>
 #include <tuple>
@@ -140,12 +141,19 @@ static int run_bin(const DevPlan &plan, int dtype, int prec, const MixBin &bn, c
     return EGG_OK;
 }
 
-// Time each candidate on the bin's first instances (at most 64) and keep the fastest per instance.
+// Instances a degree is tuned on: the whole bin up to this many, so that the timing sees the
+// groups the batch will run (a small sample favoured small groups that the full batch runs slower).
+static constexpr int64_t kTuneSample = 512;
+
+// Time each candidate on the bin's first instances (at most kTuneSample) and keep the fastest.
+// Each candidate is timed in three rounds, the candidates taking turns within a round, and its best
+// round counts: one timing alone can be thrown off (a clock change, the host falling behind a run
+// of many small launches) and pick a grouping that is slower in the batch.
 static int tune_bin(const DevPlan &plan, int dtype, int prec, const MixBin &bn, const void *dA, int64_t n,
                     const int64_t *doff, const int32_t *drows, const int32_t *dorder, char *tmpP, char *tmpO, size_t es,
                     size_t oes, cudaStream_t st, BinExec *best)
 {
-    const int64_t S = bn.count < 64 ? bn.count : 64;
+    const int64_t S = bn.count < kTuneSample ? bn.count : kTuneSample;
     std::vector<BinExec> cands;
     for (int64_t L : {(int64_t)64, (int64_t)16})
         if (L <= S || L == 64) cands.push_back({true, L < S ? L : S});
@@ -155,35 +163,44 @@ static int tune_bin(const DevPlan &plan, int dtype, int prec, const MixBin &bn, 
     cudaEvent_t e0, e1;
     EGG_CUDA_TRY(cudaEventCreate(&e0));
     EGG_CUDA_TRY(cudaEventCreate(&e1));
-    float bestv = 0;
+    std::vector<float> bestms(cands.size(), 0.0f);
     bool have = false;
     int rc = EGG_OK;
-    for (const BinExec &cand : cands) {
-        MixBins one;
-        one.nb = 1;
-        one.b[0] = bn;
-        one.b[0].count = S;
-        one.b[0].poff = 0;
-        one.b[0].ebase = 0;
-        one.b[0].lay = cand.batched ? cand.group : 1;
-        rc = launch_gather(dtype, dA, n, doff, drows, dorder, one, (int64_t)bn.npairs * S, tmpP, st);
-        if (!rc) rc = run_bin(plan, dtype, prec, one.b[0], cand, tmpP, tmpO, es, oes, st);  // warm-up
-        if (rc) break;
-        cudaEventRecord(e0, st);
-        rc = run_bin(plan, dtype, prec, one.b[0], cand, tmpP, tmpO, es, oes, st);
-        cudaEventRecord(e1, st);
-        if (rc) break;
-        if (cudaEventSynchronize(e1) != cudaSuccess) {
-            rc = fail(EGG_ERR_CUDA, "tuning run failed");
-            break;
+    constexpr int kRounds = 3;
+    for (int round = 0; round < kRounds && !rc; ++round) {
+        for (size_t ci = 0; ci < cands.size() && !rc; ++ci) {
+            const BinExec &cand = cands[ci];
+            MixBins one;
+            one.nb = 1;
+            one.b[0] = bn;
+            one.b[0].count = S;
+            one.b[0].poff = 0;
+            one.b[0].ebase = 0;
+            one.b[0].lay = cand.batched ? cand.group : 1;
+            rc = launch_gather(dtype, dA, n, doff, drows, dorder, one, (int64_t)bn.npairs * S, tmpP, st);
+            if (!rc && round == 0) rc = run_bin(plan, dtype, prec, one.b[0], cand, tmpP, tmpO, es, oes, st);  // warm-up
+            if (rc) break;
+            cudaEventRecord(e0, st);
+            rc = run_bin(plan, dtype, prec, one.b[0], cand, tmpP, tmpO, es, oes, st);
+            cudaEventRecord(e1, st);
+            if (rc) break;
+            if (cudaEventSynchronize(e1) != cudaSuccess) {
+                rc = fail(EGG_ERR_CUDA, "tuning run failed");
+                break;
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (round == 0 || ms < bestms[ci]) bestms[ci] = ms;
         }
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (!have || ms < bestv) {
-            bestv = ms;
-            *best = cand;
-            have = true;
-        }
+    }
+    if (!rc) {
+        float bestv = 0;
+        for (size_t ci = 0; ci < cands.size(); ++ci)
+            if (!have || bestms[ci] < bestv) {
+                bestv = bestms[ci];
+                *best = cands[ci];
+                have = true;
+            }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -305,7 +322,7 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
     for (int k = 0; k < bins.nb; ++k) npmax = bins.b[k].npairs > npmax ? bins.b[k].npairs : npmax;
     const size_t off_o = align256((size_t)(B + 1) * 8), off_p = off_o + align256((size_t)B * 4);
     const size_t off_r = off_p + align256((size_t)total * es), off_t = off_r + align256((size_t)(ndp ? ndp : 1) * oes);
-    const size_t off_to = off_t + align256((size_t)64 * npmax * es), arena = off_to + align256((size_t)64 * oes);
+    const size_t off_to = off_t + align256((size_t)kTuneSample * npmax * es), arena = off_to + align256((size_t)kTuneSample * oes);
     int rc = ensure_buf(c.scratch[6], arena);
     if (rc) return rc;
     char *base = (char *)c.scratch[6].ptr;

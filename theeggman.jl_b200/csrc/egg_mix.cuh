@@ -89,8 +89,9 @@ int mix_persistent_run(int dtype, int prec, const void *dA, int64_t n, int64_t B
 // EGG_ERR_TIMEOUT (once) if a persistent launch that has ended gave up waiting at a barrier.
 int mix_persistent_take_timeout();
 
-// The engine a mix runs on: kMixPersistent (the default) where mix_persistent_ok, else per-level
-// launches (recorded as one CUDA graph on a shape's second call and replayed after that).
+// The engine a mix runs on: per-level launches (the default; recorded as one CUDA graph on a
+// shape's second call and replayed after that), or kMixPersistent, one cooperative launch, where
+// mix_persistent_ok.
 constexpr int kMixLevels = 0;
 constexpr int kMixPersistent = 1;
 int mix_engine();

@@ -10,13 +10,22 @@
 //      mixes run several waves);
 //   3. the scatter of the results into the caller's order.
 // Within a step the work is a list of units -- (bin, instance, chunk of 2048 consecutive states of
-// the level) -- that blocks claim one at a time from a counter, so bins of every size share the
+// the level) -- that blocks claim in short runs from a counter, so bins of every size share the
 // SMs and small levels fill the gaps of large ones.  A unit is evaluated exactly as the per-level
 // engine's fixed-popcount kernel evaluates a chunk (egg_dp_fixed.cuh: colex unrank and successors,
 // then walk_fixed in plan order), so every result is bit-identical to that engine's and to
-// hafnian(A[r, r]; method = :dp) in the same precision mode.  Level buffers are rewritten within
-// the launch, so every value another block wrote (the pairs, the previous level, the results) is
-// read through L2 only.
+// hafnian(A[r, r]; method = :dp) in the same precision mode.  Values other blocks wrote earlier in
+// the launch are read after a grid barrier: the previous level with weak loads cached in L1
+// (ld_ca), the pairs and the results through L2 only; never through the read-only path.
+//
+// Measured on the 4096-instance configuration-4 mix (ComplexF64, degrees 8..32, one B200): this
+// engine 50.4 ms a batch, the per-level engine (tuned groups, graph replay) 45.3 ms, so the
+// per-level engine is the default.  The level kernels there are compiled per popcount, each with
+// the registers its walk needs; one kernel serving every popcount carries the largest walk's
+// registers (or spills them at three blocks per SM), and that is most of the difference.
+// Measured variants: two blocks per SM 53.1 ms, four 53.6 ms; a claim of one unit at a time
+// 61.7 ms; the previous level read through L2 only instead of L1, no change; waves of 1 GiB,
+// 8 GiB and 16 GiB of level buffers 54.7, 49.8 and 50.6 ms.
 #include "egg_gridbar.cuh"
 #include "egg_internal.cuh"
 #include "egg_dp_fixed.cuh"
@@ -28,6 +37,12 @@ static constexpr int kChunk = kRun * kLevelThreads;                             
 static constexpr int kMaxU = 32;                                                    // mask positions
 static constexpr size_t kTableBytes = (size_t)kMaxU * (kMaxU + 1) * sizeof(uint2);  // pair table, c <= 32
 static constexpr unsigned long long kBarrierWaitNs = 2000000000ull;                  // 2 s per barrier
+// Blocks per SM the kernel is compiled for (at most 85 registers a thread at three).
+static constexpr int kPersistMinBlocks = 3;
+// A block claims about 1/kClaimsPerBlock of its share of a step's units at a time: consecutive
+// chunks of one instance stay on one SM (its pairs and pair table stay in shared memory, and
+// neighbouring chunks share children in L1), while late claims still even out the blocks.
+static constexpr int64_t kClaimsPerBlock = 64;
 
 // One (bin, level) of a step: the level's states for `ninst` consecutive instances of the bin.
 struct PSeg {
@@ -45,6 +60,7 @@ struct PSeg {
 struct PStep {
     int seg0, nseg;
     int64_t units;
+    int64_t grab;  // units per claim
 };
 
 struct PersistArgs {
@@ -79,7 +95,7 @@ template <class Op, class PT, class HT, class AT>
 __device__ __forceinline__ AT walk_level(int c, uint32_t m, const uint2 *TP, int K, int m0, const PT *Ps, const HT *Hp)
 {
 #define EGG_WALK_CASE(CC) \
-    case CC: return walk_fixed<CC, Op, uint32_t, PT, HT, AT, true>(m, TP, K, m0, Ps, Hp);
+    case CC: return walk_fixed<CC, Op, uint32_t, PT, HT, AT, kLoadCA>(m, TP, K, m0, Ps, Hp);
     switch (c) {
         EGG_WALK_CASE(4) EGG_WALK_CASE(6) EGG_WALK_CASE(8) EGG_WALK_CASE(10) EGG_WALK_CASE(12) EGG_WALK_CASE(14)
         EGG_WALK_CASE(16) EGG_WALK_CASE(18) EGG_WALK_CASE(20) EGG_WALK_CASE(22) EGG_WALK_CASE(24) EGG_WALK_CASE(26)
@@ -89,10 +105,8 @@ __device__ __forceinline__ AT walk_level(int c, uint32_t m, const uint2 *TP, int
     return zero_of<AT>();
 }
 
-// Two blocks of 256 threads per SM (at most 128 registers a thread): the fixed-popcount level
-// kernels run two to three blocks per SM at the levels that dominate.
 template <class Op, class T, class PT, class HT, class AT, class OT>
-__global__ void __launch_bounds__(kLevelThreads, 2) mix_persistent_kernel(PersistArgs a)
+__global__ void __launch_bounds__(kLevelThreads, kPersistMinBlocks) mix_persistent_kernel(PersistArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t *masks = reinterpret_cast<uint32_t *>(smem_raw);
@@ -117,55 +131,59 @@ __global__ void __launch_bounds__(kLevelThreads, 2) mix_persistent_kernel(Persis
         const PStep sd = a.steps[st];
         for (int i = tid; i < sd.nseg; i += blockDim.x) sseg[i] = a.segs[sd.seg0 + i];
         for (;;) {
-            __syncthreads();  // the previous unit is done with s_unit, the masks, the table and the pairs
-            if (tid == 0) s_unit = (int64_t)atomicAdd(&a.ctr[st], 1u);
+            __syncthreads();  // the previous claim is done with s_unit, the masks, the table and the pairs
+            if (tid == 0) s_unit = (int64_t)atomicAdd(&a.ctr[st], (unsigned)sd.grab);
             __syncthreads();
-            const int64_t u = s_unit;
-            if (u >= sd.units) break;
-            int j = 0;
-            while (j + 1 < sd.nseg && sseg[j + 1].ubegin <= u) ++j;
-            const PSeg &sg = sseg[j];
-            const int64_t w = u - sg.ubegin, inst = w / sg.nchunk;
-            const int64_t s0 = (w - inst * sg.nchunk) * (int64_t)kChunk;
-            const int K = sg.K, c = sg.c, npairs = K * (K - 1) / 2;
-            const int cnt = (int)(sg.n - s0 < kChunk ? sg.n - s0 : kChunk);
-            const PT *Pi = (const PT *)sg.P + inst * npairs;
-            if (c > 2 && tkey != K * 64 + c) {
-                fill_pair_table(TP, a.binom, (K + c) / 2, c + 1, tid, blockDim.x);
-                tkey = K * 64 + c;
-            }
-            if (pkey != Pi) {
-                for (int q = tid; q < npairs; q += blockDim.x) Ps[q] = ld_l2(Pi + q);
-                pkey = Pi;
-            }
-            __syncthreads();
-            if (c == 2) {
-                for (int i = tid; i < cnt; i += blockDim.x) {
-                    const HT v = first_level_value<Op, PT, HT, AT>(s0 + i, K, Ps, 1, 0);
-                    if (c == K) store(((OT *)sg.out)[inst], v);
-                    else ((HT *)sg.cur)[inst * sg.ldh + s0 + i] = v;
+            const int64_t u0 = s_unit;
+            if (u0 >= sd.units) break;
+            const int64_t u1 = u0 + sd.grab < sd.units ? u0 + sd.grab : sd.units;
+            for (int64_t u = u0; u < u1; ++u) {
+                if (u > u0) __syncthreads();  // the previous unit is done with the masks, the table and the pairs
+                int j = 0;
+                while (j + 1 < sd.nseg && sseg[j + 1].ubegin <= u) ++j;
+                const PSeg &sg = sseg[j];
+                const int64_t w = u - sg.ubegin, inst = w / sg.nchunk;
+                const int64_t s0 = (w - inst * sg.nchunk) * (int64_t)kChunk;
+                const int K = sg.K, c = sg.c, npairs = K * (K - 1) / 2;
+                const int cnt = (int)(sg.n - s0 < kChunk ? sg.n - s0 : kChunk);
+                const PT *Pi = (const PT *)sg.P + inst * npairs;
+                if (c > 2 && tkey != K * 64 + c) {
+                    fill_pair_table(TP, a.binom, (K + c) / 2, c + 1, tid, blockDim.x);
+                    tkey = K * 64 + c;
                 }
-            } else {
-                const int m0 = (K - c) / 2, U = K - m0;
-                const int r0 = tid * kRun;
-                if (r0 < cnt) {
-                    uint32_t m = colex_unrank<uint32_t>(TP, c + 1, U, c, (uint32_t)(s0 + r0));
-                    masks[r0] = m;
-                    for (int r = 1; r < kRun && r0 + r < cnt; ++r) {
-                        m = colex_next<uint32_t>(m);
-                        masks[r0 + r] = m;
-                    }
+                if (pkey != Pi) {
+                    for (int q = tid; q < npairs; q += blockDim.x) Ps[q] = ld_l2(Pi + q);
+                    pkey = Pi;
                 }
                 __syncthreads();
-                const HT *Hp = (const HT *)sg.prev + inst * sg.ldh;
-                for (int i = tid; i < cnt; i += blockDim.x) {
-                    const AT acc = walk_level<Op, PT, HT, AT>(c, masks[i], TP, K, m0, Ps, Hp);
-                    if (c == K) {
-                        HT h;
-                        store(h, acc);
-                        store(((OT *)sg.out)[inst], h);
-                    } else {
-                        store(((HT *)sg.cur)[inst * sg.ldh + s0 + i], acc);
+                if (c == 2) {
+                    for (int i = tid; i < cnt; i += blockDim.x) {
+                        const HT v = first_level_value<Op, PT, HT, AT>(s0 + i, K, Ps, 1, 0);
+                        if (c == K) store(((OT *)sg.out)[inst], v);
+                        else ((HT *)sg.cur)[inst * sg.ldh + s0 + i] = v;
+                    }
+                } else {
+                    const int m0 = (K - c) / 2, U = K - m0;
+                    const int r0 = tid * kRun;
+                    if (r0 < cnt) {
+                        uint32_t m = colex_unrank<uint32_t>(TP, c + 1, U, c, (uint32_t)(s0 + r0));
+                        masks[r0] = m;
+                        for (int r = 1; r < kRun && r0 + r < cnt; ++r) {
+                            m = colex_next<uint32_t>(m);
+                            masks[r0 + r] = m;
+                        }
+                    }
+                    __syncthreads();
+                    const HT *Hp = (const HT *)sg.prev + inst * sg.ldh;
+                    for (int i = tid; i < cnt; i += blockDim.x) {
+                        const AT acc = walk_level<Op, PT, HT, AT>(c, masks[i], TP, K, m0, Ps, Hp);
+                        if (c == K) {
+                            HT h;
+                            store(h, acc);
+                            store(((OT *)sg.out)[inst], h);
+                        } else {
+                            store(((HT *)sg.cur)[inst * sg.ldh + s0 + i], acc);
+                        }
                     }
                 }
             }
@@ -223,7 +241,7 @@ int mix_persistent_take_timeout()
     return EGG_OK;
 }
 
-static int g_engine = kMixPersistent;
+static int g_engine = kMixLevels;
 
 int mix_engine() { return g_engine; }
 
@@ -289,6 +307,15 @@ static int persistent_launch(const void *dA, int64_t n, const MixBins &bins, con
     if (rc) return rc;
     char *base = (char *)cx.scratch[0].ptr;
     PT *dP = (PT *)base;
+    auto kfn = mix_persistent_kernel<Op, T, PT, HT, AT, OT>;
+    const size_t smem = (size_t)kChunk * sizeof(uint32_t) + kTableBytes + (size_t)kMaxU * (kMaxU - 1) / 2 * sizeof(PT);
+    rc = smem_limit_at_least((const void *)kfn, smem);
+    if (rc) return rc;
+    int bps = 0;
+    rc = blocks_per_sm((const void *)kfn, kLevelThreads, smem, &bps);
+    if (rc) return rc;
+    if (bps < 1) return fail(EGG_ERR_CUDA, "the persistent mixed-degree kernel does not fit on an SM");
+    const int64_t nblocks = (int64_t)bps * cx.num_sms;
     // Steps and segments: for each wave, steps t = 1 .. Kmax/2 (level c = 2t of every bin with K >= c).
     MixBins gb = bins;
     for (int k = 0; k < gb.nb; ++k) gb.b[k].lay = 1;  // instance-major pairs
@@ -300,7 +327,7 @@ static int persistent_launch(const void *dA, int64_t n, const MixBins &bins, con
     for (int64_t wv = 0; wv < nwaves; ++wv) {
         for (int t = 1; 2 * t <= Kmax; ++t) {
             const int c = 2 * t;
-            PStep sp{(int)segs.size(), 0, 0};
+            PStep sp{(int)segs.size(), 0, 0, 1};
             for (int k = 0; k < bins.nb; ++k) {
                 const MixBin &bn = bins.b[k];
                 const int64_t inst0 = wv * W;
@@ -324,7 +351,11 @@ static int persistent_launch(const void *dA, int64_t n, const MixBins &bins, con
                 segs.push_back(sg);
                 ++sp.nseg;
             }
-            if (sp.units) steps.push_back(sp);
+            if (sp.units) {
+                sp.grab = sp.units / (nblocks * kClaimsPerBlock);
+                if (sp.grab < 1) sp.grab = 1;
+                steps.push_back(sp);
+            }
         }
     }
     if (steps.size() > (size_t)INT32_MAX / 2) return fail(EGG_ERR_TOO_LARGE, "too many steps for one launch");
@@ -344,14 +375,6 @@ static int persistent_launch(const void *dA, int64_t n, const MixBins &bins, con
     rc = host_flag(&hflag, &hflag_dev);
     if (rc) return rc;
     // One cooperative launch of as many blocks as fit on the device at once.
-    auto kfn = mix_persistent_kernel<Op, T, PT, HT, AT, OT>;
-    const size_t smem = (size_t)kChunk * sizeof(uint32_t) + kTableBytes + (size_t)kMaxU * (kMaxU - 1) / 2 * sizeof(PT);
-    rc = smem_limit_at_least((const void *)kfn, smem);
-    if (rc) return rc;
-    int bps = 0;
-    rc = blocks_per_sm((const void *)kfn, kLevelThreads, smem, &bps);
-    if (rc) return rc;
-    if (bps < 1) return fail(EGG_ERR_CUDA, "the persistent mixed-degree kernel does not fit on an SM");
     PersistArgs a{};
     a.A = dA;
     a.n = n;
@@ -373,7 +396,7 @@ static int persistent_launch(const void *dA, int64_t n, const MixBins &bins, con
     a.ctr = (unsigned *)(tb + off_ctr);
     a.flag = (int *)(tb + off_flag);
     a.host_flag = hflag_dev;
-    a.nblocks = (unsigned)(bps * cx.num_sms);
+    a.nblocks = (unsigned)nblocks;
     a.wait_ns = kBarrierWaitNs;
     void *params[] = {&a};
     const cudaError_t e = cudaLaunchCooperativeKernel((const void *)kfn, dim3(a.nblocks), dim3(kLevelThreads), params, smem, st);
