@@ -270,16 +270,20 @@ int egg_selfcheck_barrier(int extra, int64_t wait_ns, int64_t *passes);
  * timing the candidates on the first batch that had more than one instance of that degree:
  * batched = 1 runs groups of `group` instances instance-fastest (one thread per state and
  * instance); batched = 0 runs `group` single-instance evaluations side by side.  Degrees up to 22
- * always run as one whole-instance launch per batch and are not tuned.  Choices are kept in a JSON
- * file per GPU model and SM count ($EGG_TUNE_CACHE, else $XDG_CACHE_HOME/eggman_b200/mix_tuning.json
- * or ~/.cache/eggman_b200/mix_tuning.json; an empty $EGG_TUNE_CACHE turns the file off), which a
- * process reads before its first batch, so a degree tuned once is not timed again.
- * EGG_ERR_NO_PLAN if K has not been tuned yet.  No counterpart in the reference. */
+ * always run as one whole-instance launch per batch and are not tuned.  A choice is made per size
+ * class of the degree's bin (fewer than 4, 16, 64, 256 instances, or more); this reports a pinned
+ * choice, else the one last tuned in this process, else the file's for the largest class.  Choices
+ * are kept in a JSON file per GPU model and SM count ($EGG_TUNE_CACHE, else
+ * $XDG_CACHE_HOME/eggman_b200/mix_tuning.json or ~/.cache/eggman_b200/mix_tuning.json; an empty
+ * $EGG_TUNE_CACHE turns the file off), which a process reads before its first batch, so a degree
+ * tuned once for a size class is not timed again.  EGG_ERR_NO_PLAN if K has not been tuned yet.
+ * No counterpart in the reference. */
 int egg_dp_mix_tuning(int K, int dtype, int prec, int *batched, int64_t *group);
 
-/* Pin the evaluation of degree K (> 22) for this dtype and mode instead of timing candidates:
- * for callers that tuned offline, and for tests that must cover both evaluations.  Results do
- * not depend on the choice.  No counterpart in the reference. */
+/* Pin the evaluation of degree K (> 22) for this dtype and mode, for batches of every size, instead
+ * of timing candidates: for callers that tuned offline, and for tests that must cover both
+ * evaluations.  Process-local.  Results do not depend on the choice.  No counterpart in the
+ * reference. */
 int egg_dp_mix_set_tuning(int K, int dtype, int prec, int batched, int64_t group);
 
 #ifdef __cplusplus

@@ -17,6 +17,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+# The mixed-degree tuner's file stays out of the test session: tests tune on a few instances,
+# choices a later batch of hundreds should not inherit.  (The test of the file itself sets its own.)
+os.environ.setdefault("EGG_TUNE_CACHE", "")
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built libeggman_b200.so")

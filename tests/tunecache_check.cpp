@@ -39,10 +39,25 @@ int main(int argc, char **argv)
         if (r.same_key(a)) found = r.batched == 1 && r.group == 16;
     CHECK(found);
     CHECK(rs[2].device == "Other GPU" && rs[2].sms == 132);
+    // The same degree tuned on a batch of another size class is another record.
+    egg::TuneRecord a3 = a;
+    a3.size = 4;
+    a3.group = 32;
+    CHECK(egg::tune_merge_file(path, a3));
+    CHECK(egg::tune_read_file(path, rs));
+    CHECK(rs.size() == 4);
+    found = false;
+    for (const auto &r : rs)
+        if (r.same_key(a3)) found = r.group == 32 && r.size == 4;
+    CHECK(found);
     // Malformed text is refused; a missing file reads as empty.
     std::vector<egg::TuneRecord> bad;
     CHECK(!egg::tune_parse("{\"format\": 1, \"entries\": [{\"device\": \"x\", \"K\": 2}]}", bad));
     CHECK(!egg::tune_parse("not json", bad));
+    // A record without "size" (the first format) is refused, so such a file is tuned again.
+    CHECK(!egg::tune_parse("{\"format\": 1, \"entries\": [{\"device\": \"x\", \"sms\": 1, \"K\": 24, "
+                           "\"dtype\": 1, \"prec\": 0, \"batched\": 0, \"group\": 64}]}",
+                           bad));
     CHECK(!egg::tune_read_file(std::string(argv[1]) + "/missing.json", bad) && bad.empty());
     if (fails == 0) std::printf("ok\n");
     return fails ? 1 : 0;

@@ -59,11 +59,23 @@ struct BinExec {
     int64_t group;
 };
 
-// Chosen per (degree, dtype, precision) by timing on first use, kept for the process and in the
-// tuning file (egg_tunecache.h), from which the next process on the same GPU model starts.
-static std::map<std::tuple<int, int, int>, BinExec> g_tuned;
+// Chosen per (degree, dtype, precision, size class of the bin) by timing on first use, kept for the
+// process and in the tuning file (egg_tunecache.h), from which the next process on the same GPU
+// model starts.  The size class keeps a choice timed on a handful of instances (where small groups
+// can win) from deciding a batch of hundreds (where they lose by 2x).  Choices pinned with
+// mix_set_tuning apply to every size; g_last is what egg_dp_mix_tuning reports.
+static std::map<std::tuple<int, int, int, int>, BinExec> g_tuned;
+static std::map<std::tuple<int, int, int>, BinExec> g_pinned, g_last;
 static std::mutex g_tuned_mu;
 static bool g_tuned_loaded = false;
+
+// Size class of a bin of `count` instances: fewer than 4, 16, 64, 256, or more.
+static int size_class(int64_t count)
+{
+    int cls = 0;
+    for (int64_t lim = 4; cls < 4 && count >= lim; lim *= 4) ++cls;
+    return cls;
+}
 
 // This device's identity in the tuning file: its model name and SM count.
 static TuneRecord tune_identity()
@@ -89,13 +101,22 @@ static void tuned_load_once()
     std::vector<TuneRecord> rs;
     if (!tune_read_file(path, rs)) return;
     const TuneRecord me = tune_identity();
-    for (const TuneRecord &r : rs)
-        if (r.device == me.device && r.sms == me.sms && r.group >= 1 && r.K >= 2 && r.K <= 64)
-            g_tuned.emplace(std::make_tuple((int)r.K, (int)r.dtype, (int)r.prec), BinExec{r.batched != 0, r.group});
+    // Per (degree, type, mode) the file's choice for the largest size class is the one reported.
+    std::map<std::tuple<int, int, int>, std::pair<long long, BinExec>> largest;
+    for (const TuneRecord &r : rs) {
+        if (r.device != me.device || r.sms != me.sms || r.group < 1 || r.K < 2 || r.K > 64 || r.size < 0 || r.size > 4)
+            continue;
+        const BinExec ex{r.batched != 0, r.group};
+        g_tuned.emplace(std::make_tuple((int)r.K, (int)r.dtype, (int)r.prec, (int)r.size), ex);
+        const auto k3 = std::make_tuple((int)r.K, (int)r.dtype, (int)r.prec);
+        auto it = largest.find(k3);
+        if (it == largest.end() || r.size > it->second.first) largest[k3] = std::make_pair(r.size, ex);
+    }
+    for (const auto &kv : largest) g_last.emplace(kv.first, kv.second.second);
 }
 
 // Adds one tuned choice to the tuning file (a failure to write only costs a re-tune later).
-static void tuned_save(int K, int dtype, int prec, const BinExec &ex)
+static void tuned_save(int K, int dtype, int prec, int cls, const BinExec &ex)
 {
     const std::string path = tune_cache_path();
     if (path.empty()) return;
@@ -105,6 +126,7 @@ static void tuned_save(int K, int dtype, int prec, const BinExec &ex)
     r.prec = prec;
     r.batched = ex.batched ? 1 : 0;
     r.group = ex.group;
+    r.size = cls;
     tune_merge_file(path, r);
 }
 
@@ -348,13 +370,19 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
         MixBin &bn = bins.b[k];
         BinExec ex{true, bn.count};
         if (bn.K > 22 && bn.count > 1) {
-            const auto key = std::make_tuple(bn.K, dtype, prec);
+            const int cls = size_class(bn.count);
+            const auto key3 = std::make_tuple(bn.K, dtype, prec);
+            const auto key = std::make_tuple(bn.K, dtype, prec, cls);
             bool found = false;
             {
                 std::lock_guard<std::mutex> lk(g_tuned_mu);
                 tuned_load_once();
+                auto ip = g_pinned.find(key3);
                 auto it = g_tuned.find(key);
-                if (it != g_tuned.end()) {
+                if (ip != g_pinned.end()) {
+                    ex = ip->second;
+                    found = true;
+                } else if (it != g_tuned.end()) {
                     ex = it->second;
                     found = true;
                 }
@@ -369,7 +397,8 @@ int mix_run(int dtype, int prec, const void *dA, int64_t n, int64_t B, const int
                 if (rc) return rc;
                 std::lock_guard<std::mutex> lk(g_tuned_mu);
                 g_tuned[key] = ex;
-                tuned_save(bn.K, dtype, prec, ex);
+                g_last[key3] = ex;
+                tuned_save(bn.K, dtype, prec, cls, ex);
             } else if (!found) {
                 ex = dp_grouped_ok(bn.K, dtype, prec) && plans[k]->closed_form() ? BinExec{false, 4} : BinExec{true, bn.count};
             }
@@ -475,7 +504,8 @@ int mix_set_tuning(int K, int dtype, int prec, int batched, int64_t group)
     if (!batched && !dp_grouped_ok(K, dtype, prec))
         return fail(EGG_ERR_ARGUMENT, "no grouped single-instance evaluation for this degree and type");
     std::lock_guard<std::mutex> lk(g_tuned_mu);
-    g_tuned[std::make_tuple(K, dtype, prec)] = BinExec{batched != 0, group};
+    g_pinned[std::make_tuple(K, dtype, prec)] = BinExec{batched != 0, group};
+    g_last[std::make_tuple(K, dtype, prec)] = BinExec{batched != 0, group};
     return EGG_OK;
 }
 
@@ -483,8 +513,8 @@ int mix_tuned(int K, int dtype, int prec, int *batched, int64_t *group)
 {
     std::lock_guard<std::mutex> lk(g_tuned_mu);
     tuned_load_once();
-    auto it = g_tuned.find(std::make_tuple(K, dtype, prec));
-    if (it == g_tuned.end()) return fail(EGG_ERR_NO_PLAN, "degree " + std::to_string(K) + " has not been tuned");
+    auto it = g_last.find(std::make_tuple(K, dtype, prec));
+    if (it == g_last.end()) return fail(EGG_ERR_NO_PLAN, "degree " + std::to_string(K) + " has not been tuned");
     *batched = it->second.batched ? 1 : 0;
     *group = it->second.group;
     return EGG_OK;

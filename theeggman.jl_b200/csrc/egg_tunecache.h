@@ -1,11 +1,12 @@
 // egg_tunecache.h -- the mixed-degree batch tuner's choices, kept in a JSON file across processes.
 //
 // The tuner (egg_mix.cu) times the candidate evaluations of a degree on the first batch that has
-// it.  Its choice depends on the GPU model and SM count, the degree, the element type and the
-// rounding mode, so each record names all of them:
+// it.  Its choice depends on the GPU model and SM count, the degree, the element type, the
+// rounding mode and how many instances of the degree the batch holds (a class: `size` 0..4 for
+// fewer than 4, 16, 64, 256 instances, or more), so each record names all of them:
 //
-//   {"format": 1, "entries": [
-//     {"device": "NVIDIA B200", "sms": 148, "K": 24, "dtype": 1, "prec": 0, "batched": 0, "group": 64},
+//   {"format": 2, "entries": [
+//     {"device": "NVIDIA B200", "sms": 148, "K": 24, "dtype": 1, "prec": 0, "size": 4, "batched": 0, "group": 64},
 //     ...]}
 //
 // A process reads the file once, on its first mixed-degree batch, and takes the records of its
@@ -26,10 +27,10 @@ namespace egg {
 
 struct TuneRecord {
     std::string device;
-    long long sms = 0, K = 0, dtype = 0, prec = 0, batched = 0, group = 0;
+    long long sms = 0, K = 0, dtype = 0, prec = 0, batched = 0, group = 0, size = 0;
     bool same_key(const TuneRecord &o) const
     {
-        return device == o.device && sms == o.sms && K == o.K && dtype == o.dtype && prec == o.prec;
+        return device == o.device && sms == o.sms && K == o.K && dtype == o.dtype && prec == o.prec && size == o.size;
     }
 };
 
@@ -77,10 +78,11 @@ inline bool tune_parse(const std::string &s, std::vector<TuneRecord> &out)
                 else if (key == "prec") { r.prec = x; seen |= 16; }
                 else if (key == "batched") { r.batched = x; seen |= 32; }
                 else if (key == "group") { r.group = x; seen |= 64; }
+                else if (key == "size") { r.size = x; seen |= 128; }
                 q = (size_t)(end - obj.c_str());
             }
         }
-        if (seen != 127) return false;
+        if (seen != 255) return false;  // every field, "size" included (format 1 files are re-tuned)
         out.push_back(r);
         p = cb;
     }
@@ -88,7 +90,7 @@ inline bool tune_parse(const std::string &s, std::vector<TuneRecord> &out)
 
 inline std::string tune_format(const std::vector<TuneRecord> &rs)
 {
-    std::string s = "{\"format\": 1, \"entries\": [";
+    std::string s = "{\"format\": 2, \"entries\": [";
     for (size_t i = 0; i < rs.size(); ++i) {
         const TuneRecord &r = rs[i];
         std::string dev;
@@ -97,6 +99,7 @@ inline std::string tune_format(const std::vector<TuneRecord> &rs)
         s += i ? ",\n  " : "\n  ";
         s += "{\"device\": \"" + dev + "\", \"sms\": " + std::to_string(r.sms) + ", \"K\": " + std::to_string(r.K) +
              ", \"dtype\": " + std::to_string(r.dtype) + ", \"prec\": " + std::to_string(r.prec) +
+             ", \"size\": " + std::to_string(r.size) +
              ", \"batched\": " + std::to_string(r.batched) + ", \"group\": " + std::to_string(r.group) + "}";
     }
     s += "\n]}\n";
