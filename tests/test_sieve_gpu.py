@@ -290,6 +290,43 @@ def test_reference_order_bit_identical(egg, orc, W, cplx, glynn):
 
 
 @pytest.mark.parametrize("cplx", [False, True])
+def test_reference_order_pivot_edge_cases(egg, orc, cplx):
+    """Matrices of small integers (entries -2..2, a third of them zero): the Hessenberg pivots meet
+    exact ties of magnitude (the first row of largest |entry| wins, src/hafnian.jl:212-221) and zero
+    columns (the step is skipped, :231-232) at every size, on the register tiles (m <= 32) and the
+    shared-memory kernel (m > 32, N = 34); the reference order must still be matched to the bit.
+    Then a NaN and an infinity among the entries: the result is NaN exactly when the reference's
+    is, and otherwise equal."""
+    rng = np.random.default_rng(4242 + cplx)
+
+    def draw(N):
+        v = rng.choice([-2, -1, 0, 0, 1, 2], size=(N, N)).astype(float)
+        if cplx:
+            v = v + 1j * rng.choice([-1, 0, 0, 1], size=(N, N))
+        return np.triu(v) + np.triu(v, 1).T
+
+    for N in (6, 12, 20, 26, 34):
+        for _ in range(2):
+            A = draw(N)
+            E = N // 2
+            Ax = orc.permuted(A, distinct_x(E))
+            for glynn in (False, True):
+                want = orc.calc_hafnian(Ax, [1] * E, glynn, nthreads=1, sum_mode=0)
+                got = egg.sieve(Ax, [1] * E, glynn=glynn, prec="reference", nthreads=1)
+                assert complex(got) == complex(want), (N, glynn, got, want)
+    for bad in (float("nan"), float("inf")):
+        A = draw(12)
+        A[3, 7] = A[7, 3] = bad
+        Ax = orc.permuted(A, distinct_x(6))
+        for glynn in (False, True):
+            want = complex(orc.calc_hafnian(Ax, [1] * 6, glynn, nthreads=1, sum_mode=0))
+            got = complex(egg.sieve(Ax, [1] * 6, glynn=glynn, prec="reference", nthreads=1))
+            assert np.isnan(got) == np.isnan(want), (bad, glynn, got, want)
+            if not np.isnan(want):
+                assert got == want, (bad, glynn, got, want)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
 def test_reference_order_repeated_rows(egg, orc, W, cplx):
     """hafnian_repeated's mixed-radix odometer, both variants, through the public entry point."""
     A = W.dense_complex(10, 91, 0.5) if cplx else W.dense_real(10, 91)

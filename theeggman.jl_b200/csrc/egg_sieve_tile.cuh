@@ -156,13 +156,12 @@ __device__ __forceinline__ void step_real(TileCtx<MW, G, EXACT> &c)
     int plab, pl;
     if constexpr (EXACT) {
         // The first (lowest label) row achieving the maximum; if row K's own entry is NaN the
-        // reference keeps it (no comparison with NaN succeeds, :212-218).
+        // reference keeps it (no comparison with NaN succeeds, :212-218), so that row's key is the
+        // largest there is, while any other NaN row's key is 0.
         const double v = R[K - 1];
-        if (__any_sync(c.gm, lab == K && v != v)) {
-            plab = K;
-            pl = -1;
-        } else {
-            const unsigned long long key = cand ? abs_key(v) : 0ull;
+        {
+            unsigned long long key = cand ? abs_key(v) : 0ull;
+            if (lab == K && v != v) key = ~0ull;
             const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
             const unsigned mhi = __reduce_max_sync(c.gm, hi);
             const unsigned mlo = __reduce_max_sync(c.gm, hi == mhi ? lo : 0u);
@@ -453,11 +452,9 @@ __device__ __forceinline__ void step_cplx(CTileCtx<MW, G> &c)
     // -- pivot: the first row of largest squared modulus (:277-286); NaN as in the real form
     const double a = __dadd_rn(__dmul_rn(Rr[K - 1], Rr[K - 1]), __dmul_rn(Ri[K - 1], Ri[K - 1]));
     int plab, pl;
-    if (__any_sync(c.gm, lab == K && a != a)) {
-        plab = K;
-        pl = -1;
-    } else {
-        const unsigned long long key = cand ? abs_key(a) : 0ull;
+    {
+        unsigned long long key = cand ? abs_key(a) : 0ull;
+        if (lab == K && a != a) key = ~0ull;  // row K's NaN keeps row K, as in the real form
         const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
         const unsigned mhi = __reduce_max_sync(c.gm, hi);
         const unsigned mlo = __reduce_max_sync(c.gm, hi == mhi ? lo : 0u);
