@@ -166,18 +166,11 @@ __device__ __forceinline__ void step_real(TileCtx<MW, G, EXACT> &c)
             const unsigned mhi = __reduce_max_sync(c.gm, hi);
             const unsigned mlo = __reduce_max_sync(c.gm, hi == mhi ? lo : 0u);
             const bool win = key != 0ull && hi == mhi && lo == mlo;
-            const unsigned wb = __ballot_sync(c.gm, win);
-            if (__popc(wb) == 1) {
-                // One row holds the maximum (the usual case): it is the pivot.
-                pl = __ffs((int)wb) - 1;
-                if (G < 32) pl &= G - 1;
-                plab = __shfl_sync(c.gm, lab, pl, G);
-            } else {
-                // Ties (or every candidate NaN): the lowest label among the maxima.
-                plab = (int)__reduce_min_sync(c.gm, win ? (unsigned)lab : 0x7fffffffu);
-                if (plab == 0x7fffffff) plab = K;
-                pl = -1;
-            }
+            // The lowest label among the maxima (one reduction serves the usual single maximum and
+            // exact ties alike; the lane is found from the label below).
+            plab = (int)__reduce_min_sync(c.gm, win ? (unsigned)lab : 0x7fffffffu);
+            if (plab == 0x7fffffff) plab = K;
+            pl = -1;
         }
     } else {
         const unsigned key = cand ? pivot_key(fabs(R[K - 1]), c.lane) : 0u;
@@ -459,21 +452,11 @@ __device__ __forceinline__ void step_cplx(CTileCtx<MW, G> &c)
         const unsigned mhi = __reduce_max_sync(c.gm, hi);
         const unsigned mlo = __reduce_max_sync(c.gm, hi == mhi ? lo : 0u);
         const bool win = key != 0ull && hi == mhi && lo == mlo;
-        const unsigned wb = __ballot_sync(c.gm, win);
-        if (__popc(wb) == 1) {
-            pl = __ffs((int)wb) - 1;
-            if (G < 32) pl &= G - 1;
-            plab = __shfl_sync(c.gm, lab, pl, G);
-        } else {
-            plab = (int)__reduce_min_sync(c.gm, win ? (unsigned)lab : 0x7fffffffu);
-            if (plab == 0x7fffffff) plab = K;
-            pl = -1;
-        }
+        plab = (int)__reduce_min_sync(c.gm, win ? (unsigned)lab : 0x7fffffffu);  // lowest label among the maxima
+        if (plab == 0x7fffffff) plab = K;
     }
-    if (pl < 0) {
-        pl = __ffs((int)__ballot_sync(c.gm, lab == plab)) - 1;
-        if (G < 32) pl &= G - 1;
-    }
+    pl = __ffs((int)__ballot_sync(c.gm, lab == plab)) - 1;
+    if (G < 32) pl &= G - 1;
     const double xr = __shfl_sync(c.gm, Rr[K - 1], pl, G), xi = __shfl_sync(c.gm, Ri[K - 1], pl, G);
     // -- swap rows (relabel) and columns (move)
     if (lab == K) lab = plab;
