@@ -8,6 +8,8 @@
 // Included by the egg_dp_fixed_*.cu files, which instantiate fixed_level per type.
 #pragma once
 
+#include <type_traits>
+
 #include "egg_dp_common.cuh"
 
 namespace egg {
@@ -75,8 +77,21 @@ __device__ __forceinline__ AT walk_fixed(M m, const uint2 *__restrict__ TP, int 
 // one state per thread and step), with walk_fixed<C>.  blockIdx.y selects one of several
 // independent instances stored instance-major: pairs at P + y * ldp, the level read at
 // Hprev + y * ldhp and the level written at Hcur + y * ldhc.
+// Blocks of kLevelThreads per SM the level kernel is compiled for.  The child gathers are latency
+// bound (long-scoreboard stalls dominate), so more resident warps help, as long as the walk's
+// registers still fit: 4 blocks (64 registers) through c = 14, 3 (80) through c = 24, 2 (128)
+// through c = 38.  Int128 states, and the 64-bit-mask levels from c = 40, spill under those caps and
+// keep the compiler's own allocation.  Measured on the 4096 mix 45.5 -> 42.9 ms, N = 40 FP64
+// 3.46 -> 3.33 ms, N = 36 complex 0.83 -> 0.79 ms.
+template <int C, class HT>
+constexpr int fixed_min_blocks()
+{
+    if (std::is_same<HT, __int128>::value) return 1;
+    return C <= 14 ? 4 : (C <= 24 ? 3 : (C <= 38 ? 2 : 1));
+}
+
 template <int C, class Op, class M, class PT, class HT, class AT>
-__global__ void __launch_bounds__(kLevelThreads) dpc_fixed_kernel(const uint32_t *__restrict__ binom, const PT *__restrict__ P,
+__global__ void __launch_bounds__(kLevelThreads, (fixed_min_blocks<C, HT>())) dpc_fixed_kernel(const uint32_t *__restrict__ binom, const PT *__restrict__ P,
                                                                   const HT *__restrict__ Hprev, HT *__restrict__ Hcur, int K,
                                                                   int64_t n, int run, int64_t ldp, int64_t ldhp, int64_t ldhc)
 {
