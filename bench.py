@@ -72,7 +72,7 @@ def rel_err(a, b) -> float:
 PROFILE_OF = {"sieve40": "sieve_level_kernel_exact_sieve40.md", "sieve40f": "sieve_level_kernel_sieve40.md",
               "sieve40cf": "sieve_level_kernel_sieve40c.md", "sieve40gf": "sieve_level_kernel_sieve40g.md",
               "rep14f": "sieve_level_kernel_rep14.md", "dp40": "dpc_fixed_kernel_dp40.md",
-              "dp20": "dpc_cluster_kernel_dp20.md"}
+              "dp20": "dpc_cluster_kernel_dp20.md", "mix4096": "dpc_fixed_kernel_mix4096.md"}
 
 
 def profile_traffic(name: str):
