@@ -19,7 +19,8 @@
 // (ld_ca), the pairs and the results through L2 only; never through the read-only path.
 //
 // Measured on the 4096-instance configuration-4 mix (ComplexF64, degrees 8..32, one B200): this
-// engine 50.4 ms a batch, the per-level engine (tuned groups, graph replay) 45.3 ms, so the
+// engine 50.4 ms a batch, the per-level engine (tuned groups, graph replay) 45.3 ms at the time and
+// 39.1 ms since its level kernels got per-popcount block counts and one block per chunk, so the
 // per-level engine is the default.  The level kernels there are compiled per popcount, each with
 // the registers its walk needs; one kernel serving every popcount carries the largest walk's
 // registers (or spills them at three blocks per SM), and that is most of the difference.
