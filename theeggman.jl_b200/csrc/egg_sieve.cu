@@ -749,7 +749,8 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         const int k = inst[0].E;
         const bool narrow = 2 * k <= 16;
         int cw = 0, bps = 0;
-        int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, exact, &cw, &bps) : level_shape_real(nmax, k, narrow, exact, &cw, &bps);
+        int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, exact, true, &cw, &bps)
+                       : level_shape_real(nmax, k, narrow, exact, true, &cw, &bps);
         if (rc0) return rc0;
         if (bps < 1) return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
         const int64_t terms_all = ((int64_t)1 << k) - 1, per_block = (int64_t)cw * (narrow ? 2 : 1);
@@ -785,7 +786,8 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             if (lvl[(size_t)k] <= 0.0) continue;
             const bool narrow = 2 * k <= 16 && e_odo <= 16;
             int cw = 0, bps = 0;
-            int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, exact, &cw, &bps) : level_shape_real(nmax, k, narrow, exact, &cw, &bps);
+            int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, exact, false, &cw, &bps)
+                           : level_shape_real(nmax, k, narrow, exact, false, &cw, &bps);
             if (rc0) return rc0;
             if (bps < 1 || (size_t)cw * (narrow ? 2 : 1) * level_ws_bytes(nmax, cplx, k, exact) > 220 * 1024)
                 return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");

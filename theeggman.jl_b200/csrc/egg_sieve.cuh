@@ -64,8 +64,8 @@ int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, bool exact, dd
 int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, bool exact, dd *partial,
                       int blocks_x, cudaStream_t st);
 // The level's block size in warps and how many of its blocks one SM holds.
-int level_shape_real(int nmax, int k, bool narrow, bool exact, int *warps_per_block, int *blocks_per_sm);
+int level_shape_real(int nmax, int k, bool narrow, bool exact, bool all, int *warps_per_block, int *blocks_per_sm);
 int level_shape_real_hi(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm);
-int level_shape_cplx(int nmax, int k, bool narrow, bool exact, int *warps_per_block, int *blocks_per_sm);
+int level_shape_cplx(int nmax, int k, bool narrow, bool exact, bool all, int *warps_per_block, int *blocks_per_sm);
 
 }  // namespace egg

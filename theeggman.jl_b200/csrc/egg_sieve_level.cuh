@@ -25,16 +25,23 @@ namespace egg {
 // registers per thread): a real tile holds m doubles per row, a complex one 2m.
 // The reference-arithmetic tiles keep more values live per step (separately rounded products, the
 // buffered term series), so from 24 rows on they take one block fewer.
-template <bool CPLX, int K, int G = 32, bool EXACT = false>
+template <bool CPLX, int K, int G = 32, bool EXACT = false, bool ALL = false>
 struct LevelShape {
     static constexpr int MW = 2 * K;
-    static constexpr int threads = 128;
     static constexpr int full =
         CPLX ? (MW <= 8 ? 6 : (MW <= 10 ? 5 : (MW <= 16 ? 4 : (MW <= 24 ? 3 : 2))))
              : (MW <= 8 ? 8 : (MW <= 12 ? 7 : (MW <= 18 ? 6 : (MW <= (EXACT ? 22 : 26) ? 5 : (MW <= 32 ? 4 : 2)))));
     // Two terms per warp need more registers per thread (the series holds two coefficients per
     // lane); one block fewer still keeps more terms in flight.
-    static constexpr int min_blocks = G == 32 ? full : (full > 2 ? full - 1 : 1);
+    static constexpr int per_sm = G == 32 ? full : (full > 2 ? full - 1 : 1);
+    // Lockstep: the reference-arithmetic real tiles of 17..32 rows run as ONE block per SM holding
+    // all of its warps, which take their terms in rounds separated by a block barrier.  Each term
+    // runs about 5 k instructions of straight-line code (every Hessenberg step is its own code), and
+    // warps spread over different parts of it stall on instruction fetch; in lockstep the warps of
+    // an SM run the same part at the same time.  The N = 40 sieve took 10.52 -> 9.67 ms.
+    static constexpr bool lockstep = !ALL && EXACT && !CPLX && G == 32 && MW > 16 && MW <= 32;
+    static constexpr int threads = lockstep ? 128 * per_sm : 128;
+    static constexpr int min_blocks = lockstep ? 1 : per_sm;
 };
 
 // Lanes per term: tiles of up to 16 rows (m <= 16) run two terms per warp, one per half-warp group
@@ -77,15 +84,15 @@ __device__ __forceinline__ dd group_tree_sum(dd v, unsigned gm, int G)
 // series are evaluated in batches of G terms, one term per lane, and with a.terms set each term's
 // signed value is written at its index instead of being summed.
 template <bool CPLX, int K, int G, bool ALL = false, bool EXACT = false>
-__global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT>::threads, LevelShape<CPLX, K, G, EXACT>::min_blocks)
+__global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT, ALL>::threads, LevelShape<CPLX, K, G, EXACT, ALL>::min_blocks)
     sieve_level_kernel(SieveArgs a, const int64_t *__restrict__ strides, dd *partial)
 {
     constexpr int MW = 2 * K;
     constexpr bool TILE = level_tile<CPLX, K, EXACT>();
     static_assert(!EXACT || TILE, "the exact form runs on the logical-order tiles");
-    constexpr int cw = LevelShape<CPLX, K>::threads / 32;
     constexpr int NG = 32 / G;   // groups per warp
-    constexpr int GB = cw * NG;  // groups per block
+    constexpr int GB_MAX = LevelShape<CPLX, K, G, EXACT, ALL>::threads / 32 * NG;
+    const int GB = (int)(blockDim.x >> 5) * NG;  // groups per block (a lockstep block may hold fewer warps)
     extern __shared__ double smem[];
     const int grp = threadIdx.x / G, gl = threadIdx.x & (G - 1);
     const int gbase = (threadIdx.x & 31) & ~(G - 1);  // the group's first lane within its warp
@@ -352,7 +359,11 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT>::threads, LevelS
                 if (hit) break;
             }
         }
-        if (!__any_sync(FULL, has)) break;
+        if constexpr (LevelShape<CPLX, K, G, EXACT, ALL>::lockstep) {
+            if (!__syncthreads_or(has)) break;  // the block's warps take their terms in rounds
+        } else {
+            if (!__any_sync(FULL, has)) break;
+        }
         if (has) {
             __syncwarp(gm);
             eval_term(prefac, mE, jidx);
@@ -361,7 +372,7 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT>::threads, LevelS
     }
     flush();
     // The block's groups summed in a fixed order: one partial per block.
-    __shared__ dd red[2 * GB];
+    __shared__ dd red[2 * GB_MAX];
     if (gl == 0) {
         red[2 * grp] = acc_re;
         red[2 * grp + 1] = acc_im;
@@ -430,10 +441,27 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT>::threads, LevelS
     }
 }
 
+// Warps per block of a level kernel: the shape's, except that a lockstep block takes only as many
+// warps as their workspaces fit in shared memory (the buffered series grow with N: 20 warps of the
+// 22-row tile fit up to N = 42, 15 at N = 62).
+template <bool CPLX, int K, int G, bool EXACT, bool ALL>
+inline int level_warps(int nmax)
+{
+    using S = LevelShape<CPLX, K, G, EXACT, ALL>;
+    constexpr int cw_max = S::threads / 32;
+    if constexpr (!S::lockstep) {
+        return cw_max;
+    } else {
+        const size_t per_warp = (size_t)(32 / G) * level_ws_doubles<CPLX, K, EXACT>(nmax) * sizeof(double);
+        const int fit = (int)((size_t)(218 * 1024) / per_warp);
+        return fit < 1 ? 1 : (fit < cw_max ? fit : cw_max);
+    }
+}
+
 template <bool CPLX, int K, int G, bool EXACT = false>
 static int level_launch_k(const SieveArgs &a, const int64_t *strides, int B, dd *partial, int blocks_x, cudaStream_t st)
 {
-    constexpr int cw = LevelShape<CPLX, K>::threads / 32;
+    const int cw = level_warps<CPLX, K, G, EXACT, false>(a.nmax);
     const size_t smem = (size_t)cw * (32 / G) * level_ws_doubles<CPLX, K, EXACT>(a.nmax) * sizeof(double);
     auto k = sieve_level_kernel<CPLX, K, G, false, EXACT>;
     int rc = smem_limit_at_least((const void *)k, smem);
@@ -447,7 +475,7 @@ static int level_launch_k(const SieveArgs &a, const int64_t *strides, int B, dd 
 template <bool CPLX, int K, int G, bool EXACT = false>
 static int level_launch_all_k(const SieveArgs &a, dd *partial, int blocks_x, cudaStream_t st)
 {
-    constexpr int cw = LevelShape<CPLX, K>::threads / 32;
+    const int cw = level_warps<CPLX, K, G, EXACT, true>(a.nmax);
     const size_t smem = (size_t)cw * (32 / G) * level_ws_doubles<CPLX, K, EXACT>(a.nmax) * sizeof(double);
     auto k = sieve_level_kernel<CPLX, K, G, true, EXACT>;
     int rc = smem_limit_at_least((const void *)k, smem);
@@ -458,12 +486,12 @@ static int level_launch_all_k(const SieveArgs &a, dd *partial, int blocks_x, cud
     return EGG_OK;
 }
 
-template <bool CPLX, int K, int G, bool EXACT = false>
+template <bool CPLX, int K, int G, bool EXACT = false, bool ALL = false>
 static int level_shape_k(int nmax, int *warps_per_block, int *blocks_per_sm)
 {
-    constexpr int cw = LevelShape<CPLX, K>::threads / 32;
+    const int cw = level_warps<CPLX, K, G, EXACT, ALL>(nmax);
     const size_t smem = (size_t)cw * (32 / G) * level_ws_doubles<CPLX, K, EXACT>(nmax) * sizeof(double);
-    auto k = sieve_level_kernel<CPLX, K, G, false, EXACT>;
+    auto k = sieve_level_kernel<CPLX, K, G, ALL, EXACT>;
     int nb = 0;
     int rc = smem_limit_at_least((const void *)k, smem);
     if (!rc) rc = egg::blocks_per_sm((const void *)k, cw * 32, smem, &nb);
@@ -484,6 +512,12 @@ static int level_shape_k(int nmax, int *warps_per_block, int *blocks_per_sm)
     case K:                                                                                          \
         return narrow ? level_launch_all_k<CPLX, K, level_group<K>(true), EXACT>(a, partial, blocks_x, st)  \
                       : level_launch_all_k<CPLX, K, 32, EXACT>(a, partial, blocks_x, st);
+// Case K of a switch over the all-levels launches' shapes.
+#define EGG_ALL_SHAPE(CPLX, K)                                                                         \
+    case K:                                                                                            \
+        rc = narrow ? level_shape_k<CPLX, K, level_group<K>(true), EXACT, true>(nmax, warps_per_block, blocks_per_sm) \
+                    : level_shape_k<CPLX, K, 32, EXACT, true>(nmax, warps_per_block, blocks_per_sm);   \
+        break;
 #define EGG_FUSED_CASES(CPLX, X)                                                                    \
     X(CPLX, 1) X(CPLX, 2) X(CPLX, 3) X(CPLX, 4) X(CPLX, 5) X(CPLX, 6) X(CPLX, 7) X(CPLX, 8) X(CPLX, 9) \
     X(CPLX, 10)

@@ -7,10 +7,10 @@ namespace egg {
 
 template int level_launch_cplx_lo<false>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
 template int level_launch_all_cplx_lo<false>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
-template int level_shape_cplx_lo<false>(int, int, bool, int *, int *);
+template int level_shape_cplx_lo<false>(int, int, bool, bool, int *, int *);
 extern template int level_launch_cplx_lo<true>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
 extern template int level_launch_all_cplx_lo<true>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
-extern template int level_shape_cplx_lo<true>(int, int, bool, int *, int *);
+extern template int level_shape_cplx_lo<true>(int, int, bool, bool, int *, int *);
 
 int level_launch_cplx(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, bool exact, dd *partial,
                       int blocks_x, cudaStream_t st)
@@ -25,10 +25,10 @@ int level_launch_all_cplx(const SieveArgs &a, int k, bool narrow, bool exact, dd
                  : level_launch_all_cplx_lo<false>(a, k, narrow, partial, blocks_x, st);
 }
 
-int level_shape_cplx(int nmax, int k, bool narrow, bool exact, int *warps_per_block, int *blocks_per_sm)
+int level_shape_cplx(int nmax, int k, bool narrow, bool exact, bool all, int *warps_per_block, int *blocks_per_sm)
 {
-    return exact ? level_shape_cplx_lo<true>(nmax, k, narrow, warps_per_block, blocks_per_sm)
-                 : level_shape_cplx_lo<false>(nmax, k, narrow, warps_per_block, blocks_per_sm);
+    return exact ? level_shape_cplx_lo<true>(nmax, k, narrow, all, warps_per_block, blocks_per_sm)
+                 : level_shape_cplx_lo<false>(nmax, k, narrow, all, warps_per_block, blocks_per_sm);
 }
 
 }  // namespace egg

@@ -6,6 +6,6 @@ namespace egg {
 
 template int level_launch_cplx_lo<true>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
 template int level_launch_all_cplx_lo<true>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
-template int level_shape_cplx_lo<true>(int, int, bool, int *, int *);
+template int level_shape_cplx_lo<true>(int, int, bool, bool, int *, int *);
 
 }  // namespace egg

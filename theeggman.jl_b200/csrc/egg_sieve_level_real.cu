@@ -15,10 +15,10 @@ size_t level_ws_bytes(int nmax, int cplx, int k, bool exact)
 
 template int level_launch_real_lo<false>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
 template int level_launch_all_real_lo<false>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
-template int level_shape_real_lo<false>(int, int, bool, int *, int *);
+template int level_shape_real_lo<false>(int, int, bool, bool, int *, int *);
 extern template int level_launch_real_lo<true>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
 extern template int level_launch_all_real_lo<true>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
-extern template int level_shape_real_lo<true>(int, int, bool, int *, int *);
+extern template int level_shape_real_lo<true>(int, int, bool, bool, int *, int *);
 
 int level_launch_real(const SieveArgs &a, const int64_t *strides, int B, int k, bool narrow, bool exact, dd *partial,
                       int blocks_x, cudaStream_t st)
@@ -37,14 +37,14 @@ int level_launch_all_real(const SieveArgs &a, int k, bool narrow, bool exact, dd
                  : level_launch_all_real_lo<false>(a, k, narrow, partial, blocks_x, st);
 }
 
-int level_shape_real(int nmax, int k, bool narrow, bool exact, int *warps_per_block, int *blocks_per_sm)
+int level_shape_real(int nmax, int k, bool narrow, bool exact, bool all, int *warps_per_block, int *blocks_per_sm)
 {
     if (k > 16) {
         if (exact) return fail(EGG_ERR_ARGUMENT, "the reference-arithmetic tiles hold up to 32 rows");
         return level_shape_real_hi(nmax, k, narrow, warps_per_block, blocks_per_sm);
     }
-    return exact ? level_shape_real_lo<true>(nmax, k, narrow, warps_per_block, blocks_per_sm)
-                 : level_shape_real_lo<false>(nmax, k, narrow, warps_per_block, blocks_per_sm);
+    return exact ? level_shape_real_lo<true>(nmax, k, narrow, all, warps_per_block, blocks_per_sm)
+                 : level_shape_real_lo<false>(nmax, k, narrow, all, warps_per_block, blocks_per_sm);
 }
 
 }  // namespace egg

@@ -41,21 +41,28 @@ int level_launch_all_real_lo(const SieveArgs &a, int k, bool narrow, dd *partial
 }
 
 template <bool EXACT>
-int level_shape_real_lo(int nmax, int k, bool narrow, int *warps_per_block, int *blocks_per_sm)
+int level_shape_real_lo(int nmax, int k, bool narrow, bool all, int *warps_per_block, int *blocks_per_sm)
 {
     static std::mutex mu;  // the entry point that allocates nothing reaches this without the library's lock
     std::lock_guard<std::mutex> lk(mu);
-    // Occupancy figures, the same on every device of one model.
-    static int cache[16 + 1][2][2];
-    int *slot = (k >= 1 && k <= 16) ? cache[k][narrow ? 1 : 0] : nullptr;
+    // Occupancy figures, the same on every device of one model; they depend on the largest term
+    // size n (the workspaces' buffered series), hence nmax in the key.
+    static int cache[16 + 1][2][2][33][2];
+    int *slot = (k >= 1 && k <= 16 && nmax >= 0 && nmax <= 32) ? cache[k][narrow ? 1 : 0][all ? 1 : 0][nmax] : nullptr;
     if (slot && slot[1] > 0) {
         *warps_per_block = slot[0];
         *blocks_per_sm = slot[1];
         return EGG_OK;
     }
-    int rc = fail(EGG_ERR_ARGUMENT, "no such sieve level");
-    switch (k) {
-        EGG_LEVEL_CASES(false, EGG_LVLR_SHAPE)
+    int rc = fail(EGG_ERR_ARGUMENT, all ? "no all-levels sieve launch for this edge count" : "no such sieve level");
+    if (all) {
+        switch (k) {
+            EGG_FUSED_CASES(false, EGG_ALL_SHAPE)
+        }
+    } else {
+        switch (k) {
+            EGG_LEVEL_CASES(false, EGG_LVLR_SHAPE)
+        }
     }
     if (rc) return rc;
     if (slot) {

@@ -6,6 +6,6 @@ namespace egg {
 
 template int level_launch_real_lo<true>(const SieveArgs &, const int64_t *, int, int, bool, dd *, int, cudaStream_t);
 template int level_launch_all_real_lo<true>(const SieveArgs &, int, bool, dd *, int, cudaStream_t);
-template int level_shape_real_lo<true>(int, int, bool, int *, int *);
+template int level_shape_real_lo<true>(int, int, bool, bool, int *, int *);
 
 }  // namespace egg
