@@ -78,8 +78,13 @@ __device__ __forceinline__ int warp_first_argmax(double a, int i)
     return __shfl_sync(0xffffffffu, i, 0);
 }
 
-// _hessenberg!(M, m, mult), src/hafnian.jl:210-258, one warp, exact order.
-__device__ void hessenberg_real_exact(WarpWs &w, int m, int lane)
+// _hessenberg!(M, m, mult), src/hafnian.jl:210-258, one warp, exact order, m <= 32 * NP.
+// Each lane keeps its rows' multipliers (rows k+1+lane+32p) and its column-update sums (rows
+// lane+32p) in registers, so that every element's chain of separately rounded operations runs in
+// registers, in the reference's order, instead of through shared memory; the row update's skip of
+// a zero M[k, j] is a select (the same value), so that four columns' loads overlap.
+template <int NP>
+__device__ void hessenberg_real_exact_np(WarpWs &w, int m, int lane)
 {
     double *M = w.M;
     const int ld = w.ldm;
@@ -117,29 +122,90 @@ __device__ void hessenberg_real_exact(WarpWs &w, int m, int lane)
         }
         const double x = MX(k, col);
         if (x == 0.0) continue;
-        for (int i = k + 1 + lane; i < m; i += 32) {
-            w.u[i] = __ddiv_rn(MX(i, col), x);
-            MX(i, col) = 0.0;
+        double ui[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const int i = k + 1 + lane + 32 * p;
+            ui[p] = 0.0;
+            if (i < m) {
+                ui[p] = __ddiv_rn(MX(i, col), x);
+                w.u[i] = ui[p];
+                MX(i, col) = 0.0;
+            }
         }
         __syncwarp();
-        for (int j = k; j < m; ++j) {
+        // Rows k+1.. minus u[i] * M[k, j], for j = k..m-1; a zero M[k, j] leaves its column as it is.
+        int j = k;
+        for (; j + 4 <= m; j += 4) {
+            double a4[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a4[q] = MX(k, j + q);
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const int i = k + 1 + lane + 32 * p;
+                if (i < m) {
+                    double v[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) v[q] = MX(i, j + q);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        MX(i, j + q) = a4[q] == 0.0 ? v[q] : __dsub_rn(v[q], __dmul_rn(ui[p], a4[q]));
+                }
+            }
+        }
+        for (; j < m; ++j) {
             const double akj = MX(k, j);
-            if (akj == 0.0) continue;
-            for (int i = k + 1 + lane; i < m; i += 32) MX(i, j) = __dsub_rn(MX(i, j), __dmul_rn(w.u[i], akj));
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const int i = k + 1 + lane + 32 * p;
+                if (i < m) {
+                    const double v = MX(i, j);
+                    MX(i, j) = akj == 0.0 ? v : __dsub_rn(v, __dmul_rn(ui[p], akj));
+                }
+            }
         }
         __syncwarp();
+        // Column k plus u[i] * column i for i = k+1..m-1 in order; a zero u[i] adds nothing.
+        double acc[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const int l = lane + 32 * p;
+            acc[p] = l < m ? MX(l, k) : 0.0;
+        }
+#pragma unroll 4
         for (int i = k + 1; i < m; ++i) {
             const double mi = w.u[i];
-            if (mi == 0.0) continue;
-            for (int l = lane; l < m; l += 32) MX(l, k) = __dadd_rn(MX(l, k), __dmul_rn(mi, MX(l, i)));
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const int l = lane + 32 * p;
+                if (l < m) {
+                    const double s = __dadd_rn(acc[p], __dmul_rn(mi, MX(l, i)));
+                    acc[p] = mi == 0.0 ? acc[p] : s;
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const int l = lane + 32 * p;
+            if (l < m) MX(l, k) = acc[p];
         }
         __syncwarp();
     }
 #undef MX
 }
 
-// _hessenberg_split!(Mr, Mi, m, ur, ui), src/hafnian.jl:271-335, one warp, exact order.
-__device__ void hessenberg_split_exact(WarpWs &w, int m, int lane)
+__device__ void hessenberg_real_exact(WarpWs &w, int m, int lane)
+{
+    if (m <= 32) hessenberg_real_exact_np<1>(w, m, lane);
+    else if (m <= 64) hessenberg_real_exact_np<2>(w, m, lane);
+    else if (m <= 96) hessenberg_real_exact_np<3>(w, m, lane);
+    else hessenberg_real_exact_np<4>(w, m, lane);
+}
+
+// _hessenberg_split!(Mr, Mi, m, ur, ui), src/hafnian.jl:271-335, one warp, exact order, m <= 32 * NP;
+// multipliers and column-update sums in registers as in the real form.
+template <int NP>
+__device__ void hessenberg_split_exact_np(WarpWs &w, int m, int lane)
 {
     double *R = w.M, *I = w.Mi;
     const int ld = w.ldm;
@@ -177,29 +243,63 @@ __device__ void hessenberg_split_exact(WarpWs &w, int m, int lane)
         const double xr = RX(k, col), xi = IX(k, col);
         const double d = __dadd_rn(__dmul_rn(xr, xr), __dmul_rn(xi, xi));
         if (d == 0.0) continue;
-        for (int i = k + 1 + lane; i < m; i += 32) {
-            const double ar = RX(i, col), ai = IX(i, col);
-            w.u[i] = __ddiv_rn(__dadd_rn(__dmul_rn(ar, xr), __dmul_rn(ai, xi)), d);
-            w.ui[i] = __ddiv_rn(__dsub_rn(__dmul_rn(ai, xr), __dmul_rn(ar, xi)), d);
-            RX(i, col) = 0.0;
-            IX(i, col) = 0.0;
-        }
-        __syncwarp();
-        for (int j = k; j < m; ++j) {
-            const double ar = RX(k, j), ai = IX(k, j);
-            for (int i = k + 1 + lane; i < m; i += 32) {
-                const double ur = w.u[i], ui = w.ui[i];
-                RX(i, j) = __dsub_rn(RX(i, j), __dsub_rn(__dmul_rn(ur, ar), __dmul_rn(ui, ai)));
-                IX(i, j) = __dsub_rn(IX(i, j), __dadd_rn(__dmul_rn(ur, ai), __dmul_rn(ui, ar)));
+        double ur[NP], uim[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const int i = k + 1 + lane + 32 * p;
+            ur[p] = 0.0;
+            uim[p] = 0.0;
+            if (i < m) {
+                const double ar = RX(i, col), ai = IX(i, col);
+                ur[p] = __ddiv_rn(__dadd_rn(__dmul_rn(ar, xr), __dmul_rn(ai, xi)), d);
+                uim[p] = __ddiv_rn(__dsub_rn(__dmul_rn(ai, xr), __dmul_rn(ar, xi)), d);
+                w.u[i] = ur[p];
+                w.ui[i] = uim[p];
+                RX(i, col) = 0.0;
+                IX(i, col) = 0.0;
             }
         }
         __syncwarp();
+#pragma unroll 2
+        for (int j = k; j < m; ++j) {
+            const double ar = RX(k, j), ai = IX(k, j);
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const int i = k + 1 + lane + 32 * p;
+                if (i < m) {
+                    const double vr = RX(i, j), vi = IX(i, j);
+                    RX(i, j) = __dsub_rn(vr, __dsub_rn(__dmul_rn(ur[p], ar), __dmul_rn(uim[p], ai)));
+                    IX(i, j) = __dsub_rn(vi, __dadd_rn(__dmul_rn(ur[p], ai), __dmul_rn(uim[p], ar)));
+                }
+            }
+        }
+        __syncwarp();
+        double sr[NP], si[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const int l = lane + 32 * p;
+            sr[p] = l < m ? RX(l, k) : 0.0;
+            si[p] = l < m ? IX(l, k) : 0.0;
+        }
+#pragma unroll 2
         for (int i = k + 1; i < m; ++i) {
             const double mr = w.u[i], mi = w.ui[i];
-            for (int l = lane; l < m; l += 32) {
-                const double r = RX(l, i), im = IX(l, i);
-                RX(l, k) = __dadd_rn(RX(l, k), __dsub_rn(__dmul_rn(mr, r), __dmul_rn(mi, im)));
-                IX(l, k) = __dadd_rn(IX(l, k), __dadd_rn(__dmul_rn(mr, im), __dmul_rn(mi, r)));
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const int l = lane + 32 * p;
+                if (l < m) {
+                    const double r = RX(l, i), im = IX(l, i);
+                    sr[p] = __dadd_rn(sr[p], __dsub_rn(__dmul_rn(mr, r), __dmul_rn(mi, im)));
+                    si[p] = __dadd_rn(si[p], __dadd_rn(__dmul_rn(mr, im), __dmul_rn(mi, r)));
+                }
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const int l = lane + 32 * p;
+            if (l < m) {
+                RX(l, k) = sr[p];
+                IX(l, k) = si[p];
             }
         }
         __syncwarp();
@@ -208,8 +308,18 @@ __device__ void hessenberg_split_exact(WarpWs &w, int m, int lane)
 #undef IX
 }
 
+__device__ void hessenberg_split_exact(WarpWs &w, int m, int lane)
+{
+    if (m <= 32) hessenberg_split_exact_np<1>(w, m, lane);
+    else if (m <= 64) hessenberg_split_exact_np<2>(w, m, lane);
+    else if (m <= 96) hessenberg_split_exact_np<3>(w, m, lane);
+    else hessenberg_split_exact_np<4>(w, m, lane);
+}
+
 // _charpoly_hessenberg!(C, H, m, n), src/hafnian.jl:454-492 (real), exact order.  Row k of C
-// (k = 0..m) holds p_k; C[k*(n+1) + t] is the coefficient of lambda^(k-t).
+// (k = 0..m) holds p_k; C[k*(n+1) + t] is the coefficient of lambda^(k-t).  Lane <-> t is fixed
+// (t = lane + 32p, n <= 63), and each lane keeps its coefficients of row k in registers while the
+// i loop updates them in the reference's order (i descending); the row is stored once at the end.
 __device__ void charpoly_real_exact(WarpWs &w, int m, int n, int lane)
 {
     const double *H = w.M;
@@ -223,10 +333,13 @@ __device__ void charpoly_real_exact(WarpWs &w, int m, int n, int lane)
         const int tmax = k < n ? k : n, prevmax = (k - 1) < n ? (k - 1) : n;
         const double *Cp = C + (size_t)(k - 1) * cs;
         double *Ck = C + (size_t)k * cs;
-        for (int t = lane; t <= n; t += 32) {
-            if (t == 0) Ck[0] = Cp[0];
-            else if (t <= tmax) Ck[t] = __dsub_rn(t <= prevmax ? Cp[t] : 0.0, __dmul_rn(hkk, Cp[t - 1]));
-            else Ck[t] = 0.0;
+        double ck[2];
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const int t = lane + 32 * p;
+            ck[p] = 0.0;
+            if (t == 0) ck[p] = Cp[0];
+            else if (t <= tmax) ck[p] = __dsub_rn(t <= prevmax ? Cp[t] : 0.0, __dmul_rn(hkk, Cp[t - 1]));
         }
         double beta = 1.0;
         const int ilo = 1 > k - n + 1 ? 1 : k - n + 1;
@@ -238,11 +351,17 @@ __device__ void charpoly_real_exact(WarpWs &w, int m, int n, int lane)
             if (coef != 0.0) {
                 const int tt = n < d + i - 1 ? n : d + i - 1;
                 const double *Ci = C + (size_t)(i - 1) * cs;
-                // Lane <-> t stays fixed across i, so each coefficient is updated in the
-                // reference's order (i descending) by one lane.
-                for (int t = lane; t <= tt; t += 32)
-                    if (t >= d) Ck[t] = __dsub_rn(Ck[t], __dmul_rn(coef, Ci[t - d]));
+#pragma unroll
+                for (int p = 0; p < 2; ++p) {
+                    const int t = lane + 32 * p;
+                    if (t >= d && t <= tt) ck[p] = __dsub_rn(ck[p], __dmul_rn(coef, Ci[t - d]));
+                }
             }
+        }
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const int t = lane + 32 * p;
+            if (t <= n) Ck[t] = ck[p];
         }
         __syncwarp();
     }
@@ -252,7 +371,8 @@ __device__ void charpoly_real_exact(WarpWs &w, int m, int n, int lane)
 __device__ __forceinline__ cd c_mul_x(cd a, cd b) { return x_cmul(a, b); }
 __device__ __forceinline__ cd c_sub_x(cd a, cd b) { return cd{__dsub_rn(a.re, b.re), __dsub_rn(a.im, b.im)}; }
 
-// Complex charpoly on the split storage (the band of Mr/Mi equals the copied-back M, :358-363).
+// Complex charpoly on the split storage (the band of Mr/Mi equals the copied-back M, :358-363);
+// row k's coefficients in registers as in the real form.
 __device__ void charpoly_cplx_exact(WarpWs &w, int m, int n, int lane)
 {
     const int ld = w.ldm, cs = n + 1;
@@ -265,10 +385,13 @@ __device__ void charpoly_cplx_exact(WarpWs &w, int m, int n, int lane)
         const int tmax = k < n ? k : n, prevmax = (k - 1) < n ? (k - 1) : n;
         const cd *Cp = C + (size_t)(k - 1) * cs;
         cd *Ck = C + (size_t)k * cs;
-        for (int t = lane; t <= n; t += 32) {
-            if (t == 0) Ck[0] = Cp[0];
-            else if (t <= tmax) Ck[t] = c_sub_x(t <= prevmax ? Cp[t] : cd{0.0, 0.0}, c_mul_x(hkk, Cp[t - 1]));
-            else Ck[t] = cd{0.0, 0.0};
+        cd ck[2];
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const int t = lane + 32 * p;
+            ck[p] = cd{0.0, 0.0};
+            if (t == 0) ck[p] = Cp[0];
+            else if (t <= tmax) ck[p] = c_sub_x(t <= prevmax ? Cp[t] : cd{0.0, 0.0}, c_mul_x(hkk, Cp[t - 1]));
         }
         cd beta{1.0, 0.0};
         const int ilo = 1 > k - n + 1 ? 1 : k - n + 1;
@@ -280,9 +403,17 @@ __device__ void charpoly_cplx_exact(WarpWs &w, int m, int n, int lane)
             if (!(coef.re == 0.0 && coef.im == 0.0)) {
                 const int tt = n < d + i - 1 ? n : d + i - 1;
                 const cd *Ci = C + (size_t)(i - 1) * cs;
-                for (int t = lane; t <= tt; t += 32)
-                    if (t >= d) Ck[t] = c_sub_x(Ck[t], c_mul_x(coef, Ci[t - d]));
+#pragma unroll
+                for (int p = 0; p < 2; ++p) {
+                    const int t = lane + 32 * p;
+                    if (t >= d && t <= tt) ck[p] = c_sub_x(ck[p], c_mul_x(coef, Ci[t - d]));
+                }
             }
+        }
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const int t = lane + 32 * p;
+            if (t <= n) Ck[t] = ck[p];
         }
         __syncwarp();
     }
