@@ -147,12 +147,12 @@ def _check_symmetric(A: np.ndarray) -> None:
         return
     X = np.asarray(A)
     kind = X.dtype.kind
+    neq = X != X.T  # comparisons raise no floating-point warnings
+    if not neq.any():
+        return
     real_t = np.float32 if X.dtype in (np.float32, np.complex64) else np.float64
     tol = float(np.finfo(real_t).eps)
     with np.errstate(invalid="ignore", over="ignore"):
-        neq = X != X.T
-        if not neq.any():
-            return
         if kind in "iub":
             Xf = X.astype(np.float64)
         else:
