@@ -161,6 +161,34 @@ def test_input_validation(egg, W):
         egg.hafnian(bad)
 
 
+def test_batch_symmetry_check_matches_per_matrix(egg, W):
+    # A batch checks every matrix as hafnian(As[b]) would (src/hafnian.jl:1297-1300); the stacked
+    # check raises the same error for the first offending matrix, as a list or as a 3-D array.
+    from theeggman_b200.hafnian import _check_symmetric, _check_symmetric_stack
+
+    mats = [W.dense_complex(8, 300 + b, 0.5) for b in range(6)]
+    near = mats[1].copy()
+    near[2, 5] = mats[1][5, 2] * (1 + np.sqrt(np.finfo(float).eps) / 8)  # inside the tolerance
+    mats[1] = near
+    _check_symmetric_stack(np.array(mats))
+    bad3, bad4 = mats[3].copy(), mats[4].copy()
+    bad3[6, 2] += 1
+    bad4[0, 1] += 1
+    mats[3], mats[4] = bad3, bad4
+    with pytest.raises(egg.ArgumentError) as one:
+        _check_symmetric(bad3)
+    for batch in (mats, np.array(mats)):
+        with pytest.raises(egg.ArgumentError) as got:
+            egg.hafnian(batch)
+        assert str(got.value) == str(one.value)
+    nan = np.ones((3, 4, 4))
+    nan[1, 2, 2] = np.nan  # the diagonal is not compared
+    _check_symmetric_stack(nan)
+    nan[2, 0, 3] = nan[2, 3, 0] = np.nan
+    with pytest.raises(egg.ArgumentError):
+        _check_symmetric_stack(nan)
+
+
 def test_degenerate_sizes_need_no_device(egg, W):
     # N = 0 -> 1, odd -> 0, total 0 -> 1, odd total -> 0: no kernel is reached (src/hafnian.jl:1121-1122)
     assert egg.hafnian(np.zeros((0, 0))) == 1

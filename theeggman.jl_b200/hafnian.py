@@ -168,6 +168,18 @@ def _check_symmetric(A: np.ndarray) -> None:
         raise ArgumentError(f"matrix is not symmetric at ({ii[0] + 1}, {jj[0] + 1})")
 
 
+def _check_symmetric_stack(S: np.ndarray) -> None:
+    """_check_symmetric for each matrix of a (B, N, N) stack in order: one comparison of the stack
+    with its transpose when every matrix is exactly symmetric (the usual case); otherwise the
+    per-matrix check, which reports the first matrix that is not symmetric to tolerance."""
+    if S.shape[1] < 2:
+        return
+    if not (S != S.transpose(0, 2, 1)).any():
+        return
+    for m in S:
+        _check_symmetric(m)
+
+
 # ----------------------------------------------------------------------------------------------
 # Device calls
 # ----------------------------------------------------------------------------------------------
@@ -527,13 +539,18 @@ def _hafnian_batch(As, *, nthreads, glynn, method, check_symmetric, backend, max
     exact_int = exact and all(d.kind in "iub" for d in dtypes)
     T = np.dtype(np.int64) if exact_int else np.result_type(*[_haf_dtype_of(d) for d in dtypes])
     N = _checksquare(mats[0])
-    if check_symmetric or len({m.shape for m in mats}) > 1:
+    stack = None
+    if len({m.shape for m in mats}) > 1:
         for b, m in enumerate(mats):
             if _checksquare(m) != N:
                 raise DimensionMismatch(f"matrix {b + 1} is {m.shape[0]}×{m.shape[1]}, expected {N}×{N}; a batch "
                                         "shares one strategy and one plan")
             if check_symmetric:
                 _check_symmetric(m)
+    else:
+        stack = As if isinstance(As, np.ndarray) and As.ndim == 3 else np.array(mats)
+        if check_symmetric:
+            _check_symmetric_stack(stack)
     if N == 0:
         return [1] * B if exact_int else np.ones(B, T)
     if N % 2:
@@ -548,7 +565,7 @@ def _hafnian_batch(As, *, nthreads, glynn, method, check_symmetric, backend, max
         # every instance has the same size, so they all choose alike.
         chosen = pol._choose_method_distinct(N, N // 2, 1)[0] if method == "auto" else method
     if chosen in ("unrolled", "dp"):
-        P = _gather_pairs_stack(T, np.stack(mats))
+        P = _gather_pairs_stack(T, np.ascontiguousarray(stack))
         return _dp_device(T, P, N, _dp_prec(prec), max_batch, exact_int)
     if exact_int:
         raise ArgumentError("exact integer hafnians run on the DP; pass method='dp'")
