@@ -24,13 +24,14 @@ namespace egg {
 // 128-thread blocks; resident blocks per SM from the tile's register need (65536 / (128 * blocks)
 // registers per thread): a real tile holds m doubles per row, a complex one 2m.
 // The reference-arithmetic tiles keep more values live per step (separately rounded products, the
-// buffered term series), so from 24 rows on they take one block fewer.
+// buffered term series), so from 18 rows on they take one block fewer, and from 22 rows two: the
+// fewer warps spill less (N = 40: 9.25 -> 8.98 ms against 6 and 5 blocks' worth).
 template <bool CPLX, int K, int G = 32, bool EXACT = false, bool ALL = false>
 struct LevelShape {
     static constexpr int MW = 2 * K;
     static constexpr int full =
         CPLX ? (MW <= 8 ? 6 : (MW <= 10 ? 5 : (MW <= 16 ? 4 : (MW <= 24 ? 3 : 2))))
-             : (MW <= 8 ? 8 : (MW <= 12 ? 7 : (MW <= 18 ? 6 : (MW <= (EXACT ? 22 : 26) ? 5 : (MW <= 32 ? 4 : 2)))));
+             : (MW <= 8 ? 8 : (MW <= 12 ? 7 : (MW <= (EXACT ? 16 : 18) ? 6 : (MW <= (EXACT ? 20 : 26) ? 5 : (MW <= 32 ? 4 : 2)))));
     // Two terms per warp need more registers per thread (the series holds two coefficients per
     // lane); one block fewer still keeps more terms in flight.
     static constexpr int per_sm = G == 32 ? full : (full > 2 ? full - 1 : 1);
@@ -442,8 +443,9 @@ __global__ void __launch_bounds__(LevelShape<CPLX, K, G, EXACT, ALL>::threads, L
 }
 
 // Warps per block of a level kernel: the shape's, except that a lockstep block takes only as many
-// warps as their workspaces fit in shared memory (the buffered series grow with N: 20 warps of the
-// 22-row tile fit up to N = 42, 15 at N = 62).
+// warps as their workspaces fit in shared memory (the buffered series grow with the order n: the
+// 17..20-row tiles keep their 20 warps up to n = 25, the 21..32-row tiles their 16 up to n = 26;
+// at n = 32 the 20-row tile holds 17 warps and the 32-row tile 14).
 template <bool CPLX, int K, int G, bool EXACT, bool ALL>
 inline int level_warps(int nmax)
 {
