@@ -23,15 +23,16 @@ namespace egg {
 
 // 128-thread blocks; resident blocks per SM from the tile's register need (65536 / (128 * blocks)
 // registers per thread): a real tile holds m doubles per row, a complex one 2m.
-// The reference-arithmetic tiles keep more values live per step (separately rounded products, the
-// buffered term series), so from 18 rows on they take one block fewer, and from 22 rows two: the
-// fewer warps spill less (N = 40: 9.25 -> 8.98 ms against 6 and 5 blocks' worth).
+// The real reference-arithmetic tiles keep more values live per step (separately rounded products,
+// the buffered term series) and run fewer blocks, whose larger register share spills less (the
+// N = 40 sieve 9.25 -> 8.91 ms against the fused tiles' block counts).
 template <bool CPLX, int K, int G = 32, bool EXACT = false, bool ALL = false>
 struct LevelShape {
     static constexpr int MW = 2 * K;
     static constexpr int full =
-        CPLX ? (MW <= 8 ? 6 : (MW <= 10 ? 5 : (MW <= 16 ? 4 : (MW <= 24 ? 3 : 2))))
-             : (MW <= 8 ? 8 : (MW <= 12 ? 7 : (MW <= (EXACT ? 16 : 18) ? 6 : (MW <= (EXACT ? 20 : 26) ? 5 : (MW <= 32 ? 4 : 2)))));
+        CPLX    ? (MW <= 8 ? 6 : (MW <= 10 ? 5 : (MW <= 16 ? 4 : (MW <= 24 ? 3 : 2))))
+        : EXACT ? (MW <= 8 ? 8 : (MW <= 12 ? 6 : (MW <= 20 ? 5 : (MW <= 32 ? 4 : 2))))
+                : (MW <= 8 ? 8 : (MW <= 12 ? 7 : (MW <= 18 ? 6 : (MW <= 26 ? 5 : (MW <= 32 ? 4 : 2)))));
     // Two terms per warp need more registers per thread (the series holds two coefficients per
     // lane); one block fewer still keeps more terms in flight.
     static constexpr int per_sm = G == 32 ? full : (full > 2 ? full - 1 : 1);
