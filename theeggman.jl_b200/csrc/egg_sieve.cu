@@ -687,6 +687,10 @@ static int64_t term_count(const int64_t *reps, int64_t E, int glynn)
 
 static int64_t align256(int64_t x) { return (x + 255) & ~(int64_t)255; }
 
+// Rounds of terms (the level's terms over the machine's warps in lockstep blocks) below which a
+// complex level runs in blocks of four warps instead.
+constexpr double kLockstepMinRounds = 8.0;
+
 int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
                     const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st,
                     const FixedScratch *fixed, double *terms, void *stage, size_t stage_cap)
@@ -920,6 +924,15 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
             int rc0 = cplx ? level_shape_cplx(nmax, k, narrow, exact, false, &cw, &bps)
                            : level_shape_real(nmax, k, narrow, exact, false, &cw, &bps);
             if (rc0) return rc0;
+            // A lockstep shape (one block of all an SM's warps) pays off over many rounds of terms;
+            // a complex level with fewer runs in blocks of four warps, several per SM, as the
+            // other shapes do.  The complex N = 40 sieve took 30.77 -> 29.87 ms with its large
+            // levels in lockstep; at N = 24 and 32, whose levels have few rounds, lockstep blocks
+            // were 10 % and 3.5 % slower.
+            if (cplx && cw > 4 && lvl[(size_t)k] < kLockstepMinRounds * (double)num_sms * cw) {
+                bps = cw / 4;
+                cw = 4;
+            }
             if (bps < 1 || (size_t)cw * (narrow ? 2 : 1) * level_ws_bytes(nmax, cplx, k, exact) > 220 * 1024)
                 return fail(EGG_ERR_TOO_LARGE, "sieve workspace exceeds shared memory");
             // Distinct-row levels deal equal shares: one wave.  Odometer runs are only balanced on
@@ -1019,6 +1032,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
     a.maxrep = maxrep;
     a.Emax = Ews;
     a.nmax = nmax;
+    a.block_warps = 0;
     a.skip_le = skip_le;
     a.terms = terms;
     if (terms) {
@@ -1069,6 +1083,7 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
         const int64_t *dstr = (const int64_t *)(base + off_str);
         for (const FastLaunch &L : fl) {
             a.warps_per_inst = L.bx * L.cw;
+            a.block_warps = fused ? 0 : L.cw;
             cudaStream_t ls = st;
             if (side_ok && L.side) ls = c.side[next_side++ % Context::kSideStreams];
             if (fused)

@@ -23,6 +23,7 @@ struct SieveArgs {
     dd *partial;           // exact kernel: [B][warps_per_inst][2]
     double *terms;         // if set (one instance, exact kernel only): term j's value at j (complex: 2j, 2j+1)
     int maxrep, warps_per_inst, Emax, nmax;
+    int block_warps;       // level launches: warps per block when below the shape's own (0: the shape's)
     int skip_le;           // the exact kernel leaves terms with m <= skip_le to the fast kernels
     // Term lists of repeated multiplicity patterns: the digits of each term of pattern p and level k
     // (4 bits per edge, edge i at bits 4i..4i+3) at lists[list_off[p * list_stride + k] ..

@@ -36,12 +36,14 @@ struct LevelShape {
     // Two terms per warp need more registers per thread (the series holds two coefficients per
     // lane); one block fewer still keeps more terms in flight.
     static constexpr int per_sm = G == 32 ? full : (full > 2 ? full - 1 : 1);
-    // Lockstep: the reference-arithmetic real tiles of 17..32 rows run as ONE block per SM holding
-    // all of its warps, which take their terms in rounds separated by a block barrier.  Each term
-    // runs about 5 k instructions of straight-line code (every Hessenberg step is its own code), and
+    // Lockstep: the reference-arithmetic tiles of 17..32 rows run as ONE block per SM holding all
+    // of its warps, which take their terms in rounds separated by a block barrier.  Each term runs
+    // about 5 k instructions of straight-line code (every Hessenberg step is its own code), and
     // warps spread over different parts of it stall on instruction fetch; in lockstep the warps of
-    // an SM run the same part at the same time.  The N = 40 sieve took 10.52 -> 9.67 ms.
-    static constexpr bool lockstep = !ALL && EXACT && !CPLX && G == 32 && MW > 16 && MW <= 32;
+    // an SM run the same part at the same time.  The real N = 40 sieve took 10.52 -> 9.67 ms.  The
+    // launch planner may instead launch such a kernel in blocks of four warps (SieveArgs::
+    // block_warps): a complex level with few rounds of terms (egg_sieve.cu, kLockstepMinRounds).
+    static constexpr bool lockstep = !ALL && EXACT && G == 32 && MW > 16 && MW <= 32;
     static constexpr int threads = lockstep ? 128 * per_sm : 128;
     static constexpr int min_blocks = lockstep ? 1 : per_sm;
 };
@@ -464,7 +466,8 @@ inline int level_warps(int nmax)
 template <bool CPLX, int K, int G, bool EXACT = false>
 static int level_launch_k(const SieveArgs &a, const int64_t *strides, int B, dd *partial, int blocks_x, cudaStream_t st)
 {
-    const int cw = level_warps<CPLX, K, G, EXACT, false>(a.nmax);
+    int cw = level_warps<CPLX, K, G, EXACT, false>(a.nmax);
+    if (a.block_warps > 0 && a.block_warps < cw) cw = a.block_warps;  // the planner's smaller blocks
     const size_t smem = (size_t)cw * (32 / G) * level_ws_doubles<CPLX, K, EXACT>(a.nmax) * sizeof(double);
     auto k = sieve_level_kernel<CPLX, K, G, false, EXACT>;
     int rc = smem_limit_at_least((const void *)k, smem);
