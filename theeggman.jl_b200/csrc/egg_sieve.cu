@@ -688,8 +688,8 @@ static int64_t term_count(const int64_t *reps, int64_t E, int glynn)
 static int64_t align256(int64_t x) { return (x + 255) & ~(int64_t)255; }
 
 // Rounds of terms (the level's terms over the machine's warps in lockstep blocks) below which a
-// complex level runs in blocks of four warps instead.
-constexpr double kLockstepMinRounds = 8.0;
+// level runs in blocks of four warps instead: complex and real tiles.
+constexpr double kLockstepMinRoundsCplx = 8.0, kLockstepMinRoundsReal = 3.0;
 
 int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dAx, const int64_t *E,
                     const int64_t *edge_reps, const int32_t *glynn, void *dout, cudaStream_t st,
@@ -925,11 +925,13 @@ int sieve_batch_run(int dtype, int prec, int64_t B, int64_t Emax, const void *dA
                            : level_shape_real(nmax, k, narrow, exact, false, &cw, &bps);
             if (rc0) return rc0;
             // A lockstep shape (one block of all an SM's warps) pays off over many rounds of terms;
-            // a complex level with fewer runs in blocks of four warps, several per SM, as the
-            // other shapes do.  The complex N = 40 sieve took 30.77 -> 29.87 ms with its large
-            // levels in lockstep; at N = 24 and 32, whose levels have few rounds, lockstep blocks
-            // were 10 % and 3.5 % slower.
-            if (cplx && cw > 4 && lvl[(size_t)k] < kLockstepMinRounds * (double)num_sms * cw) {
+            // a level with fewer runs in blocks of four warps, several per SM, as the other shapes
+            // do.  The complex N = 40 sieve took 30.77 -> 29.87 ms with its large levels in
+            // lockstep (at N = 24 and 32, whose levels have few rounds, lockstep blocks were 10 %
+            // and 3.5 % slower); the real N = 32 sieve 0.686 -> 0.656 ms with its levels of under
+            // three rounds in four-warp blocks (N = 40 unchanged; under eight rounds, 1 % slower).
+            const double min_rounds = cplx ? kLockstepMinRoundsCplx : kLockstepMinRoundsReal;
+            if (cw > 4 && lvl[(size_t)k] < min_rounds * (double)num_sms * cw) {
                 bps = cw / 4;
                 cw = 4;
             }

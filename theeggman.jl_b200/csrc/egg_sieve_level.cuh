@@ -42,7 +42,7 @@ struct LevelShape {
     // warps spread over different parts of it stall on instruction fetch; in lockstep the warps of
     // an SM run the same part at the same time.  The real N = 40 sieve took 10.52 -> 9.67 ms.  The
     // launch planner may instead launch such a kernel in blocks of four warps (SieveArgs::
-    // block_warps): a complex level with few rounds of terms (egg_sieve.cu, kLockstepMinRounds).
+    // block_warps): a level with few rounds of terms (egg_sieve.cu, kLockstepMinRounds*).
     static constexpr bool lockstep = !ALL && EXACT && G == 32 && MW > 16 && MW <= 32;
     static constexpr int threads = lockstep ? 128 * per_sm : 128;
     static constexpr int min_blocks = lockstep ? 1 : per_sm;
