@@ -143,8 +143,8 @@ def main():
     out["random"] = cases
 
     # The distributions of the N = 40 sieve workloads, at N = 24 where 256-bit gold is cheap (the
-    # error check BASELINE's sieve configuration asks for, and the N of the reference's own
-    # envelope test, test/runtests.jl:123-133): real U[-1, 1]/sqrt(N), complex parts N(0, 1/(2N)).
+    # error check of the N = 40 sieve configuration, at the N of the reference's own envelope
+    # test, test/runtests.jl:123-133): real U[-1, 1]/sqrt(N), complex parts N(0, 1/(2N)).
     c2 = []
     for i in range(4):
         for kind in ("real", "complex"):
