@@ -70,6 +70,7 @@ def rel_err(a, b) -> float:
 
 # The committed ncu summary (kernel and workload) whose DRAM traffic figure belongs to a workload.
 PROFILE_OF = {"sieve40": "sieve_level_kernel_exact_sieve40.md", "sieve40f": "sieve_level_kernel_sieve40.md",
+              "sieve40c": "sieve_level_kernel_exact_sieve40c.md",
               "sieve40cf": "sieve_level_kernel_sieve40c.md", "sieve40gf": "sieve_level_kernel_sieve40g.md",
               "rep14f": "sieve_level_kernel_rep14.md", "dp40": "dpc_fixed_kernel_dp40.md",
               "dp20": "dpc_cluster_kernel_dp20.md", "mix4096": "dpc_fixed_kernel_mix4096.md"}
